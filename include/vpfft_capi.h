@@ -1,0 +1,280 @@
+/*
+ * vpfft_capi.h -- C ABI of vpfft_b200, a B200 (sm_100a) implementation of
+ * VPFFT's fixed-point solve on a periodic 3D voxel polycrystal.
+ *
+ * Plain C types only (pointers, sizes, doubles); no exceptions cross this
+ * boundary and nothing calls exit(): every entry point returns a vpfft_status.
+ * Host arrays are caller-owned and only read or written during the call.
+ *
+ * Layout conventions (the reference's, so arrays written for it can be passed
+ * unchanged):
+ *   voxel index        v = x*Ny*Nz + y*Nz + z            (MaterialGrid.h:121-124)
+ *   orientation R      9 doubles per voxel, row-major 3x3 (SMatrix3x3, LinearAlgebra.h:114)
+ *   5-vectors          deviatoric basis coefficients      (EigenRep, LinearAlgebra.h:298-521;
+ *                      basis EigenBasis, LinearAlgebra.h:207-247)
+ *   5x5 matrices       column-major m[j*5+i]              (SMatrix5x5, LinearAlgebra.h:574)
+ *   per-voxel arrays   voxel-major: R[v*9+k], sigma[v*5+c], crss[v*12+s]
+ *
+ * Threading: a vpfft_grid is bound to the CUDA device current at creation and
+ * owns one CUDA stream; it is not thread-safe.  Different grids may be used
+ * from different threads.
+ */
+#ifndef VPFFT_CAPI_H
+#define VPFFT_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VPFFT_NUM_SLIP_SYSTEMS 12
+
+typedef enum {
+  VPFFT_OK = 0,
+  VPFFT_ERR_INVALID_ARGUMENT = 1,
+  VPFFT_ERR_UNSUPPORTED_SIZE = 2, /* a grid dimension is not a product of 2, 3 and 5, or > 512 */
+  VPFFT_ERR_CUDA = 3,             /* a CUDA runtime call failed; see vpfft_last_error() */
+  VPFFT_ERR_OUT_OF_MEMORY = 4,
+  VPFFT_ERR_NO_DEVICE = 5,        /* no usable CUDA device: there is no CPU fallback */
+  VPFFT_ERR_MAX_RSS_TINY = 6,     /* a voxel's max resolved shear stress < 1e-10
+                                     (the reference exits: MaterialGrid.h:560-564,
+                                     MaterialGrid.cpp:186-190) */
+  VPFFT_ERR_NONFINITE = 7,        /* NaN/Inf produced (e.g. singular reference medium) */
+  VPFFT_ERR_NOT_INITIALIZED = 8,  /* fields not set before a solve */
+  VPFFT_ERR_IO = 9,               /* file could not be read or parsed */
+  VPFFT_ERR_CANCELLED = 10,
+  VPFFT_ERR_TIMEOUT = 11
+} vpfft_status;
+
+typedef enum {
+  VPFFT_PREC_FP64 = 0,  /* everything in FP64: the GPU oracle path */
+  VPFFT_PREC_MIXED = 1  /* FP32 fields, FFT and Green operator; FP64 Newton-Raphson
+                           residual/Jacobian and FP64 compensated reductions */
+} vpfft_precision;
+
+/* Per-slip-system material constants.  The reference hard-codes them in
+ * MaterialGrid::InitializeMemory (MaterialGrid.cpp:322-336, 390); the
+ * defaults below (vpfft_material_default) are those values. */
+typedef struct {
+  double gamma_dot_base[VPFFT_NUM_SLIP_SYSTEMS];  /* reference rate, default 15.5 */
+  int32_t rate_sensitivity[VPFFT_NUM_SLIP_SYSTEMS]; /* power-law exponent n, default 10 */
+  double crss[VPFFT_NUM_SLIP_SYSTEMS];            /* initial CRSS tau_s, default 11 */
+  double tau0[VPFFT_NUM_SLIP_SYSTEMS];            /* Voce tau0, default 11 */
+  double tau1[VPFFT_NUM_SLIP_SYSTEMS];            /* Voce tau1, default 11 */
+  double theta0[VPFFT_NUM_SLIP_SYSTEMS];          /* Voce theta0, default 430 */
+  double theta1[VPFFT_NUM_SLIP_SYSTEMS];          /* Voce theta1, default 110 */
+  double hardening[VPFFT_NUM_SLIP_SYSTEMS * VPFFT_NUM_SLIP_SYSTEMS]; /* h[s*12+t], default 1 */
+} vpfft_material;
+
+/* Newton-Raphson and fixed-point constants.  The reference hard-codes them
+ * (MaterialGrid.cpp:159-160, 909-911); defaults are those values. */
+typedef struct {
+  double init_nr_epsilon;     /* 5e-4  (InitializeComputation) */
+  int32_t init_nr_max_iter;   /* 1000 */
+  double nr_epsilon;          /* 5e-4  (fixed-point loop) */
+  double nr_max_resolved;     /* 1e9 */
+  int32_t nr_max_iter;        /* 100 */
+  int32_t pad_;
+} vpfft_solver_options;
+
+typedef struct {
+  int32_t iterations;         /* fixed-point iterations executed */
+  int32_t converged;          /* 1 when both error norms fell below epsilon */
+  double stress_error;        /* final delta_sigma (MaterialGrid.cpp:1052) */
+  double strain_rate_error;   /* final delta_eps   (MaterialGrid.cpp:1053) */
+  double avg_strain_rate[5];  /* <edot> of the last iteration */
+  int64_t nr_not_converged;   /* voxel-iterations whose NR hit its cap */
+  int32_t status_bits;        /* OR of device-side warnings */
+  int32_t pad_;
+  double seconds_init;        /* InitializeComputation + reference medium */
+  double seconds_loop;        /* the fixed-point loop */
+  double seconds_post;        /* texture, voxel length, hardening */
+  double L0[25];              /* reference medium of the increment, column-major */
+} vpfft_stats;
+
+typedef enum {
+  VPFFT_FIELD_STRESS = 0,          /* N x 5   Stress(x,y,z)            MaterialGrid.h:166-173 */
+  VPFFT_FIELD_LAGRANGE = 1,        /* N x 5   LagrangeMultiplier       MaterialGrid.h:178-185 */
+  VPFFT_FIELD_ORIENTATION = 2,     /* N x 9   Orientation              MaterialGrid.h:129-136 */
+  VPFFT_FIELD_CRSS = 3,            /* N x 12  CRSS                     MaterialGrid.h:431-434 */
+  VPFFT_FIELD_ACCUMULATED_SHEAR = 4, /* N     AccumulatedShear         MaterialGrid.h:293 */
+  VPFFT_FIELD_POLARIZATION = 5,    /* N x 5   Re PolarizationField of the last iteration */
+  VPFFT_FIELD_STRAIN_RATE_VARIATION = 6, /* N x 5 Re DisplacementVariation (d~) of the last iteration */
+  VPFFT_FIELD_STRAIN_RATE = 7,     /* N x 5   ApplyConstitutiveEquations(sigma) */
+  VPFFT_FIELD_SCHMID = 8           /* N x 60  SchmidtTensorList (12 x 5 per voxel) */
+} vpfft_field;
+
+typedef struct vpfft_grid vpfft_grid;
+
+/* ------------------------------------------------------------------ library */
+const char *vpfft_version(void);
+const char *vpfft_status_string(vpfft_status s);
+/* number of usable CUDA devices (0 on a machine without a GPU) */
+int vpfft_device_count(void);
+void vpfft_material_default(vpfft_material *m);
+void vpfft_solver_options_default(vpfft_solver_options *o);
+
+/* ------------------------------------------------------------------ MaterialGrid
+ * Replaces VPFFT::DataStructures::MaterialGrid (MaterialGrid.h:59-577).     */
+
+/* MaterialGrid(int DimX, int DimY, int DimZ) (MaterialGrid.h:72-78) + InitializeMemory
+ * (MaterialGrid.cpp:312-394).  material/options may be NULL for the defaults. */
+vpfft_status vpfft_grid_create(int nx, int ny, int nz, const vpfft_material *material,
+                               const vpfft_solver_options *options, vpfft_precision precision,
+                               vpfft_grid **out);
+/* The reference never frees (no destructor; Cleanup is private and unused,
+ * MaterialGrid.cpp:287-305). */
+vpfft_status vpfft_grid_destroy(vpfft_grid *g);
+/* NumX/NumY/NumZ (MaterialGrid.h:235-237) */
+vpfft_status vpfft_grid_dims(const vpfft_grid *g, int *nx, int *ny, int *nz);
+/* SendDataAndInitialize(SMatrix3x3*, EigenRep*) (MaterialGrid.cpp:425-534):
+ * copies orientations (N x 9) and stresses (N x 5, may be NULL = zeros) to the
+ * device and resets CRSS to the material's initial values. */
+vpfft_status vpfft_grid_set_fields(vpfft_grid *g, const double *orientations,
+                                   const double *stress);
+/* Same, from device pointers already holding the arrays (FP64, same layout). */
+vpfft_status vpfft_grid_set_fields_device(vpfft_grid *g, const double *d_orientations,
+                                          const double *d_stress);
+/* SetVoxelLength (MaterialGrid.h:97-102) */
+vpfft_status vpfft_grid_set_voxel_length(vpfft_grid *g, double hx, double hy, double hz);
+vpfft_status vpfft_grid_get_voxel_length(const vpfft_grid *g, double h[3]);
+/* Per-voxel CRSS (N x 12) or NULL to reset to the material's uniform values
+ * (LocalCRSS, MaterialGrid.cpp:384-391). */
+vpfft_status vpfft_grid_set_crss(vpfft_grid *g, const double *crss);
+/* Read any field to a host buffer (see vpfft_field for sizes); FP32 fields
+ * are widened to double. */
+vpfft_status vpfft_grid_get_field(vpfft_grid *g, vpfft_field which, double *dst);
+/* Write a field from a host buffer (snapshot/restore). */
+vpfft_status vpfft_grid_set_field(vpfft_grid *g, vpfft_field which, const double *src);
+
+/* RunSingleStrainStep(Edot, NumMaxIterations, TimeStep, ConvergenceEpsilon) -> <sigma>
+ * (MaterialGrid.cpp:897-1084).  stats may be NULL. */
+vpfft_status vpfft_run_single_strain_step(vpfft_grid *g, const double edot[5], int max_iter,
+                                          double dt, double eps, double avg_stress_out[5],
+                                          vpfft_stats *stats);
+
+/* Callback after every increment of vpfft_run: step index, accumulated macroscopic
+ * strain and <sigma> (the row RunVPFFT writes to Stress_Strain.txt,
+ * MaterialGrid.cpp:1217-1226).  Return nonzero to stop. */
+typedef int (*vpfft_step_callback)(int step, const double strain5[5], const double stress5[5],
+                                   void *user);
+/* RunVPFFT (MaterialGrid.cpp:1202-1228).  If stress_strain_path is not NULL the
+ * same text file as the reference is written there. */
+vpfft_status vpfft_run(vpfft_grid *g, const double edot[5], int max_iter, int n_steps, double dt,
+                       double eps, const char *stress_strain_path, vpfft_step_callback cb,
+                       void *user);
+
+/* --- phases of RunSingleStrainStep, for drivers that time or script them --- */
+/* InitializeComputation (MaterialGrid.cpp:153-210) */
+vpfft_status vpfft_initialize_computation(vpfft_grid *g, const double edot[5]);
+/* BuildLinearRefMediumStiffness (MaterialGrid.cpp:219-282); L0 out column-major */
+vpfft_status vpfft_build_reference_medium(vpfft_grid *g, double L0_out[25]);
+/* The fixed-point loop body (MaterialGrid.cpp:930-1068) run until convergence or
+ * max_iter; needs the two phases above first.  history (may be NULL) receives
+ * 12 doubles per iteration: <sigma>(5), <edot>(5), delta_sigma, delta_eps. */
+vpfft_status vpfft_fixed_point(vpfft_grid *g, const double edot[5], int max_iter, double eps,
+                               double *history, vpfft_stats *stats);
+/* OrientationEvolutionWithFFT + UpdateVoxelLength + UpdateHardeningCRSS
+ * (MaterialGrid.cpp:1074-1080, 769-876, 1190-1196, 1127-1157) */
+vpfft_status vpfft_post_increment(vpfft_grid *g, const double edot[5], double dt);
+/* Blocks until the grid's stream is idle. */
+vpfft_status vpfft_grid_synchronize(vpfft_grid *g);
+/* The grid's CUDA stream (a cudaStream_t), for callers that time with events. */
+void *vpfft_grid_stream(vpfft_grid *g);
+/* Count of this library's kernel launches on the grid so far. */
+int64_t vpfft_grid_launch_count(const vpfft_grid *g);
+/* Last error message of the grid (or of the library when g is NULL). */
+const char *vpfft_last_error(const vpfft_grid *g);
+
+/* ------------------------------------------------------------------ Solvers
+ * Batched device versions of the per-voxel routines of VPFFT::Solvers
+ * (Solvers.h:51-153).  All arrays are host arrays of n voxels; schmid is
+ * n x 12 x 5, crss n x 12.  They run on the current CUDA device.        */
+
+/* SolveConstitutiveEquations (Solvers.cpp:19-101) */
+vpfft_status vpfft_solve_constitutive(int n, const double *stress0, const double *schmid,
+                                      const double *crss, const vpfft_material *m,
+                                      const double edot[5], double eps, double max_rss,
+                                      int max_iter, double *stress_out);
+/* SolveConstrainedConstitutiveEquations (Solvers.cpp:111-222); L0 column-major;
+ * nr_error (may be NULL) gets NR_Error_Out per voxel. */
+vpfft_status vpfft_solve_constrained_constitutive(int n, const double *stress0,
+                                                  const double *schmid, const double *crss,
+                                                  const vpfft_material *m, const double edot[5],
+                                                  const double *lambda, const double *dtilde,
+                                                  const double L0[25], double eps,
+                                                  double max_rss, int max_iter,
+                                                  double *stress_out, double *nr_error);
+/* ApplyConstitutiveEquations (Solvers.cpp:255-274) */
+vpfft_status vpfft_apply_constitutive(int n, const double *stress, const double *schmid,
+                                      const double *crss, const vpfft_material *m,
+                                      double *strain_rate_out);
+/* SolveSachEquation (Solvers.cpp:230-243) */
+vpfft_status vpfft_solve_sachs(int n, const double *schmid, const double *crss,
+                               const double edot[5], double *stress_out);
+/* UpdateSchmidtTensors for n orientations (MaterialGrid.cpp:107-124): n x 9 -> n x 60 */
+vpfft_status vpfft_schmid_tensors(int n, const double *orientations, double *schmid_out);
+/* The symmetrised, projected Green operator applied to n complex 5-vectors at
+ * wave-vector indices (ix,iy,iz) of an nx x ny x nz grid with voxel lengths h,
+ * including the Nyquist-plane override and the Hermitian average of k and -k
+ * that the reference's "real part of a c2c transform" amounts to
+ * (MaterialGrid.cpp:682-743, 583-615).  phat/dhat: n x 5 x 2 (re, im). */
+vpfft_status vpfft_green_apply(int n, const int32_t *k_index, int nx, int ny, int nz,
+                               const double h[3], const double L0[25], const double *phat,
+                               double *dhat, vpfft_precision precision);
+
+/* ------------------------------------------------------------------ FFT
+ * The device 3D real<->half-complex transform used by the solve, exposed for
+ * testing: forward is unnormalised (FFTW_FORWARD sign), inverse divides by N.
+ * real: n_comp x N (component-major); spec: n_comp x nx x ny x (nz/2+1) x 2. */
+vpfft_status vpfft_fft3d_r2c(int nx, int ny, int nz, int n_comp, const double *real,
+                             double *spec, vpfft_precision precision);
+vpfft_status vpfft_fft3d_c2r(int nx, int ny, int nz, int n_comp, const double *spec,
+                             double *real, vpfft_precision precision);
+
+/* ------------------------------------------------------------------ fixtures
+ * Host-only generators of synthetic microstructures (no GPU needed). */
+/* Periodic Voronoi polycrystal: n_grains seeds uniform in [0,nx)x[0,ny)x[0,nz),
+ * each voxel takes the orientation of the nearest seed under the minimum-image
+ * distance (ties -> lower seed index); orientations are uniform on SO(3) by
+ * Shoemake's method.  Pseudo-random numbers: SplitMix64 seeded with `seed`.
+ * orientations_out: N x 9; grain_out (may be NULL): N int32 seed index. */
+vpfft_status vpfft_fixture_polycrystal(int nx, int ny, int nz, int n_grains, uint64_t seed,
+                                       double *orientations_out, int32_t *grain_out);
+/* EigenRep(SMatrix3x3) of a velocity gradient (LinearAlgebra.h:307-312): only
+ * the symmetric part survives the projection. */
+void vpfft_edot_from_matrix(const double L[9], double edot_out[5]);
+/* EigenRep::ToMatrixRep (LinearAlgebra.h:352-360) */
+void vpfft_matrix_from_edot(const double edot[5], double L_out[9]);
+
+/* ------------------------------------------------------------------ config
+ * Utilities::ConfigFile (Config.h:21-85, Config.cpp:11-300) with its defects
+ * fixed: slip-system lists are read into indices 0..11 (the reference writes
+ * 1..12 into size-12 vectors), Parse returns its status, continuation lines
+ * are detected correctly, and NRTolerence/TimeStep are double.  Errors are
+ * returned, never exit(). */
+typedef struct {
+  int32_t num_x, num_y, num_z;       /* GridDimension */
+  double input_strain_rate[9];       /* InputStrainRate, row-major 3x3 */
+  int32_t max_nr_iter;               /* MaxNRIter */
+  double nr_tolerance;               /* NRTolerence */
+  double time_step;                  /* TimeStep */
+  int32_t num_time_iter;             /* NumTimeIter */
+  int32_t init_method;               /* 0 = TwoGrainInit, 1 = FileInit */
+  char input_microstructure[1024];   /* FileInit filename */
+  vpfft_material material;           /* CRSS, GammaDotBase, RateSensitivity, Tau0, Tau1,
+                                        Theta0, Theta1, HardeningMatrix */
+  double voxel_length[3];            /* VoxelLength (default 1 1 1) */
+  double convergence_epsilon;        /* ConvergenceEpsilon (default 1e-5) */
+  int32_t max_iter;                  /* MaxIter: fixed-point iterations (default 100) */
+  int32_t precision;                 /* Precision: FP64 | MIXED (default FP64) */
+} vpfft_config;
+vpfft_status vpfft_config_read(const char *path, vpfft_config *out, char *err, size_t err_len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VPFFT_CAPI_H */

@@ -23,7 +23,7 @@
 //     forward FFT of polarization component 0 (MaterialGrid.cpp:639, 780):
 //     at that moment they hold P and d~ produced by the previous iteration.
 //
-// Usage: vpfft_ref <input.bin> <outdir> [--dump-iter K]... [--quiet]
+// Usage: vpfft_ref <input.bin> <outdir> [--dump-iter K]... [--dump-increments] [--quiet]
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -189,12 +189,14 @@ int main(int argc, char **argv) {
     std::fprintf(stderr, "usage: vpfft_ref <input.bin> <outdir> [--dump-iter K]... [--quiet]\n");
     return 2;
   }
-  bool quiet = false;
+  bool quiet = false, dump_increments = false;
   for (int a = 3; a < argc; ++a) {
     if (!std::strcmp(argv[a], "--dump-iter") && a + 1 < argc)
       g_obs.dump_iters.push_back(std::atoi(argv[++a]));
     else if (!std::strcmp(argv[a], "--quiet"))
       quiet = true;
+    else if (!std::strcmp(argv[a], "--dump-increments"))
+      dump_increments = true;
   }
   Input in = read_input(argv[1]);
   const size_t N = (size_t)in.nx * in.ny * in.nz;
@@ -248,6 +250,17 @@ int main(int argc, char **argv) {
     step_seconds.push_back(std::chrono::duration<double>(t1 - t0).count());
     // P and d~ of the last fixed-point iteration are the last snapshot taken,
     // at the forward FFT that starts OrientationEvolutionWithFFT.
+    if (dump_increments) {
+      const std::string pre = g_obs.outdir + "/inc" + std::to_string(step) + "_";
+      write_bin(pre + "sigma.bin", reinterpret_cast<const double *>(grid.StressField), N * 5);
+      write_bin(pre + "lambda.bin",
+                reinterpret_cast<const double *>(grid.LagrangeMultiplierField.data()), N * 5);
+      write_bin(pre + "R.bin", reinterpret_cast<const double *>(grid.OrientationField), N * 9);
+      std::vector<double> cr(N * 12);
+      for (size_t v = 0; v < N; ++v)
+        for (int s = 0; s < 12; ++s) cr[v * 12 + s] = grid.LocalCRSS[v][s];
+      write_bin(pre + "crss.bin", cr.data(), cr.size());
+    }
   }
   std::cout.rdbuf(saved);
 

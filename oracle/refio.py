@@ -117,10 +117,11 @@ def read_output(outdir: str, n: int) -> dict:
         out[name] = _rd(outdir, name + ".bin", (n, w))
     out["accshear"] = _rd(outdir, "accshear.bin")
     out["voxlen"] = _rd(outdir, "voxlen.bin")
+    widths = {"sigma": 5, "lambda": 5, "R": 9, "crss": 12, "P": 5, "dtilde": 5}
     for fn in os.listdir(outdir):
-        if fn.startswith("it") and fn.endswith(".bin"):
+        if (fn.startswith("it") or fn.startswith("inc")) and fn.endswith(".bin"):
             key = fn[:-4]
-            out[key] = _rd(outdir, fn, (n, 5))
+            out[key] = _rd(outdir, fn, (n, widths[key.split("_", 1)[1]]))
     return out
 
 
@@ -164,13 +165,16 @@ def iteration_history(out: dict, dims) -> list:
     return hist
 
 
-def run(binary: str, case: Case, workdir: str, dump_iters=(), timeout=None) -> dict:
+def run(binary: str, case: Case, workdir: str, dump_iters=(), dump_increments=False,
+        timeout=None) -> dict:
     os.makedirs(workdir, exist_ok=True)
     inp = os.path.join(workdir, "input.bin")
     write_input(inp, case)
     cmd = [binary, inp, workdir, "--quiet"]
     for k in dump_iters:
         cmd += ["--dump-iter", str(int(k))]
+    if dump_increments:
+        cmd += ["--dump-increments"]
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
     if r.returncode != 0:
         raise RuntimeError(f"{binary} failed ({r.returncode}): {r.stderr[-2000:]}")

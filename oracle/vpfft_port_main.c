@@ -3,7 +3,7 @@
  * same input file and output files as ref_harness.cpp (see oracle/refio.py),
  * so tests can run either oracle interchangeably.  TEST ORACLE ONLY.
  *
- * Usage: vpfft_port <input.bin> <outdir> [--dump-iter K]... [--quiet]
+ * Usage: vpfft_port <input.bin> <outdir> [--dump-iter K]... [--dump-increments] [--quiet]
  */
 #define _POSIX_C_SOURCE 199309L
 #include <stdint.h>
@@ -104,9 +104,12 @@ int main(int argc, char **argv) {
   ctx_t c;
   memset(&c, 0, sizeof(c));
   c.outdir = argv[2];
+  int dump_increments = 0;
   for (int a = 3; a < argc; ++a) {
     if (!strcmp(argv[a], "--dump-iter") && a + 1 < argc && c.ndump < 64)
       c.dump[c.ndump++] = atoi(argv[++a]);
+    else if (!strcmp(argv[a], "--dump-increments"))
+      dump_increments = 1;
   }
   FILE *f = fopen(argv[1], "rb");
   if (!f) die("cannot open input");
@@ -170,6 +173,18 @@ int main(int argc, char **argv) {
     memcpy(steps + 6 * s + 1, avg, sizeof(avg));
     counts[s] = (double)(c.nar - ar0);
     secs[s] = t1 - t0;
+    if (dump_increments) {
+      const char *names[4] = {"sigma", "lambda", "R", "crss"};
+      const size_t widths[4] = {5, 5, 9, 12};
+      double *buf = (double *)malloc(sizeof(double) * 12 * n);
+      for (int k = 0; k < 4; ++k) {
+        char fn[64];
+        snprintf(fn, sizeof(fn), "inc%d_%s.bin", s, names[k]);
+        oracle_grid_get(g, names[k], buf);
+        wr(c.outdir, fn, buf, widths[k] * n);
+      }
+      free(buf);
+    }
   }
   const char *od = c.outdir;
   wr(od, "steps.bin", steps, 6 * (size_t)nsteps);

@@ -1,0 +1,1043 @@
+// capi.cu -- host implementation of the C ABI declared in include/vpfft_capi.h.
+//
+// A vpfft_grid owns the device-resident state of one RVE (representative
+// volume element): orientation, stress, Lagrange multiplier, CRSS and
+// accumulated shear as component-major arrays, one real work field (P / d~),
+// the half spectrum and the twiddle tables, plus a CUDA stream.  The host only
+// sequences kernels; all per-voxel and per-wave-vector arithmetic runs on the
+// device.  There is no CPU fallback: without a CUDA device every entry point
+// that needs one returns VPFFT_ERR_NO_DEVICE.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/vpfft_capi.h"
+#include "kernels.h"
+
+using namespace vpfft;
+
+struct vpfft_grid {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int nx = 0, ny = 0, nz = 0, nh = 0;
+  long long n = 0;
+  vpfft_precision prec = VPFFT_PREC_FP64;
+  vpfft_material mat{};
+  vpfft_solver_options opt{};
+  double h[3] = {1, 1, 1};
+  bool fields_set = false;
+  bool crss_per_voxel = false;
+  bool keep_d = false;
+  bool have_L0 = false;
+  LinePlan px{}, py{}, pz{};
+  // device storage (element type = double for FP64, float for MIXED)
+  void* R = nullptr;
+  void* sigma = nullptr;
+  void* lambda = nullptr;
+  void* work = nullptr;
+  void* dkeep = nullptr;
+  void* crss = nullptr;
+  double* acc = nullptr;
+  void* X = nullptr;
+  void* twx = nullptr;
+  void* twy = nullptr;
+  void* twz = nullptr;
+  double* partials = nullptr;
+  double* sum25 = nullptr;
+  IterCtrl* ctrl = nullptr;
+  IterCtrl* h_ctrl = nullptr;  // pinned
+  double* hist = nullptr;
+  int hist_cap = 0;
+  double L0[25] = {0};
+  double Linv[25] = {0};
+  double last_edot[5] = {0};
+  long long launches = 0;
+  std::string err;
+};
+
+namespace {
+
+thread_local std::string g_lib_err;
+
+size_t elem_size(vpfft_precision p) { return p == VPFFT_PREC_FP64 ? sizeof(double) : sizeof(float); }
+
+vpfft_status fail(vpfft_grid* g, vpfft_status s, const std::string& msg) {
+  if (g)
+    g->err = msg;
+  else
+    g_lib_err = msg;
+  return s;
+}
+
+#define CK(g, call)                                                                       \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess) {                                                              \
+      return fail((g), e_ == cudaErrorMemoryAllocation ? VPFFT_ERR_OUT_OF_MEMORY          \
+                                                       : VPFFT_ERR_CUDA,                  \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                    \
+    }                                                                                     \
+  } while (0)
+
+#define CKL(g) CK(g, cudaGetLastError())
+
+vpfft_status need_device(vpfft_grid* g) {
+  int cnt = 0;
+  cudaError_t e = cudaGetDeviceCount(&cnt);
+  if (e != cudaSuccess || cnt <= 0) {
+    cudaGetLastError();
+    return fail(g, VPFFT_ERR_NO_DEVICE,
+                "no CUDA device available (vpfft_b200 has no CPU fallback)");
+  }
+  return VPFFT_OK;
+}
+
+// twiddle table exp(-2 pi i e / n), e in [0, n), from long double
+template <typename R>
+std::vector<R> twiddles(int n) {
+  std::vector<R> t(2 * (size_t)n);
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  for (int e = 0; e < n; ++e) {
+    const long double a = two_pi * (long double)e / (long double)n;
+    t[2 * e] = (R)cosl(a);
+    t[2 * e + 1] = (R)(-sinl(a));
+  }
+  return t;
+}
+
+// LU with row pivoting inverse of a column-major 5x5 (host, FP64)
+void inverse5_host(const double* a, double* out) {
+  double lu[5][5];
+  int perm[5];
+  for (int i = 0; i < 5; ++i) {
+    perm[i] = i;
+    for (int j = 0; j < 5; ++j) lu[i][j] = a[j * 5 + i];
+  }
+  for (int k = 0; k < 5; ++k) {
+    int piv = k;
+    double best = std::fabs(lu[k][k]);
+    for (int i = k + 1; i < 5; ++i)
+      if (std::fabs(lu[i][k]) > best) {
+        best = std::fabs(lu[i][k]);
+        piv = i;
+      }
+    if (piv != k) {
+      for (int j = 0; j < 5; ++j) std::swap(lu[k][j], lu[piv][j]);
+      std::swap(perm[k], perm[piv]);
+    }
+    for (int i = k + 1; i < 5; ++i) {
+      lu[i][k] /= lu[k][k];
+      for (int j = k + 1; j < 5; ++j) lu[i][j] -= lu[i][k] * lu[k][j];
+    }
+  }
+  for (int col = 0; col < 5; ++col) {
+    double y[5];
+    for (int i = 0; i < 5; ++i) {
+      double s = (perm[i] == col) ? 1.0 : 0.0;
+      for (int j = 0; j < i; ++j) s -= lu[i][j] * y[j];
+      y[i] = s;
+    }
+    for (int i = 4; i >= 0; --i) {
+      double s = y[i];
+      for (int j = i + 1; j < 5; ++j) s -= lu[i][j] * y[j];
+      y[i] = s / lu[i][i];
+    }
+    for (int i = 0; i < 5; ++i) out[col * 5 + i] = y[i];
+  }
+}
+
+MaterialParams mat_params(const vpfft_material& m) {
+  MaterialParams p;
+  for (int k = 0; k < kNS; ++k) {
+    p.gdot[k] = m.gamma_dot_base[k];
+    p.nexp[k] = m.rate_sensitivity[k];
+  }
+  return p;
+}
+
+template <typename S>
+FieldPtrs<S> fields(vpfft_grid* g) {
+  FieldPtrs<S> f;
+  f.R = (S*)g->R;
+  f.sigma = (S*)g->sigma;
+  f.lambda = (S*)g->lambda;
+  f.work = (S*)g->work;
+  f.dkeep = g->keep_d ? (S*)g->dkeep : nullptr;
+  f.crss = g->crss_per_voxel ? (S*)g->crss : nullptr;
+  f.acc = g->acc;
+  return f;
+}
+
+VoxelParams voxel_params(vpfft_grid* g, const double edot[5]) {
+  VoxelParams p{};
+  p.n = g->n;
+  for (int c = 0; c < 5; ++c) p.edot[c] = edot[c];
+  for (int k = 0; k < 25; ++k) p.L0[k] = g->L0[k];
+  p.mat = mat_params(g->mat);
+  for (int k = 0; k < kNS; ++k) p.crss[k] = g->mat.crss[k];
+  p.nr_eps = g->opt.nr_epsilon;
+  p.nr_max_rss = g->opt.nr_max_resolved;
+  p.nr_max_iter = g->opt.nr_max_iter;
+  p.init_max_iter = g->opt.init_nr_max_iter;
+  p.init_eps = g->opt.init_nr_epsilon;
+  // MaterialGrid.cpp:162-166
+  int min_n = g->mat.rate_sensitivity[0];
+  for (int k = 1; k < kNS; ++k) min_n = std::min(min_n, (int)g->mat.rate_sensitivity[k]);
+  const double ee = edot[0] * edot[0] + edot[1] * edot[1] + edot[2] * edot[2] +
+                    edot[3] * edot[3] + edot[4] * edot[4];
+  double imposed = 2.0 * std::pow(ee / g->mat.gamma_dot_base[0], (double)(1. / (float)min_n));
+  p.imposed_max_rss = (2.0 < imposed) ? imposed : 2.0;
+  return p;
+}
+
+template <typename S>
+GreenParams<S> green_params(int nx, int ny, int nz, const double h[3], const double* L0,
+                            const double* Linv) {
+  GreenParams<S> gp{};
+  gp.nx = nx;
+  gp.ny = ny;
+  gp.nz = nz;
+  gp.inv_len[0] = (S)(1.0 / (nx * h[0]));
+  gp.inv_len[1] = (S)(1.0 / (ny * h[1]));
+  gp.inv_len[2] = (S)(1.0 / (nz * h[2]));
+  for (int k = 0; k < 25; ++k) {
+    gp.L0[k] = (S)L0[k];
+    gp.Linv[k] = (S)Linv[k];
+  }
+  return gp;
+}
+
+template <typename S>
+Spectral<S> spectral(vpfft_grid* g) {
+  Spectral<S> sp;
+  sp.nx = g->nx;
+  sp.ny = g->ny;
+  sp.nz = g->nz;
+  sp.nh = g->nh;
+  sp.px = g->px;
+  sp.py = g->py;
+  sp.pz = g->pz;
+  sp.twx = g->twx;
+  sp.twy = g->twy;
+  sp.twz = g->twz;
+  sp.X = g->X;
+  return sp;
+}
+
+template <typename S>
+vpfft_status upload_twiddles(vpfft_grid* g) {
+  const int dims[3] = {g->nx, g->ny, g->nz};
+  void** dst[3] = {&g->twx, &g->twy, &g->twz};
+  for (int a = 0; a < 3; ++a) {
+    std::vector<S> t = twiddles<S>(dims[a]);
+    CK(g, cudaMalloc(dst[a], t.size() * sizeof(S)));
+    CK(g, cudaMemcpy(*dst[a], t.data(), t.size() * sizeof(S), cudaMemcpyHostToDevice));
+  }
+  return VPFFT_OK;
+}
+
+void free_grid_buffers(vpfft_grid* g) {
+  void* ptrs[] = {g->R,   g->sigma, g->lambda, g->work,     g->dkeep, g->crss,
+                  g->acc, g->X,     g->twx,    g->twy,      g->twz,   g->partials,
+                  g->sum25, g->ctrl, g->hist};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (g->h_ctrl) cudaFreeHost(g->h_ctrl);
+  if (g->stream) cudaStreamDestroy(g->stream);
+}
+
+// Lines up to 512 points keep every FFT tile (5 components, FP64, ping-pong
+// buffers) inside one block's shared memory.
+bool valid_dim(int n) {
+  LinePlan p;
+  return n >= 1 && n <= 512 && make_line_plan(n, &p);
+}
+
+template <typename S>
+vpfft_status to_device_field(vpfft_grid* g, const double* host_or_dev, bool is_device, S* dst,
+                             int width) {
+  const size_t bytes = sizeof(double) * (size_t)g->n * width;
+  double* tmp = nullptr;
+  CK(g, cudaMalloc(&tmp, bytes));
+  cudaError_t e = is_device ? cudaMemcpyAsync(tmp, host_or_dev, bytes, cudaMemcpyDeviceToDevice, g->stream)
+                            : cudaMemcpyAsync(tmp, host_or_dev, bytes, cudaMemcpyHostToDevice, g->stream);
+  if (e != cudaSuccess) {
+    cudaFree(tmp);
+    return fail(g, VPFFT_ERR_CUDA, std::string("copy to device: ") + cudaGetErrorString(e));
+  }
+  g->launches += launch_to_soa<S>(tmp, dst, g->n, width, g->stream);
+  e = cudaGetLastError();
+  cudaError_t e2 = cudaStreamSynchronize(g->stream);
+  cudaFree(tmp);
+  if (e != cudaSuccess || e2 != cudaSuccess)
+    return fail(g, VPFFT_ERR_CUDA, std::string("to_soa: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+  return VPFFT_OK;
+}
+
+template <typename S>
+vpfft_status from_device_field(vpfft_grid* g, const S* src, int width, double* host) {
+  const size_t bytes = sizeof(double) * (size_t)g->n * width;
+  double* tmp = nullptr;
+  CK(g, cudaMalloc(&tmp, bytes));
+  g->launches += launch_from_soa<S>(src, tmp, g->n, width, g->stream);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(host, tmp, bytes, cudaMemcpyDeviceToHost, g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return fail(g, VPFFT_ERR_CUDA, std::string("from_soa: ") + cudaGetErrorString(e));
+  return VPFFT_OK;
+}
+
+template <typename S>
+vpfft_status ensure_crss_array(vpfft_grid* g) {
+  if (!g->crss) CK(g, cudaMalloc(&g->crss, sizeof(S) * (size_t)g->n * kNS));
+  return VPFFT_OK;
+}
+
+// ---------------------------------------------------------------- phases
+template <typename S>
+vpfft_status do_init(vpfft_grid* g, const double edot[5]) {
+  if (!g->fields_set) return fail(g, VPFFT_ERR_NOT_INITIALIZED, "fields not set");
+  VoxelParams p = voxel_params(g, edot);
+  IterCtrl h{};
+  h.n_voxels = (double)g->n;
+  CK(g, cudaMemcpyAsync(g->ctrl, &h, sizeof(h), cudaMemcpyHostToDevice, g->stream));
+  g->launches += launch_init<S>(p, fields<S>(g), g->ctrl, g->stream);
+  CKL(g);
+  CK(g, cudaMemcpyAsync(g->h_ctrl, g->ctrl, sizeof(IterCtrl), cudaMemcpyDeviceToHost, g->stream));
+  CK(g, cudaStreamSynchronize(g->stream));
+  if (g->h_ctrl->status & kStatusMaxRssTiny)
+    return fail(g, VPFFT_ERR_MAX_RSS_TINY,
+                "max resolved shear stress < 1e-10 in the initial guess (zero strain rate?)");
+  for (int c = 0; c < 5; ++c) g->last_edot[c] = edot[c];
+  return VPFFT_OK;
+}
+
+template <typename S>
+vpfft_status do_ref_medium(vpfft_grid* g, double* L0_out) {
+  VoxelParams p = voxel_params(g, g->last_edot);
+  g->launches += launch_ref_medium<S>(p, fields<S>(g), g->partials, g->sum25, g->stream);
+  CKL(g);
+  double sums[25];
+  CK(g, cudaMemcpyAsync(sums, g->sum25, sizeof(sums), cudaMemcpyDeviceToHost, g->stream));
+  CK(g, cudaStreamSynchronize(g->stream));
+  const double N = (double)g->n;
+  for (int k = 0; k < 25; ++k) {
+    double m = sums[k] / N;                        // mean of the per-voxel inverses (H4)
+    double tmp = m * (double)g->nx;                // * DimXLocal   (MaterialGrid.cpp:262)
+    m = tmp / (double)g->nx;                       // / DimX        (269)
+    g->L0[k] = std::fabs(m) < 1e-10 ? 0.0 : m;     // NormalizeValues (LinearAlgebra.h:605-613)
+  }
+  for (int k = 0; k < 25; ++k)
+    if (!std::isfinite(g->L0[k]))
+      return fail(g, VPFFT_ERR_NONFINITE, "reference medium is not finite (singular voxel compliance)");
+  double negL[25];
+  for (int k = 0; k < 25; ++k) negL[k] = -g->L0[k];
+  inverse5_host(negL, g->Linv);  // StrainRateEvolutionWithFFT, MaterialGrid.cpp:628-632
+  g->have_L0 = true;
+  if (L0_out) std::memcpy(L0_out, g->L0, sizeof(g->L0));
+  return VPFFT_OK;
+}
+
+template <typename S>
+vpfft_status do_fixed_point(vpfft_grid* g, const double edot[5], int max_iter, double eps,
+                            double* history, vpfft_stats* st) {
+  if (!g->have_L0) return fail(g, VPFFT_ERR_NOT_INITIALIZED, "reference medium not built");
+  if (std::max(max_iter, 1) > g->hist_cap) {
+    if (g->hist) cudaFree(g->hist);
+    g->hist = nullptr;
+    CK(g, cudaMalloc(&g->hist, sizeof(double) * 12 * (size_t)std::max(max_iter, 1)));
+    g->hist_cap = std::max(max_iter, 1);
+  }
+  // like the reference's do { } while (StepsTaken < NumMaxIterations && ...)
+  // (MaterialGrid.cpp:930-1068), at least one iteration always runs
+  IterCtrl h{};
+  h.iter = 0;
+  h.done = 0;
+  h.max_iter = max_iter;
+  h.eps = eps;
+  h.edot_norm = std::sqrt(edot[0] * edot[0] + edot[1] * edot[1] + edot[2] * edot[2] +
+                          edot[3] * edot[3] + edot[4] * edot[4]);
+  h.n_voxels = (double)g->n;
+  CK(g, cudaMemcpyAsync(g->ctrl, &h, sizeof(h), cudaMemcpyHostToDevice, g->stream));
+  VoxelParams p = voxel_params(g, edot);
+  GreenParams<S> gp = green_params<S>(g->nx, g->ny, g->nz, g->h, g->L0, g->Linv);
+  Spectral<S> sp = spectral<S>(g);
+  FieldPtrs<S> f = fields<S>(g);
+  const int batch = g->n >= (1LL << 21) ? 4 : 16;
+  for (;;) {
+    for (int b = 0; b < batch; ++b) {
+      g->launches += launch_spectral_iteration<S>(sp, gp, (S*)g->work, g->ctrl, g->stream, 5);
+      g->launches += launch_nr_update<S>(p, f, g->partials, g->ctrl, g->hist, g->stream);
+    }
+    CKL(g);
+    CK(g, cudaMemcpyAsync(g->h_ctrl, g->ctrl, sizeof(IterCtrl), cudaMemcpyDeviceToHost, g->stream));
+    CK(g, cudaStreamSynchronize(g->stream));
+    if (g->h_ctrl->done) break;
+  }
+  const IterCtrl& c = *g->h_ctrl;
+  if (history && c.iter > 0)
+    CK(g, cudaMemcpy(history, g->hist, sizeof(double) * 12 * (size_t)c.iter, cudaMemcpyDeviceToHost));
+  if (st) {
+    st->iterations = c.iter;
+    st->stress_error = c.last[10];
+    st->strain_rate_error = c.last[11];
+    st->converged = (c.last[10] <= eps && c.last[11] <= eps) ? 1 : 0;
+    for (int k = 0; k < 5; ++k) st->avg_strain_rate[k] = c.last[5 + k];
+    st->nr_not_converged = (int64_t)c.nr_capped;
+    st->status_bits = c.status;
+    std::memcpy(st->L0, g->L0, sizeof(g->L0));
+  }
+  if (c.status & kStatusNonFinite) return fail(g, VPFFT_ERR_NONFINITE, "non-finite stress or strain rate");
+  if (c.status & kStatusMaxRssTiny)
+    return fail(g, VPFFT_ERR_MAX_RSS_TINY, "max resolved shear stress < 1e-10 during the iteration");
+  return VPFFT_OK;
+}
+
+template <typename S>
+vpfft_status do_post(vpfft_grid* g, const double edot[5], double dt) {
+  vpfft_status s = ensure_crss_array<S>(g);
+  if (s != VPFFT_OK) return s;
+  PostParams p{};
+  p.n = g->n;
+  p.dt = dt;
+  p.mat = mat_params(g->mat);
+  for (int k = 0; k < kNS; ++k) {
+    p.crss[k] = g->mat.crss[k];
+    p.tau0[k] = g->mat.tau0[k];
+    p.tau1[k] = g->mat.tau1[k];
+    p.theta0[k] = g->mat.theta0[k];
+    p.theta1[k] = g->mat.theta1[k];
+  }
+  for (int k = 0; k < kNS * kNS; ++k) p.H[k] = g->mat.hardening[k];
+  g->launches += launch_post<S>(p, fields<S>(g), (S*)g->crss, g->stream);
+  CKL(g);
+  g->crss_per_voxel = true;
+  // UpdateVoxelLength (MaterialGrid.cpp:1190-1196) with Edot as a 3x3 matrix
+  double E[9];
+  vpfft_matrix_from_edot(edot, E);
+  g->h[0] *= (1.0 + E[0] * dt);
+  g->h[1] *= (1.0 + E[4] * dt);
+  g->h[2] *= (1.0 + E[8] * dt);
+  CK(g, cudaStreamSynchronize(g->stream));
+  return VPFFT_OK;
+}
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+template <typename S>
+vpfft_status do_step(vpfft_grid* g, const double edot[5], int max_iter, double dt, double eps,
+                     double avg[5], vpfft_stats* st) {
+  vpfft_stats local{};
+  vpfft_stats* s = st ? st : &local;
+  std::memset(s, 0, sizeof(*s));
+  const double t0 = now_s();
+  vpfft_status r = do_init<S>(g, edot);
+  if (r != VPFFT_OK) return r;
+  r = do_ref_medium<S>(g, nullptr);
+  if (r != VPFFT_OK) return r;
+  const double t1 = now_s();
+  r = do_fixed_point<S>(g, edot, max_iter, eps, nullptr, s);
+  if (r != VPFFT_OK) return r;
+  const double t2 = now_s();
+  if (avg)
+    for (int c = 0; c < 5; ++c) avg[c] = g->h_ctrl->last[c];
+  r = do_post<S>(g, edot, dt);
+  if (r != VPFFT_OK) return r;
+  const double t3 = now_s();
+  s->seconds_init = t1 - t0;
+  s->seconds_loop = t2 - t1;
+  s->seconds_post = t3 - t2;
+  return VPFFT_OK;
+}
+
+#define DISPATCH(g, fn, ...) \
+  ((g)->prec == VPFFT_PREC_FP64 ? fn<double>(__VA_ARGS__) : fn<float>(__VA_ARGS__))
+
+}  // namespace
+
+// ================================================================== C ABI
+extern "C" {
+
+const char* vpfft_version(void) { return "vpfft_b200 0.1 (sm_100a)"; }
+
+const char* vpfft_status_string(vpfft_status s) {
+  switch (s) {
+    case VPFFT_OK: return "ok";
+    case VPFFT_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case VPFFT_ERR_UNSUPPORTED_SIZE: return "unsupported grid size";
+    case VPFFT_ERR_CUDA: return "CUDA error";
+    case VPFFT_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case VPFFT_ERR_NO_DEVICE: return "no CUDA device";
+    case VPFFT_ERR_MAX_RSS_TINY: return "max resolved shear stress < 1e-10";
+    case VPFFT_ERR_NONFINITE: return "non-finite values";
+    case VPFFT_ERR_NOT_INITIALIZED: return "not initialized";
+    case VPFFT_ERR_IO: return "I/O or parse error";
+    case VPFFT_ERR_CANCELLED: return "cancelled";
+    case VPFFT_ERR_TIMEOUT: return "timeout";
+  }
+  return "unknown status";
+}
+
+int vpfft_device_count(void) {
+  int cnt = 0;
+  if (cudaGetDeviceCount(&cnt) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return cnt;
+}
+
+void vpfft_material_default(vpfft_material* m) {
+  if (!m) return;
+  for (int k = 0; k < kNS; ++k) {
+    m->gamma_dot_base[k] = 15.5;  // MaterialGrid.cpp:322
+    m->rate_sensitivity[k] = 10;  // 323
+    m->crss[k] = 11.0;            // 390
+    m->tau0[k] = 11.0;            // 329
+    m->tau1[k] = 11.0;            // 330
+    m->theta0[k] = 430.0;         // 331
+    m->theta1[k] = 110.0;         // 332
+  }
+  for (int k = 0; k < kNS * kNS; ++k) m->hardening[k] = 1.0;  // 334-336
+}
+
+void vpfft_solver_options_default(vpfft_solver_options* o) {
+  if (!o) return;
+  o->init_nr_epsilon = 5e-4;  // MaterialGrid.cpp:159
+  o->init_nr_max_iter = 1000; // 160
+  o->nr_epsilon = 5e-4;       // 909
+  o->nr_max_resolved = 1e9;   // 910
+  o->nr_max_iter = 100;       // 911
+  o->pad_ = 0;
+}
+
+vpfft_status vpfft_grid_create(int nx, int ny, int nz, const vpfft_material* material,
+                               const vpfft_solver_options* options, vpfft_precision precision,
+                               vpfft_grid** out) {
+  if (!out) return fail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "out is NULL");
+  *out = nullptr;
+  if (precision != VPFFT_PREC_FP64 && precision != VPFFT_PREC_MIXED)
+    return fail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "unknown precision");
+  if (!valid_dim(nx) || !valid_dim(ny) || !valid_dim(nz))
+    return fail(nullptr, VPFFT_ERR_UNSUPPORTED_SIZE,
+                "grid dimensions must be in [1, 512] and products of 2, 3 and 5");
+  if (material) {
+    for (int k = 0; k < kNS; ++k)
+      if (!(material->crss[k] > 0) || !(material->gamma_dot_base[k] > 0))
+        return fail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "CRSS and reference rates must be > 0");
+  }
+  vpfft_status s = need_device(nullptr);
+  if (s != VPFFT_OK) return s;
+  vpfft_grid* g = new vpfft_grid();
+  g->nx = nx;
+  g->ny = ny;
+  g->nz = nz;
+  g->nh = nz / 2 + 1;
+  g->n = (long long)nx * ny * nz;
+  g->prec = precision;
+  if (material)
+    g->mat = *material;
+  else
+    vpfft_material_default(&g->mat);
+  if (options)
+    g->opt = *options;
+  else
+    vpfft_solver_options_default(&g->opt);
+  make_line_plan(nx, &g->px);
+  make_line_plan(ny, &g->py);
+  make_line_plan(nz, &g->pz);
+  g->keep_d = g->n <= (1LL << 21);
+  cudaGetDevice(&g->device);
+  auto bail = [&](vpfft_status st) {
+    free_grid_buffers(g);
+    g_lib_err = g->err;
+    delete g;
+    return st;
+  };
+#define CKC(call)                                                                            \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess) {                                                                 \
+      g->err = std::string(#call) + ": " + cudaGetErrorString(e_);                           \
+      return bail(e_ == cudaErrorMemoryAllocation ? VPFFT_ERR_OUT_OF_MEMORY : VPFFT_ERR_CUDA); \
+    }                                                                                        \
+  } while (0)
+  CKC(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+  const size_t es = elem_size(precision);
+  const size_t n = (size_t)g->n;
+  CKC(cudaMalloc(&g->R, es * n * 9));
+  CKC(cudaMalloc(&g->sigma, es * n * 5));
+  CKC(cudaMalloc(&g->lambda, es * n * 5));
+  CKC(cudaMalloc(&g->work, es * n * 5));
+  if (g->keep_d) CKC(cudaMalloc(&g->dkeep, es * n * 5));
+  CKC(cudaMalloc(&g->acc, sizeof(double) * n));
+  CKC(cudaMalloc(&g->X, 2 * es * 5 * (size_t)nx * ny * g->nh));
+  const size_t nparts = (size_t)std::max(nr_blocks(g->n), ref_medium_blocks(g->n));
+  CKC(cudaMalloc(&g->partials, sizeof(double) * nparts * 25));
+  CKC(cudaMalloc(&g->sum25, sizeof(double) * 25));
+  CKC(cudaMalloc(&g->ctrl, sizeof(IterCtrl)));
+  CKC(cudaMallocHost(&g->h_ctrl, sizeof(IterCtrl)));
+  CKC(cudaMemset(g->acc, 0, sizeof(double) * n));
+#undef CKC
+  s = precision == VPFFT_PREC_FP64 ? upload_twiddles<double>(g) : upload_twiddles<float>(g);
+  if (s != VPFFT_OK) return bail(s);
+  *out = g;
+  return VPFFT_OK;
+}
+
+vpfft_status vpfft_grid_destroy(vpfft_grid* g) {
+  if (!g) return VPFFT_OK;
+  cudaSetDevice(g->device);
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  free_grid_buffers(g);
+  delete g;
+  return VPFFT_OK;
+}
+
+vpfft_status vpfft_grid_dims(const vpfft_grid* g, int* nx, int* ny, int* nz) {
+  if (!g) return VPFFT_ERR_INVALID_ARGUMENT;
+  if (nx) *nx = g->nx;
+  if (ny) *ny = g->ny;
+  if (nz) *nz = g->nz;
+  return VPFFT_OK;
+}
+
+static vpfft_status set_fields_impl(vpfft_grid* g, const double* R, const double* sigma,
+                                    bool device) {
+  if (!g) return VPFFT_ERR_INVALID_ARGUMENT;
+  if (!R) return fail(g, VPFFT_ERR_INVALID_ARGUMENT, "Orientation array not initialized");
+  cudaSetDevice(g->device);
+  vpfft_status s;
+  if (g->prec == VPFFT_PREC_FP64) {
+    s = to_device_field<double>(g, R, device, (double*)g->R, 9);
+    if (s == VPFFT_OK && sigma) s = to_device_field<double>(g, sigma, device, (double*)g->sigma, 5);
+    if (s == VPFFT_OK && !sigma) g->launches += launch_fill<double>((double*)g->sigma, g->n * 5, 0.0, g->stream);
+  } else {
+    s = to_device_field<float>(g, R, device, (float*)g->R, 9);
+    if (s == VPFFT_OK && sigma) s = to_device_field<float>(g, sigma, device, (float*)g->sigma, 5);
+    if (s == VPFFT_OK && !sigma) g->launches += launch_fill<float>((float*)g->sigma, g->n * 5, 0.0, g->stream);
+  }
+  if (s != VPFFT_OK) return s;
+  CK(g, cudaMemsetAsync(g->acc, 0, sizeof(double) * (size_t)g->n, g->stream));
+  g->crss_per_voxel = false;
+  g->have_L0 = false;
+  CK(g, cudaStreamSynchronize(g->stream));
+  g->fields_set = true;
+  return VPFFT_OK;
+}
+
+vpfft_status vpfft_grid_set_fields(vpfft_grid* g, const double* R, const double* sigma) {
+  return set_fields_impl(g, R, sigma, false);
+}
+vpfft_status vpfft_grid_set_fields_device(vpfft_grid* g, const double* R, const double* sigma) {
+  return set_fields_impl(g, R, sigma, true);
+}
+
+vpfft_status vpfft_grid_set_voxel_length(vpfft_grid* g, double hx, double hy, double hz) {
+  if (!g) return VPFFT_ERR_INVALID_ARGUMENT;
+  if (!(hx > 0) || !(hy > 0) || !(hz > 0))
+    return fail(g, VPFFT_ERR_INVALID_ARGUMENT, "voxel lengths must be > 0");
+  g->h[0] = hx;
+  g->h[1] = hy;
+  g->h[2] = hz;
+  return VPFFT_OK;
+}
+vpfft_status vpfft_grid_get_voxel_length(const vpfft_grid* g, double h[3]) {
+  if (!g || !h) return VPFFT_ERR_INVALID_ARGUMENT;
+  std::memcpy(h, g->h, sizeof(g->h));
+  return VPFFT_OK;
+}
+
+vpfft_status vpfft_grid_set_crss(vpfft_grid* g, const double* crss) {
+  if (!g) return VPFFT_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(g->device);
+  if (!crss) {
+    g->crss_per_voxel = false;
+    return VPFFT_OK;
+  }
+  vpfft_status s = g->prec == VPFFT_PREC_FP64 ? ensure_crss_array<double>(g) : ensure_crss_array<float>(g);
+  if (s != VPFFT_OK) return s;
+  s = g->prec == VPFFT_PREC_FP64 ? to_device_field<double>(g, crss, false, (double*)g->crss, kNS)
+                                 : to_device_field<float>(g, crss, false, (float*)g->crss, kNS);
+  if (s == VPFFT_OK) g->crss_per_voxel = true;
+  return s;
+}
+
+static int field_width(vpfft_field f) {
+  switch (f) {
+    case VPFFT_FIELD_STRESS:
+    case VPFFT_FIELD_LAGRANGE:
+    case VPFFT_FIELD_POLARIZATION:
+    case VPFFT_FIELD_STRAIN_RATE_VARIATION:
+    case VPFFT_FIELD_STRAIN_RATE: return 5;
+    case VPFFT_FIELD_ORIENTATION: return 9;
+    case VPFFT_FIELD_CRSS: return kNS;
+    case VPFFT_FIELD_ACCUMULATED_SHEAR: return 1;
+    case VPFFT_FIELD_SCHMID: return 60;
+  }
+  return -1;
+}
+
+}  // extern "C"
+template <typename S>
+static vpfft_status get_field_impl(vpfft_grid* g, vpfft_field which, double* dst) {
+  const long long n = g->n;
+  switch (which) {
+    case VPFFT_FIELD_STRESS: return from_device_field<S>(g, (S*)g->sigma, 5, dst);
+    case VPFFT_FIELD_LAGRANGE: return from_device_field<S>(g, (S*)g->lambda, 5, dst);
+    case VPFFT_FIELD_ORIENTATION: return from_device_field<S>(g, (S*)g->R, 9, dst);
+    case VPFFT_FIELD_POLARIZATION: return from_device_field<S>(g, (S*)g->work, 5, dst);
+    case VPFFT_FIELD_STRAIN_RATE_VARIATION:
+      if (!g->keep_d || !g->dkeep)
+        return fail(g, VPFFT_ERR_INVALID_ARGUMENT,
+                    "d~ is kept only when enabled (grids up to 128^3 by default)");
+      return from_device_field<S>(g, (S*)g->dkeep, 5, dst);
+    case VPFFT_FIELD_CRSS:
+      if (!g->crss_per_voxel) {
+        for (long long v = 0; v < n; ++v)
+          for (int k = 0; k < kNS; ++k) dst[v * kNS + k] = g->mat.crss[k];
+        return VPFFT_OK;
+      }
+      return from_device_field<S>(g, (S*)g->crss, kNS, dst);
+    case VPFFT_FIELD_ACCUMULATED_SHEAR:
+      CK(g, cudaMemcpy(dst, g->acc, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost));
+      return VPFFT_OK;
+    case VPFFT_FIELD_STRAIN_RATE: {
+      S* tmp = nullptr;
+      CK(g, cudaMalloc(&tmp, sizeof(S) * (size_t)n * 5));
+      VoxelParams p = voxel_params(g, g->last_edot);
+      g->launches += launch_strain_rate<S>(p, fields<S>(g), tmp, g->stream);
+      vpfft_status s = from_device_field<S>(g, tmp, 5, dst);
+      cudaFree(tmp);
+      return s;
+    }
+    case VPFFT_FIELD_SCHMID: {
+      double* tmp = nullptr;
+      CK(g, cudaMalloc(&tmp, sizeof(double) * (size_t)n * 60));
+      g->launches += launch_schmid_field<S>(n, (S*)g->R, tmp, g->stream);
+      cudaError_t e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaMemcpyAsync(dst, tmp, sizeof(double) * (size_t)n * 60, cudaMemcpyDeviceToHost, g->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+      cudaFree(tmp);
+      if (e != cudaSuccess) return fail(g, VPFFT_ERR_CUDA, cudaGetErrorString(e));
+      return VPFFT_OK;
+    }
+  }
+  return fail(g, VPFFT_ERR_INVALID_ARGUMENT, "unknown field");
+}
+
+extern "C" {
+
+vpfft_status vpfft_grid_get_field(vpfft_grid* g, vpfft_field which, double* dst) {
+  if (!g || !dst || field_width(which) < 0) return VPFFT_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(g->device);
+  return g->prec == VPFFT_PREC_FP64 ? get_field_impl<double>(g, which, dst)
+                                    : get_field_impl<float>(g, which, dst);
+}
+
+}  // extern "C"
+template <typename S>
+static vpfft_status set_field_impl(vpfft_grid* g, vpfft_field which, const double* src) {
+  switch (which) {
+    case VPFFT_FIELD_STRESS: return to_device_field<S>(g, src, false, (S*)g->sigma, 5);
+    case VPFFT_FIELD_LAGRANGE: return to_device_field<S>(g, src, false, (S*)g->lambda, 5);
+    case VPFFT_FIELD_ORIENTATION: return to_device_field<S>(g, src, false, (S*)g->R, 9);
+    case VPFFT_FIELD_POLARIZATION: return to_device_field<S>(g, src, false, (S*)g->work, 5);
+    case VPFFT_FIELD_CRSS: return vpfft_grid_set_crss(g, src);
+    case VPFFT_FIELD_ACCUMULATED_SHEAR:
+      CK(g, cudaMemcpy(g->acc, src, sizeof(double) * (size_t)g->n, cudaMemcpyHostToDevice));
+      return VPFFT_OK;
+    default: return fail(g, VPFFT_ERR_INVALID_ARGUMENT, "field is derived and cannot be set");
+  }
+}
+
+extern "C" {
+
+vpfft_status vpfft_grid_set_field(vpfft_grid* g, vpfft_field which, const double* src) {
+  if (!g || !src || field_width(which) < 0) return VPFFT_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(g->device);
+  vpfft_status s = g->prec == VPFFT_PREC_FP64 ? set_field_impl<double>(g, which, src)
+                                              : set_field_impl<float>(g, which, src);
+  if (s == VPFFT_OK && which == VPFFT_FIELD_ORIENTATION) g->fields_set = true;
+  return s;
+}
+
+vpfft_status vpfft_run_single_strain_step(vpfft_grid* g, const double edot[5], int max_iter,
+                                          double dt, double eps, double avg[5], vpfft_stats* st) {
+  if (!g || !edot) return VPFFT_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(g->device);
+  return DISPATCH(g, do_step, g, edot, max_iter, dt, eps, avg, st);
+}
+
+vpfft_status vpfft_run(vpfft_grid* g, const double edot[5], int max_iter, int n_steps, double dt,
+                       double eps, const char* path, vpfft_step_callback cb, void* user) {
+  if (!g || !edot || n_steps < 0) return VPFFT_ERR_INVALID_ARGUMENT;
+  FILE* os = nullptr;
+  if (path) {
+    os = std::fopen(path, "w");
+    if (!os) return fail(g, VPFFT_ERR_IO, std::string("cannot open ") + path);
+  }
+  double strain[5] = {0, 0, 0, 0, 0};
+  vpfft_status s = VPFFT_OK;
+  for (int i = 0; i < n_steps; ++i) {
+    double avg[5];
+    s = vpfft_run_single_strain_step(g, edot, max_iter, dt, eps, avg, nullptr);
+    if (s != VPFFT_OK) break;
+    for (int c = 0; c < 5; ++c) strain[c] += edot[c] * dt;  // MaterialGrid.cpp:1217
+    if (os) {
+      // one row per increment like MaterialGrid.cpp:1221-1225
+      double ne = 0, ns = 0;
+      for (int c = 0; c < 5; ++c) {
+        ne += strain[c] * strain[c];
+        ns += avg[c] * avg[c];
+      }
+      std::fprintf(os, "%d ", i);
+      for (int c = 0; c < 5; ++c) std::fprintf(os, "%g ", strain[c]);
+      std::fprintf(os, " ");
+      for (int c = 0; c < 5; ++c) std::fprintf(os, "%g ", avg[c]);
+      std::fprintf(os, " %g %g \n", std::sqrt(ne), std::sqrt(ns));
+    }
+    if (cb && cb(i, strain, avg, user)) break;
+  }
+  if (os) std::fclose(os);
+  return s;
+}
+
+vpfft_status vpfft_initialize_computation(vpfft_grid* g, const double edot[5]) {
+  if (!g || !edot) return VPFFT_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(g->device);
+  return DISPATCH(g, do_init, g, edot);
+}
+vpfft_status vpfft_build_reference_medium(vpfft_grid* g, double L0_out[25]) {
+  if (!g) return VPFFT_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(g->device);
+  return DISPATCH(g, do_ref_medium, g, L0_out);
+}
+vpfft_status vpfft_fixed_point(vpfft_grid* g, const double edot[5], int max_iter, double eps,
+                               double* history, vpfft_stats* st) {
+  if (!g || !edot) return VPFFT_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(g->device);
+  return DISPATCH(g, do_fixed_point, g, edot, max_iter, eps, history, st);
+}
+vpfft_status vpfft_post_increment(vpfft_grid* g, const double edot[5], double dt) {
+  if (!g || !edot) return VPFFT_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(g->device);
+  return DISPATCH(g, do_post, g, edot, dt);
+}
+vpfft_status vpfft_grid_synchronize(vpfft_grid* g) {
+  if (!g) return VPFFT_ERR_INVALID_ARGUMENT;
+  CK(g, cudaStreamSynchronize(g->stream));
+  return VPFFT_OK;
+}
+void* vpfft_grid_stream(vpfft_grid* g) { return g ? (void*)g->stream : nullptr; }
+int64_t vpfft_grid_launch_count(const vpfft_grid* g) { return g ? g->launches : 0; }
+const char* vpfft_last_error(const vpfft_grid* g) { return g ? g->err.c_str() : g_lib_err.c_str(); }
+
+// ------------------------------------------------------------------ Solvers batch
+namespace {
+struct DevBuf {
+  void* p = nullptr;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+vpfft_status upload(DevBuf& b, const void* src, size_t bytes) {
+  if (cudaMalloc(&b.p, bytes ? bytes : 8) != cudaSuccess)
+    return fail(nullptr, VPFFT_ERR_OUT_OF_MEMORY, "cudaMalloc failed");
+  if (src && bytes && cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(nullptr, VPFFT_ERR_CUDA, "cudaMemcpy failed");
+  return VPFFT_OK;
+}
+vpfft_status finish_batch(void* dst, const DevBuf& b, size_t bytes) {
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess && dst) e = cudaMemcpy(dst, b.p, bytes, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail(nullptr, VPFFT_ERR_CUDA, cudaGetErrorString(e));
+  return VPFFT_OK;
+}
+#define UP(buf, ptr, bytes)                        \
+  do {                                             \
+    vpfft_status s_ = upload(buf, ptr, bytes);     \
+    if (s_ != VPFFT_OK) return s_;                 \
+  } while (0)
+}  // namespace
+
+vpfft_status vpfft_solve_constrained_constitutive(int n, const double* s0, const double* schmid,
+                                                  const double* crss, const vpfft_material* m,
+                                                  const double edot[5], const double* lambda,
+                                                  const double* dtilde, const double L0[25],
+                                                  double eps, double max_rss, int max_iter,
+                                                  double* out, double* nr_error) {
+  if (n < 0 || !s0 || !schmid || !crss || !m || !edot || !lambda || !dtilde || !L0 || !out)
+    return fail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (vpfft_status s = need_device(nullptr)) return s;
+  if (n == 0) return VPFFT_OK;
+  DevBuf a, b, c, d, e, o, r;
+  UP(a, s0, sizeof(double) * 5 * n);
+  UP(b, schmid, sizeof(double) * 60 * n);
+  UP(c, crss, sizeof(double) * 12 * n);
+  UP(d, lambda, sizeof(double) * 5 * n);
+  UP(e, dtilde, sizeof(double) * 5 * n);
+  UP(o, nullptr, sizeof(double) * 5 * n);
+  UP(r, nullptr, sizeof(double) * n);
+  launch_solvers_constrained(n, (double*)a.p, (double*)b.p, (double*)c.p, mat_params(*m), edot,
+                             (double*)d.p, (double*)e.p, L0, eps, max_rss, max_iter, (double*)o.p,
+                             (double*)r.p, nullptr);
+  vpfft_status s = finish_batch(out, o, sizeof(double) * 5 * n);
+  if (s == VPFFT_OK && nr_error) s = finish_batch(nr_error, r, sizeof(double) * n);
+  return s;
+}
+
+vpfft_status vpfft_solve_constitutive(int n, const double* s0, const double* schmid,
+                                      const double* crss, const vpfft_material* m,
+                                      const double edot[5], double eps, double max_rss,
+                                      int max_iter, double* out) {
+  if (n < 0 || !s0 || !schmid || !crss || !m || !edot || !out)
+    return fail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (vpfft_status s = need_device(nullptr)) return s;
+  if (n == 0) return VPFFT_OK;
+  DevBuf a, b, c, o;
+  UP(a, s0, sizeof(double) * 5 * n);
+  UP(b, schmid, sizeof(double) * 60 * n);
+  UP(c, crss, sizeof(double) * 12 * n);
+  UP(o, nullptr, sizeof(double) * 5 * n);
+  launch_solvers_unconstrained(n, (double*)a.p, (double*)b.p, (double*)c.p, mat_params(*m), edot,
+                               eps, max_rss, max_iter, (double*)o.p, nullptr);
+  return finish_batch(out, o, sizeof(double) * 5 * n);
+}
+
+vpfft_status vpfft_apply_constitutive(int n, const double* s, const double* schmid,
+                                      const double* crss, const vpfft_material* m, double* out) {
+  if (n < 0 || !s || !schmid || !crss || !m || !out)
+    return fail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (vpfft_status st = need_device(nullptr)) return st;
+  if (n == 0) return VPFFT_OK;
+  DevBuf a, b, c, o;
+  UP(a, s, sizeof(double) * 5 * n);
+  UP(b, schmid, sizeof(double) * 60 * n);
+  UP(c, crss, sizeof(double) * 12 * n);
+  UP(o, nullptr, sizeof(double) * 5 * n);
+  launch_solvers_apply(n, (double*)a.p, (double*)b.p, (double*)c.p, mat_params(*m), (double*)o.p, nullptr);
+  return finish_batch(out, o, sizeof(double) * 5 * n);
+}
+
+vpfft_status vpfft_solve_sachs(int n, const double* schmid, const double* crss,
+                               const double edot[5], double* out) {
+  if (n < 0 || !schmid || !crss || !edot || !out)
+    return fail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (vpfft_status s = need_device(nullptr)) return s;
+  if (n == 0) return VPFFT_OK;
+  DevBuf b, c, o;
+  UP(b, schmid, sizeof(double) * 60 * n);
+  UP(c, crss, sizeof(double) * 12 * n);
+  UP(o, nullptr, sizeof(double) * 5 * n);
+  launch_solvers_sachs(n, (double*)b.p, (double*)c.p, edot, (double*)o.p, nullptr);
+  return finish_batch(out, o, sizeof(double) * 5 * n);
+}
+
+vpfft_status vpfft_schmid_tensors(int n, const double* R, double* out) {
+  if (n < 0 || !R || !out) return fail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (vpfft_status s = need_device(nullptr)) return s;
+  if (n == 0) return VPFFT_OK;
+  DevBuf a, o;
+  UP(a, R, sizeof(double) * 9 * n);
+  UP(o, nullptr, sizeof(double) * 60 * n);
+  launch_solvers_schmid(n, (double*)a.p, (double*)o.p, nullptr);
+  return finish_batch(out, o, sizeof(double) * 60 * n);
+}
+
+vpfft_status vpfft_green_apply(int n, const int32_t* kidx, int nx, int ny, int nz,
+                               const double h[3], const double L0[25], const double* phat,
+                               double* dhat, vpfft_precision prec) {
+  if (n < 0 || !kidx || !h || !L0 || !phat || !dhat || nx < 1 || ny < 1 || nz < 1)
+    return fail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "bad argument");
+  if (vpfft_status s = need_device(nullptr)) return s;
+  if (n == 0) return VPFFT_OK;
+  double negL[25], Linv[25];
+  for (int k = 0; k < 25; ++k) negL[k] = -L0[k];
+  inverse5_host(negL, Linv);
+  DevBuf k, p, o;
+  UP(k, kidx, sizeof(int32_t) * 3 * n);
+  UP(p, phat, sizeof(double) * 10 * n);
+  UP(o, nullptr, sizeof(double) * 10 * n);
+  if (prec == VPFFT_PREC_FP64)
+    launch_green_batch<double>(n, (int32_t*)k.p, green_params<double>(nx, ny, nz, h, L0, Linv),
+                               (double*)p.p, (double*)o.p, nullptr);
+  else
+    launch_green_batch<float>(n, (int32_t*)k.p, green_params<float>(nx, ny, nz, h, L0, Linv),
+                              (double*)p.p, (double*)o.p, nullptr);
+  return finish_batch(dhat, o, sizeof(double) * 10 * n);
+}
+
+// ------------------------------------------------------------------ FFT (testing)
+}  // extern "C"
+template <typename S>
+static vpfft_status fft_impl(int nx, int ny, int nz, int ncomp, const double* in, double* out,
+                             int mode) {
+  vpfft_grid tmp;  // only used for the twiddle upload / error string
+  tmp.nx = nx;
+  tmp.ny = ny;
+  tmp.nz = nz;
+  tmp.nh = nz / 2 + 1;
+  make_line_plan(nx, &tmp.px);
+  make_line_plan(ny, &tmp.py);
+  make_line_plan(nz, &tmp.pz);
+  const long long n = (long long)nx * ny * nz;
+  const size_t nspec = (size_t)ncomp * nx * ny * tmp.nh;
+  vpfft_status s = upload_twiddles<S>(&tmp);
+  DevBuf X, real, io;
+  if (s == VPFFT_OK) s = upload(X, nullptr, 2 * sizeof(S) * nspec);
+  if (s == VPFFT_OK) s = upload(real, nullptr, sizeof(S) * n * ncomp);
+  const size_t in_count = mode == 0 ? (size_t)n * ncomp : 2 * nspec;
+  const size_t out_count = mode == 0 ? 2 * nspec : (size_t)n * ncomp;
+  if (s == VPFFT_OK) s = upload(io, nullptr, sizeof(double) * std::max(in_count, out_count));
+  if (s == VPFFT_OK) {
+    cudaMemcpy(io.p, in, sizeof(double) * in_count, cudaMemcpyHostToDevice);
+    Spectral<S> sp = spectral<S>(&tmp);
+    sp.X = X.p;
+    if (mode == 0) {
+      launch_to_soa<S>((double*)io.p, (S*)real.p, (long long)in_count, 1, nullptr);
+      launch_fft3d<S>(sp, (S*)real.p, ncomp, 0, nullptr);
+      launch_from_soa<S>((S*)X.p, (double*)io.p, (long long)out_count, 1, nullptr);
+    } else {
+      launch_to_soa<S>((double*)io.p, (S*)X.p, (long long)in_count, 1, nullptr);
+      launch_fft3d<S>(sp, (S*)real.p, ncomp, 1, nullptr);
+      launch_from_soa<S>((S*)real.p, (double*)io.p, (long long)out_count, 1, nullptr);
+    }
+    s = finish_batch(out, io, sizeof(double) * out_count);
+  }
+  if (tmp.twx) cudaFree(tmp.twx);
+  if (tmp.twy) cudaFree(tmp.twy);
+  if (tmp.twz) cudaFree(tmp.twz);
+  tmp.twx = tmp.twy = tmp.twz = nullptr;
+  return s;
+}
+
+extern "C" {
+
+vpfft_status vpfft_fft3d_r2c(int nx, int ny, int nz, int ncomp, const double* real, double* spec,
+                             vpfft_precision prec) {
+  if (!valid_dim(nx) || !valid_dim(ny) || !valid_dim(nz) || ncomp < 1 || ncomp > 5 || !real || !spec)
+    return fail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "bad argument");
+  if (vpfft_status s = need_device(nullptr)) return s;
+  return prec == VPFFT_PREC_FP64 ? fft_impl<double>(nx, ny, nz, ncomp, real, spec, 0)
+                                 : fft_impl<float>(nx, ny, nz, ncomp, real, spec, 0);
+}
+vpfft_status vpfft_fft3d_c2r(int nx, int ny, int nz, int ncomp, const double* spec, double* real,
+                             vpfft_precision prec) {
+  if (!valid_dim(nx) || !valid_dim(ny) || !valid_dim(nz) || ncomp < 1 || ncomp > 5 || !real || !spec)
+    return fail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "bad argument");
+  if (vpfft_status s = need_device(nullptr)) return s;
+  return prec == VPFFT_PREC_FP64 ? fft_impl<double>(nx, ny, nz, ncomp, spec, real, 1)
+                                 : fft_impl<float>(nx, ny, nz, ncomp, spec, real, 1);
+}
+
+}  // extern "C"

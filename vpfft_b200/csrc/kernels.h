@@ -1,0 +1,139 @@
+// kernels.h -- host-side launch interface of the sm_100a kernels (kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device_math.cuh"
+
+namespace vpfft {
+
+// Per-launch constants of the per-voxel phases (kernel parameter, constant bank).
+struct VoxelParams {
+  long long n;           // voxels
+  double edot[5];        // imposed macroscopic strain rate
+  double L0[25];         // reference medium, column-major
+  MaterialParams mat;
+  double crss[kNS];      // CRSS used when the per-voxel array is absent
+  double nr_eps;         // 5e-4   (MaterialGrid.cpp:909)
+  double nr_max_rss;     // 1e9    (MaterialGrid.cpp:910)
+  int32_t nr_max_iter;   // 100    (MaterialGrid.cpp:911)
+  int32_t init_max_iter; // 1000   (MaterialGrid.cpp:160)
+  double init_eps;       // 5e-4   (MaterialGrid.cpp:159)
+  double imposed_max_rss;  // max(2, 2 (edot.edot/gdot0)^(1/n_min))  (MaterialGrid.cpp:162-166)
+};
+
+// Hardening / texture constants (UpdateHardeningCRSS, MaterialGrid.cpp:1127-1157).
+struct PostParams {
+  long long n;
+  double dt;
+  MaterialParams mat;
+  double crss[kNS];
+  double tau0[kNS], tau1[kNS], theta0[kNS], theta1[kNS];
+  double H[kNS * kNS];
+};
+
+// Device-resident control block of the fixed-point loop.  Every kernel of an
+// iteration returns immediately once `done` is set, so the host may enqueue
+// iterations ahead of the convergence decision.
+struct IterCtrl {
+  int32_t iter;       // iterations executed (StepsTaken, MaterialGrid.cpp:919)
+  int32_t done;
+  int32_t max_iter;
+  int32_t status;     // OR of kStatus* bits
+  double eps;
+  double edot_norm;   // sqrt(edot.edot)
+  double inv_n;       // 1/N  (unused; kept for alignment)
+  double n_voxels;    // N as double
+  unsigned long long nr_capped;
+  double last[12];    // <sigma>(5), <edot>(5), delta_sigma, delta_eps of the last iteration
+};
+enum : int32_t { kStatusMaxRssTiny = 1, kStatusNonFinite = 2 };
+
+struct LinePlan {
+  int n;
+  int nrad;
+  int rad[16];
+};
+bool make_line_plan(int n, LinePlan* p);
+
+template <typename S>
+struct FieldPtrs {
+  S* R;        // 9 x N
+  S* sigma;    // 5 x N
+  S* lambda;   // 5 x N
+  S* work;     // 5 x N: P before the forward FFT, d~ after the inverse FFT
+  S* dkeep;    // 5 x N copy of d~ (optional, may be null)
+  S* crss;     // 12 x N or null
+  double* acc; // N
+};
+
+// --- voxel phases (kernels.cu); each returns the number of kernels launched
+template <typename S>
+int launch_init(const VoxelParams& p, const FieldPtrs<S>& f, IterCtrl* ctrl, cudaStream_t st);
+template <typename S>
+int launch_ref_medium(const VoxelParams& p, const FieldPtrs<S>& f, double* partials,
+                      double* out25, cudaStream_t st);
+template <typename S>
+int launch_nr_update(const VoxelParams& p, const FieldPtrs<S>& f, double* partials,
+                     IterCtrl* ctrl, double* hist, cudaStream_t st);
+template <typename S>
+int launch_post(const PostParams& p, const FieldPtrs<S>& f, S* crss_out, cudaStream_t st);
+template <typename S>
+int launch_strain_rate(const VoxelParams& p, const FieldPtrs<S>& f, S* out5, cudaStream_t st);
+template <typename S>
+int launch_schmid_field(long long n, const S* R, double* out60_voxel_major, cudaStream_t st);
+int nr_blocks(long long n);
+int ref_medium_blocks(long long n);
+
+// --- layout conversion: host arrays are voxel-major double, device fields are
+// component-major S
+template <typename S>
+int launch_to_soa(const double* src_vmajor, S* dst, long long n, int width, cudaStream_t st);
+template <typename S>
+int launch_from_soa(const S* src, double* dst_vmajor, long long n, int width, cudaStream_t st);
+template <typename S>
+int launch_fill(S* dst, long long count, double value, cudaStream_t st);
+template <typename S>
+int launch_crss_broadcast(S* dst, long long n, const double crss[kNS], cudaStream_t st);
+
+// --- spectral phase (kernels.cu) ------------------------------------------
+template <typename R>
+struct Spectral {
+  int nx, ny, nz, nh;
+  LinePlan px, py, pz;
+  const void* twx;  // twiddle tables exp(-2 pi i e / n), complex R
+  const void* twy;
+  const void* twz;
+  void* X;          // 5 x nx x ny x nh complex R
+};
+// forward: work (P) -> X ; inverse: X -> work (d~, scaled by 1/N)
+template <typename S>
+int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S* work,
+                              const IterCtrl* ctrl, cudaStream_t st, int ncomp);
+// forward-only / inverse-only transforms for testing (mode 0 = forward, 1 = inverse)
+template <typename S>
+int launch_fft3d(const Spectral<S>& sp, S* real, int ncomp, int mode, cudaStream_t st);
+template <typename R>
+size_t spectral_smem_optin(int device);
+
+// --- batched solver entry points for testing (double, voxel-major) ---------
+int launch_solvers_constrained(int n, const double* s0, const double* schmid, const double* crss,
+                               const MaterialParams& mp, const double edot[5],
+                               const double* lambda, const double* dtilde, const double L0[25],
+                               double eps, double max_rss, int max_iter, double* out,
+                               double* nr_err, cudaStream_t st);
+int launch_solvers_unconstrained(int n, const double* s0, const double* schmid,
+                                 const double* crss, const MaterialParams& mp,
+                                 const double edot[5], double eps, double max_rss, int max_iter,
+                                 double* out, cudaStream_t st);
+int launch_solvers_apply(int n, const double* s, const double* schmid, const double* crss,
+                         const MaterialParams& mp, double* out, cudaStream_t st);
+int launch_solvers_sachs(int n, const double* schmid, const double* crss, const double edot[5],
+                         double* out, cudaStream_t st);
+int launch_solvers_schmid(int n, const double* R, double* out, cudaStream_t st);
+template <typename R>
+int launch_green_batch(int n, const int32_t* kidx, const GreenParams<R>& gp, const double* phat,
+                       double* dhat, cudaStream_t st);
+
+}  // namespace vpfft
