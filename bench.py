@@ -1,0 +1,504 @@
+"""Benchmark of the VPFFT fixed-point solve on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the headline configuration): a 256^3 periodic Voronoi polycrystal
+with 1000 grains and uniform random orientations, FCC 12 {111}<110> systems,
+power law n = 20, gdot0 = 1, uniform CRSS 1, plane-strain compression
+velocity gradient diag(1, 0, -1); mixed precision (FP32 fields, FFTs and
+Green operator; FP64 Newton-Raphson and compensated FP64 reductions).
+Synthetic data from the seeded fixture generator.
+
+A step is one fixed-point iteration over the whole grid (MaterialGrid.cpp:
+930-1068): forward R2C FFT of the polarization, Green operator, inverse FFT,
+per-voxel NR solve, constitutive update, reductions and convergence test.
+The metric is voxel-iterations per second (voxels x iterations / time).
+
+  value  -- K iterations timed with CUDA events on the grid's stream, state
+            resident in HBM (inputs ~2.3 GB, far larger than the 126 MB L2);
+  e2e    -- the same metric through the C ABI call a user makes,
+            vpfft_run_single_strain_step, one full increment per step
+            (initialisation, reference medium, up to 100 iterations to
+            eps = 1e-5, texture and hardening update), with the orientation and
+            stress arrays copied from pinned host memory and the stress field
+            copied back inside the timed region;
+  fp64   -- the all-FP64 GPU path on the same workload;
+  cpu_baseline -- the reference's own code (oracle/_ref, else the C
+            restatement) on a bounded sample of the same workload on the host.
+
+Multi-GPU: one process per GPU (torchrun); every rank solves its own replica
+RVE (weak scaling, no collective in the data path); the elapsed time is the
+maximum over ranks.  --impl reference times the reference's CPU solve with
+every host core running its own sample (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+# One visible GPU per rank, set before any CUDA runtime initialises.
+if "LOCAL_RANK" in os.environ and int(os.environ.get("WORLD_SIZE", "1")) > 1:
+    os.environ["CUDA_VISIBLE_DEVICES"] = os.environ["LOCAL_RANK"]
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "voxel-iters/s at 256^3 mixed precision (FP64 path reported beside)"
+UNIT = "voxel-iter/s"
+
+N_GRID = 256
+N_GRAINS = 1000
+SEED = 2024
+RATE_SENS = 20
+VEL_GRAD = np.diag([1.0, 0.0, -1.0])
+
+WORKLOAD = ("256^3 periodic Voronoi polycrystal, 1000 grains, uniform SO(3) orientations, "
+            "FCC 12 {111}<110>, n=20, gdot0=1, CRSS=1, plane-strain diag(1,0,-1), one "
+            "fixed-point iteration per step")
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self, gpu_index: int = 0):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9 or f[0] != str(gpu_index):
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ inputs
+def make_inputs(n=N_GRID, grains=N_GRAINS, seed=SEED):
+    from vpfft_b200 import fixtures
+
+    R = fixtures.polycrystal(n, n, n, grains, seed)
+    edot = fixtures.edot_from_matrix(VEL_GRAD)
+    return R, edot
+
+
+def material():
+    import vpfft_b200 as vp
+
+    return vp.material(gamma_dot_base=1.0, rate_sensitivity=RATE_SENS, crss=1.0, tau0=1.0,
+                       tau1=0.5, theta0=20.0, theta1=1.0)
+
+
+def alg_bytes_per_voxel(s: int, nz: int, keep_d: bool = False) -> dict:
+    """Compulsory HBM bytes per voxel of each kernel of one iteration, for
+    field storage size s (4 mixed, 8 FP64): complex values are 2s, the half
+    spectrum has nz/2+1 of nz points along z, 5 components everywhere."""
+    h = (nz // 2 + 1) / nz
+    spec = 5 * 2 * s * h
+    return {
+        "fft_z_r2c": 5 * s + spec,
+        "fft_y_forward": 2 * spec,
+        "fft_x_green": 2 * spec,
+        "fft_y_inverse": 2 * spec,
+        "fft_z_c2r": spec + 5 * s,
+        # R (9), sigma, lambda, d~ (5 each) read; sigma, lambda, P written
+        "nr_update": (9 + 5 + 5 + 5) * s + 15 * s + (5 * s if keep_d else 0),
+        "iter_finish": 0.0,
+    }
+
+
+# ------------------------------------------------------------------ our arm
+def device_arm(args, R, edot, precision):
+    import torch
+
+    import vpfft_b200 as vp
+
+    n = args.grid
+    N = n ** 3
+    grid = vp.MaterialGrid(n, n, n, material=material(), precision=precision)
+    grid.SendDataAndInitialize(R, None)
+    grid.InitializeComputation(edot)
+    grid.BuildLinearRefMediumStiffness()
+    stream = torch.cuda.ExternalStream(grid.stream())
+    # warm-up iterations (eps = 0: the loop runs exactly the requested count)
+    grid.FixedPoint(edot, args.warmup, 0.0)
+    grid.set_profiling(True)
+    launches0 = grid.launch_count()
+    barrier()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with ClockSampler() as clk:
+        start.record(stream)
+        hist = grid.FixedPoint(edot, args.steps, 0.0)
+        end.record(stream)
+        end.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    ms = start.elapsed_time(end)
+    launches = grid.launch_count() - launches0
+    phases = grid.phase_times()
+    avg = hist[-1, :5].copy()
+    st = grid.last_stats
+    res = dict(ms=ms, N=N, phases=phases, launches=launches, clocks=clk.summary(0), avg=avg,
+               iters=int(st.iterations), grid=grid)
+    return res
+
+
+def e2e_arm(args, R, edot):
+    """Full increments through vpfft_run_single_strain_step with pinned host I/O."""
+    import torch
+
+    import vpfft_b200 as vp
+    from vpfft_b200 import capi
+
+    n = args.grid
+    N = n ** 3
+    Rp = torch.empty((N, 9), dtype=torch.float64, pin_memory=True)
+    Rp.numpy()[:] = R
+    Sp = torch.zeros((N, 5), dtype=torch.float64, pin_memory=True)
+    Op = torch.empty((N, 5), dtype=torch.float64, pin_memory=True)
+    lib = capi.load()
+    grid = vp.MaterialGrid(n, n, n, material=material(), precision=args.precision)
+    import ctypes as C
+
+    e = np.ascontiguousarray(edot)
+    avg = np.zeros(5)
+    st = capi.Stats()
+    P = C.POINTER(C.c_double)
+
+    def one():
+        capi.check(lib.vpfft_grid_set_fields(grid._h, C.cast(Rp.data_ptr(), P),
+                                             C.cast(Sp.data_ptr(), P)), grid._h)
+        capi.check(lib.vpfft_run_single_strain_step(grid._h, e.ctypes.data_as(P), 100, 0.005,
+                                                    1e-5, avg.ctypes.data_as(P), C.byref(st)),
+                   grid._h)
+        capi.check(lib.vpfft_grid_get_field(grid._h, capi.FIELD_STRESS, C.cast(Op.data_ptr(), P)),
+                   grid._h)
+        return int(st.iterations)
+
+    one()  # warm-up increment
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    iters = 0
+    for _ in range(args.e2e_steps):
+        iters += one()
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    dt = max_over_ranks(dt)
+    grid.close()
+    return dict(seconds=dt, iters=iters, N=N, h2d=N * 14 * 8, d2h=N * 5 * 8 + 40)
+
+
+# ------------------------------------------------------------------ CPU side
+def ref_binary():
+    from oracle import refio
+
+    if os.path.exists(refio.REF_BIN):
+        return refio.REF_BIN, "reference"
+    from oracle import portlib
+
+    portlib.build()
+    return refio.PORT_BIN, "port"
+
+
+def cpu_samples(n_side, procs, warm, timed):
+    """Run `procs` concurrent single-threaded oracle processes, each solving its
+    own n_side^3 sample of the workload (same grain size and material) for
+    warm + timed fixed-point iterations with eps = 0; returns the summed
+    voxel-iters/s over the timed iterations (from the oracle's per-iteration
+    timestamps) and per-process rates."""
+    from oracle import refio
+    from vpfft_b200 import fixtures
+
+    binary, kind = ref_binary()
+    grains = max(1, round(N_GRAINS * (n_side / N_GRID) ** 3))
+    edot = fixtures.edot_from_matrix(VEL_GRAD)
+    m = refio.Material.uniform(1.0, RATE_SENS, 1.0, 0.5, 20.0, 1.0)
+    tmp = tempfile.mkdtemp(prefix="vpfft_cpu_")
+    runs = []
+    for p in range(procs):
+        R = fixtures.polycrystal(n_side, n_side, n_side, grains, SEED + p)
+        case = refio.Case((n_side,) * 3, R, np.zeros((n_side ** 3, 5)), np.ones(12), m, edot,
+                          nsteps=1, max_iter=warm + timed, dt=0.005, eps=0.0)
+        d = os.path.join(tmp, str(p))
+        os.makedirs(d)
+        refio.write_input(os.path.join(d, "input.bin"), case)
+        runs.append(d)
+    procs_ = [subprocess.Popen([binary, os.path.join(d, "input.bin"), d, "--quiet"],
+                               stdout=subprocess.DEVNULL, stderr=subprocess.PIPE) for d in runs]
+    rates = []
+    for pr, d in zip(procs_, runs):
+        _, err = pr.communicate()
+        if pr.returncode != 0:
+            raise RuntimeError(f"oracle failed: {err.decode()[-500:]}")
+        ft = np.fromfile(os.path.join(d, "fwd_times.bin"))
+        # ft[k] is taken at the start of iteration k+1's forward FFT; the last
+        # one starts the post-loop orientation update
+        span = ft[warm + timed] - ft[warm]
+        rates.append(n_side ** 3 * timed / span)
+    return float(sum(rates)), rates, kind, binary
+
+
+def cpu_baseline_ours():
+    n_side, warm, timed = 48, 1, 6
+    total, rates, kind, _ = cpu_samples(n_side, 1, warm, timed)
+    return {"value": total, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": (f"{n_side}^3 sample of the workload (same grain size and material), "
+                       f"{timed} timed fixed-point iterations after {warm} warm-up, one "
+                       "single-threaded process")}
+
+
+# ------------------------------------------------------------------ distributed helpers
+_dist = None
+
+
+def setup_dist(n_gpus):
+    global _dist
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        _dist = dist
+    return int(os.environ.get("RANK", "0")), ws
+
+
+def barrier():
+    if _dist is not None:
+        import torch
+
+        _dist.barrier(device_ids=[torch.cuda.current_device()])
+
+
+def max_over_ranks(x: float) -> float:
+    if _dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    _dist.all_reduce(t, op=_dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------ main
+def run_reference_arm(args, rank, ws):
+    if rank != 0:
+        return 0
+    procs = os.cpu_count() or 1
+    # per-process sample sized so that warm-up + steps iterations stay ~1 minute
+    n_side = 32 if args.steps + args.warmup > 20 else 48
+    total, rates, kind, binary = cpu_samples(n_side, procs, args.warmup, args.steps)
+    per_iter_ms = 1e3 * (n_side ** 3) / (total / procs)
+    line = {
+        "metric": METRIC, "value": total, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": per_iter_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": WORKLOAD, "grid": [n_side] * 3, "grains_scaled": True,
+                   "step": "one fixed-point iteration of each process's sample",
+                   "processes": procs},
+        "cpu_baseline": {"value": total, "unit": UNIT, "cores": procs, "kind": kind,
+                         "sample": (f"{procs} concurrent single-threaded processes of the "
+                                    f"reference ({os.path.relpath(binary, ROOT)}), each on its "
+                                    f"own {n_side}^3 sample of the workload (same grain size, "
+                                    f"material and strain rate), {args.warmup} warm-up + "
+                                    f"{args.steps} timed fixed-point iterations; the reference "
+                                    "has no threaded region and its MPI transport is replaced "
+                                    "by a single-rank stand-in")},
+        "e2e": {"value": total, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--grid", type=int, default=N_GRID)
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args(argv)
+    rank, ws = setup_dist(args.gpus)
+    if args.impl == "reference":
+        rc = run_reference_arm(args, rank, ws)
+        if _dist is not None:
+            _dist.destroy_process_group()
+        return rc
+
+    import torch
+
+    import vpfft_b200 as vp
+    from vpfft_b200 import build as vbuild
+
+    if not os.path.exists(vp.capi.LIB_PATH):
+        vbuild.build()
+    torch.cuda.init()
+    R, edot = make_inputs(args.grid, N_GRAINS if args.grid == N_GRID else
+                          max(1, round(N_GRAINS * (args.grid / N_GRID) ** 3)))
+    hbm, peak_kind = peaks()
+
+    main_res = device_arm(args, R, edot, args.precision)
+    ms = max_over_ranks(main_res["ms"])
+    N = main_res["N"]
+    value = N * args.steps * ws / (ms / 1e3)
+
+    # per-kernel device times and the roofline of the dominant kernel
+    s = 4 if args.precision == "mixed" else 8
+    alg = alg_bytes_per_voxel(s, args.grid)
+    kernels = {}
+    for name, (tot_ms, cnt) in main_res["phases"].items():
+        if cnt == 0:
+            continue
+        avg_ms = tot_ms / cnt
+        kernels[name] = {"avg_ms": avg_ms, "launches": cnt,
+                         "alg_bytes": alg[name] * N,
+                         "achieved_gbs": alg[name] * N / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0}
+    total_k = sum(k["avg_ms"] for k in kernels.values())
+    for k in kernels.values():
+        k["share"] = k["avg_ms"] / total_k if total_k else 0
+    dom = max(kernels, key=lambda k: kernels[k]["avg_ms"])
+    it_bytes = sum(alg.values()) * N
+    roofline = {
+        "bound": "hbm", "kernel": dom,
+        "achieved": kernels[dom]["achieved_gbs"], "peak": hbm, "unit": "GB/s",
+        "frac": kernels[dom]["achieved_gbs"] / hbm, "peak_kind": peak_kind,
+        "traffic": TRAFFIC_PER_LAUNCH.get((args.precision, args.grid, dom)),
+        "alg_bytes_per_voxel": alg[dom],
+        "iteration": {"alg_bytes_per_voxel": sum(alg.values()),
+                      "achieved_gbs": it_bytes / (ms / args.steps * 1e-3) / 1e9,
+                      "frac": it_bytes / (ms / args.steps * 1e-3) / 1e9 / hbm},
+    }
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 fields/FFT + f64 NR" if args.precision == "mixed" else "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": [args.grid] * 3, "grains": N_GRAINS,
+                   "seed": SEED, "precision": args.precision,
+                   "l2": "inputs larger than L2 (resident fields of the 256^3 grid)",
+                   "parallelism": f"replicas x{ws}"},
+        "roofline": roofline,
+        "kernels": kernels,
+        "gpu_launches": main_res["launches"],
+        "clocks": main_res["clocks"],
+    }
+    main_grid = main_res.pop("grid")
+
+    if not args.no_fp64 and args.precision == "mixed":
+        f = device_arm(args, R, edot, "fp64")
+        ms64 = max_over_ranks(f["ms"])
+        v64 = N * args.steps * ws / (ms64 / 1e3)
+        # error of the mixed path against the FP64 GPU path after the same
+        # number of iterations from the same state
+        s_m = main_grid.Stress()
+        s_d = f["grid"].Stress()
+        e_m = main_grid.StrainRate()
+        e_d = f["grid"].StrainRate()
+        line["fp64"] = {
+            "value": v64, "unit": UNIT, "ms_per_step": ms64 / args.steps,
+            "mixed_over_fp64": value / v64,
+            "error_vs_fp64": {
+                "avg_stress_rel": float(np.linalg.norm(main_res["avg"] - f["avg"]) /
+                                        np.linalg.norm(f["avg"])),
+                "stress_field_max_rel": float((np.linalg.norm(s_m - s_d, axis=1) /
+                                               np.linalg.norm(s_d, axis=1)).max()),
+                "strain_rate_field_rms_rel": float(np.sqrt(np.mean((e_m - e_d) ** 2)) /
+                                                   np.sqrt(np.mean(e_d ** 2))),
+                "iterations": args.warmup + args.steps},
+        }
+        f["grid"].close()
+    main_grid.close()
+
+    if not args.no_e2e:
+        e = e2e_arm(args, R, edot)
+        line["e2e"] = {"value": e["N"] * e["iters"] * ws / e["seconds"], "unit": UNIT,
+                       "h2d_bytes_per_step": e["h2d"], "d2h_bytes_per_step": e["d2h"],
+                       "steps": args.e2e_steps, "iterations": e["iters"],
+                       "step": ("one increment via vpfft_run_single_strain_step (max_iter 100, "
+                                "eps 1e-5) with pinned host orientation/stress in and the "
+                                "stress field out")}
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline_ours()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if _dist is not None:
+        _dist.destroy_process_group()
+    return 0
+
+
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from the
+# ncu captures summarised under profiles/; None until captured.
+TRAFFIC_PER_LAUNCH: dict = {}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

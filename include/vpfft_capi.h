@@ -185,6 +185,15 @@ vpfft_status vpfft_grid_synchronize(vpfft_grid *g);
 void *vpfft_grid_stream(vpfft_grid *g);
 /* Count of this library's kernel launches on the grid so far. */
 int64_t vpfft_grid_launch_count(const vpfft_grid *g);
+/* Device time per kernel of the fixed-point loop, measured with CUDA events on
+ * the grid's stream while profiling is enabled (enabling resets the sums).
+ * Phases: 0 fft_z_r2c, 1 fft_y_forward, 2 fft_x_green, 3 fft_y_inverse,
+ * 4 fft_z_c2r, 5 nr_update, 6 iter_finish.  The reference has no
+ * profiling (README.make:40-44 lists it as a TODO). */
+#define VPFFT_NUM_PHASES 7
+vpfft_status vpfft_grid_set_profiling(vpfft_grid *g, int enabled);
+vpfft_status vpfft_grid_phase_times(const vpfft_grid *g, double *ms_total, int64_t *launches);
+const char *vpfft_phase_name(int phase);
 /* Last error message of the grid (or of the library when g is NULL). */
 const char *vpfft_last_error(const vpfft_grid *g);
 

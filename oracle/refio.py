@@ -146,11 +146,21 @@ def l0_per_increment(out: dict, nx: int) -> list:
     return res
 
 
-def iteration_history(out: dict, dims) -> list:
-    """Per increment, per fixed-point iteration: (<sigma>, <edot>, d_sigma, d_eps)
-    exactly as the reference forms them (MaterialGrid.cpp:1009-1053)."""
+def _inner(a, b) -> float:
+    r = 0.0
+    for x, y in zip(a, b):
+        r += float(x) * float(y)
+    return r
+
+
+def iteration_history(out: dict, dims, edot) -> list:
+    """Per increment, per fixed-point iteration: (<sigma>, <edot>, delta_sigma,
+    delta_eps) formed from the reduced sums exactly as the reference does
+    (MaterialGrid.cpp:1009-1053): sums / N, then the error norms divided by
+    |<sigma>| and |Edot|."""
     nx, ny, nz = dims
     n = float(nx * ny * nz)
+    en = np.sqrt(_inner(edot, edot))
     ar = out["allreduce"]
     hist, off = [], 0
     for cnt in out["allreduce_counts"]:
@@ -159,7 +169,9 @@ def iteration_history(out: dict, dims) -> list:
         for row in vals:
             s = row[0:10:2] / n
             e = row[1:10:2] / n
-            its.append((s, e, row[10] / n, row[11] / n))
+            ds = (row[10] / n) / np.sqrt(_inner(s, s))
+            de = (row[11] / n) / en
+            its.append((s, e, ds, de))
         hist.append(its)
         off += cnt
     return hist

@@ -83,7 +83,7 @@ def make_case(name: str, binary: str = refio.REF_BIN) -> str:
     with tempfile.TemporaryDirectory() as td:
         out = refio.run(binary, case, td, dump_iters=c["dump_iters"],
                         dump_increments=sample is not None)
-    hist = refio.iteration_history(out, c["dims"])
+    hist = refio.iteration_history(out, c["dims"], edot)
     L0s = refio.l0_per_increment(out, nx)
     rec = dict(
         dims=np.array(c["dims"]), grains=np.array(c["grains"]), seed=np.array(c["seed"]),

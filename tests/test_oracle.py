@@ -32,7 +32,7 @@ def test_port_reproduces_reference_golden_bitwise(name, golden, port):
         out = refio.run(refio.PORT_BIN, case, td, dump_iters=dump)
     assert np.array_equal(out["iters"], g["iters"])
     assert np.array_equal(out["avg_stress"], g["avg_stress"])
-    hist = refio.iteration_history(out, case.dims)
+    hist = refio.iteration_history(out, case.dims, case.edot)
     rows = np.array([np.concatenate([s, e, [a, b]]) for h in hist for (s, e, a, b) in h])
     assert np.array_equal(rows, g["history"])
     assert np.array_equal(np.array(refio.l0_per_increment(out, case.dims[0])), g["L0"])

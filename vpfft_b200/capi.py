@@ -44,6 +44,8 @@ FIELD_STRAIN_RATE = 7
 FIELD_SCHMID = 8
 FIELD_WIDTH = {0: 5, 1: 5, 2: 9, 3: 12, 4: 1, 5: 5, 6: 5, 7: 5, 8: 60}
 
+NUM_PHASES = 7
+
 
 class Material(C.Structure):
     _fields_ = [
@@ -140,6 +142,9 @@ _PROTOS = {
     "vpfft_grid_stream": (C.c_void_p, [_G]),
     "vpfft_grid_launch_count": (C.c_int64, [_G]),
     "vpfft_last_error": (C.c_char_p, [_G]),
+    "vpfft_grid_set_profiling": (C.c_int, [_G, C.c_int]),
+    "vpfft_grid_phase_times": (C.c_int, [_G, _D, C.POINTER(C.c_int64)]),
+    "vpfft_phase_name": (C.c_char_p, [C.c_int]),
     "vpfft_solve_constitutive": (C.c_int, [C.c_int, _D, _D, _D, C.POINTER(Material), _D,
                                            C.c_double, C.c_double, C.c_int, _D]),
     "vpfft_solve_constrained_constitutive": (C.c_int, [C.c_int, _D, _D, _D, C.POINTER(Material),

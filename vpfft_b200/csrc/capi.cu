@@ -49,6 +49,7 @@ struct vpfft_grid {
   void* twz = nullptr;
   double* partials = nullptr;
   double* sum25 = nullptr;
+  double* staging = nullptr;  // voxel-major FP64 copy of one host field (N x 12 max)
   IterCtrl* ctrl = nullptr;
   IterCtrl* h_ctrl = nullptr;  // pinned
   double* hist = nullptr;
@@ -57,6 +58,11 @@ struct vpfft_grid {
   double Linv[25] = {0};
   double last_edot[5] = {0};
   long long launches = 0;
+  // per-kernel device timing of the fixed-point loop (vpfft_grid_set_profiling)
+  bool profile = false;
+  std::vector<cudaEvent_t> ev;
+  double phase_ms[VPFFT_NUM_PHASES] = {0};
+  int64_t phase_n[VPFFT_NUM_PHASES] = {0};
   std::string err;
 };
 
@@ -244,10 +250,12 @@ vpfft_status upload_twiddles(vpfft_grid* g) {
 void free_grid_buffers(vpfft_grid* g) {
   void* ptrs[] = {g->R,   g->sigma, g->lambda, g->work,     g->dkeep, g->crss,
                   g->acc, g->X,     g->twx,    g->twy,      g->twz,   g->partials,
-                  g->sum25, g->ctrl, g->hist};
+                  g->sum25, g->ctrl, g->hist, g->staging};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (g->h_ctrl) cudaFreeHost(g->h_ctrl);
+  for (cudaEvent_t e : g->ev) cudaEventDestroy(e);
+  g->ev.clear();
   if (g->stream) cudaStreamDestroy(g->stream);
 }
 
@@ -258,38 +266,37 @@ bool valid_dim(int n) {
   return n >= 1 && n <= 512 && make_line_plan(n, &p);
 }
 
+// The staging buffer holds one voxel-major FP64 field (up to 12 values per
+// voxel); it is allocated on first use and kept, so field uploads and
+// read-backs do not allocate.
+vpfft_status ensure_staging(vpfft_grid* g) {
+  if (!g->staging) CK(g, cudaMalloc(&g->staging, sizeof(double) * (size_t)g->n * 12));
+  return VPFFT_OK;
+}
+
 template <typename S>
 vpfft_status to_device_field(vpfft_grid* g, const double* host_or_dev, bool is_device, S* dst,
                              int width) {
   const size_t bytes = sizeof(double) * (size_t)g->n * width;
-  double* tmp = nullptr;
-  CK(g, cudaMalloc(&tmp, bytes));
-  cudaError_t e = is_device ? cudaMemcpyAsync(tmp, host_or_dev, bytes, cudaMemcpyDeviceToDevice, g->stream)
-                            : cudaMemcpyAsync(tmp, host_or_dev, bytes, cudaMemcpyHostToDevice, g->stream);
-  if (e != cudaSuccess) {
-    cudaFree(tmp);
-    return fail(g, VPFFT_ERR_CUDA, std::string("copy to device: ") + cudaGetErrorString(e));
-  }
-  g->launches += launch_to_soa<S>(tmp, dst, g->n, width, g->stream);
-  e = cudaGetLastError();
-  cudaError_t e2 = cudaStreamSynchronize(g->stream);
-  cudaFree(tmp);
-  if (e != cudaSuccess || e2 != cudaSuccess)
-    return fail(g, VPFFT_ERR_CUDA, std::string("to_soa: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+  vpfft_status s = ensure_staging(g);
+  if (s != VPFFT_OK) return s;
+  CK(g, cudaMemcpyAsync(g->staging, host_or_dev, bytes,
+                        is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, g->stream));
+  g->launches += launch_to_soa<S>(g->staging, dst, g->n, width, g->stream);
+  CKL(g);
+  CK(g, cudaStreamSynchronize(g->stream));
   return VPFFT_OK;
 }
 
 template <typename S>
 vpfft_status from_device_field(vpfft_grid* g, const S* src, int width, double* host) {
   const size_t bytes = sizeof(double) * (size_t)g->n * width;
-  double* tmp = nullptr;
-  CK(g, cudaMalloc(&tmp, bytes));
-  g->launches += launch_from_soa<S>(src, tmp, g->n, width, g->stream);
-  cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaMemcpyAsync(host, tmp, bytes, cudaMemcpyDeviceToHost, g->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
-  cudaFree(tmp);
-  if (e != cudaSuccess) return fail(g, VPFFT_ERR_CUDA, std::string("from_soa: ") + cudaGetErrorString(e));
+  vpfft_status s = ensure_staging(g);
+  if (s != VPFFT_OK) return s;
+  g->launches += launch_from_soa<S>(src, g->staging, g->n, width, g->stream);
+  CKL(g);
+  CK(g, cudaMemcpyAsync(host, g->staging, bytes, cudaMemcpyDeviceToHost, g->stream));
+  CK(g, cudaStreamSynchronize(g->stream));
   return VPFFT_OK;
 }
 
@@ -311,9 +318,11 @@ vpfft_status do_init(vpfft_grid* g, const double edot[5]) {
   CKL(g);
   CK(g, cudaMemcpyAsync(g->h_ctrl, g->ctrl, sizeof(IterCtrl), cudaMemcpyDeviceToHost, g->stream));
   CK(g, cudaStreamSynchronize(g->stream));
+  if (g->h_ctrl->status & kStatusNonFinite)
+    return fail(g, VPFFT_ERR_NONFINITE,
+                "initial guess is not finite (zero or non-finite macroscopic strain rate)");
   if (g->h_ctrl->status & kStatusMaxRssTiny)
-    return fail(g, VPFFT_ERR_MAX_RSS_TINY,
-                "max resolved shear stress < 1e-10 in the initial guess (zero strain rate?)");
+    return fail(g, VPFFT_ERR_MAX_RSS_TINY, "max resolved shear stress < 1e-10 in the initial guess");
   for (int c = 0; c < 5; ++c) g->last_edot[c] = edot[c];
   return VPFFT_OK;
 }
@@ -370,14 +379,39 @@ vpfft_status do_fixed_point(vpfft_grid* g, const double edot[5], int max_iter, d
   Spectral<S> sp = spectral<S>(g);
   FieldPtrs<S> f = fields<S>(g);
   const int batch = g->n >= (1LL << 21) ? 4 : 16;
+  constexpr int kEv = 8;  // events per iteration when profiling
+  if (g->profile && (int)g->ev.size() < batch * kEv) {
+    while ((int)g->ev.size() < batch * kEv) {
+      cudaEvent_t e;
+      CK(g, cudaEventCreate(&e));
+      g->ev.push_back(e);
+    }
+  }
+  int done_before = 0;
   for (;;) {
     for (int b = 0; b < batch; ++b) {
-      g->launches += launch_spectral_iteration<S>(sp, gp, (S*)g->work, g->ctrl, g->stream, 5);
-      g->launches += launch_nr_update<S>(p, f, g->partials, g->ctrl, g->hist, g->stream);
+      cudaEvent_t* e = g->profile ? &g->ev[(size_t)b * kEv] : nullptr;
+      g->launches += launch_spectral_iteration<S>(sp, gp, (S*)g->work, g->ctrl, g->stream, 5, e);
+      g->launches += launch_nr_update<S>(p, f, g->partials, g->ctrl, g->hist, g->stream,
+                                         e ? e + 6 : nullptr);
     }
     CKL(g);
     CK(g, cudaMemcpyAsync(g->h_ctrl, g->ctrl, sizeof(IterCtrl), cudaMemcpyDeviceToHost, g->stream));
     CK(g, cudaStreamSynchronize(g->stream));
+    if (g->profile) {
+      // only the iterations that ran (the rest returned at once on `done`)
+      const int ran = g->h_ctrl->iter - done_before;
+      for (int b = 0; b < ran && b < batch; ++b) {
+        const cudaEvent_t* e = &g->ev[(size_t)b * kEv];
+        for (int k = 0; k < VPFFT_NUM_PHASES; ++k) {
+          float ms = 0.f;
+          CK(g, cudaEventElapsedTime(&ms, e[k], e[k + 1]));
+          g->phase_ms[k] += ms;
+          g->phase_n[k] += 1;
+        }
+      }
+    }
+    done_before = g->h_ctrl->iter;
     if (g->h_ctrl->done) break;
   }
   const IterCtrl& c = *g->h_ctrl;
@@ -838,6 +872,32 @@ vpfft_status vpfft_grid_synchronize(vpfft_grid* g) {
   return VPFFT_OK;
 }
 void* vpfft_grid_stream(vpfft_grid* g) { return g ? (void*)g->stream : nullptr; }
+
+vpfft_status vpfft_grid_set_profiling(vpfft_grid* g, int enabled) {
+  if (!g) return VPFFT_ERR_INVALID_ARGUMENT;
+  g->profile = enabled != 0;
+  for (int k = 0; k < VPFFT_NUM_PHASES; ++k) {
+    g->phase_ms[k] = 0;
+    g->phase_n[k] = 0;
+  }
+  return VPFFT_OK;
+}
+
+vpfft_status vpfft_grid_phase_times(const vpfft_grid* g, double* ms, int64_t* counts) {
+  if (!g || !ms || !counts) return VPFFT_ERR_INVALID_ARGUMENT;
+  for (int k = 0; k < VPFFT_NUM_PHASES; ++k) {
+    ms[k] = g->phase_ms[k];
+    counts[k] = g->phase_n[k];
+  }
+  return VPFFT_OK;
+}
+
+const char* vpfft_phase_name(int phase) {
+  static const char* names[VPFFT_NUM_PHASES] = {"fft_z_r2c", "fft_y_forward", "fft_x_green",
+                                                "fft_y_inverse", "fft_z_c2r", "nr_update",
+                                                "iter_finish"};
+  return (phase >= 0 && phase < VPFFT_NUM_PHASES) ? names[phase] : "";
+}
 int64_t vpfft_grid_launch_count(const vpfft_grid* g) { return g ? g->launches : 0; }
 const char* vpfft_last_error(const vpfft_grid* g) { return g ? g->err.c_str() : g_lib_err.c_str(); }
 

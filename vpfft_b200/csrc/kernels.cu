@@ -293,6 +293,8 @@ __global__ void __launch_bounds__(kVoxelBlock) k_init(VoxelParams p, FieldPtrs<S
     for (int c = 0; c < 5; ++c) g[c] /= mx;
   }
   if (mx < 1e-10) atomicOr(&ctrl->status, kStatusMaxRssTiny);
+  // a zero strain rate makes the Sachs guess 0/0 (Solvers.cpp:241)
+  if (!isfinite(mx)) atomicOr(&ctrl->status, kStatusNonFinite);
   int flag;
   nr_unconstrained(m, tau, p.mat, p.edot, p.init_eps, p.imposed_max_rss, p.init_max_iter, g, &flag);
   store5(f.sigma, n, v, g);
@@ -597,10 +599,12 @@ int launch_ref_medium(const VoxelParams& p, const FieldPtrs<S>& f, double* parti
 }
 template <typename S>
 int launch_nr_update(const VoxelParams& p, const FieldPtrs<S>& f, double* partials,
-                     IterCtrl* ctrl, double* hist, cudaStream_t st) {
+                     IterCtrl* ctrl, double* hist, cudaStream_t st, cudaEvent_t* ev) {
   const int nb = nr_blocks(p.n);
   k_nr_update<S><<<nb, kVoxelBlock, 0, st>>>(p, f, partials, ctrl);
+  if (ev) cudaEventRecord(ev[0], st);
   k_iter_finish<<<1, kFinishThreads, 0, st>>>(partials, nb, ctrl, hist);
+  if (ev) cudaEventRecord(ev[1], st);
   return 2;
 }
 template <typename S>
@@ -868,7 +872,8 @@ void optin_all() {
 
 template <typename S>
 int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S* work,
-                              const IterCtrl* ctrl, cudaStream_t st, int ncomp) {
+                              const IterCtrl* ctrl, cudaStream_t st, int ncomp,
+                              cudaEvent_t* ev) {
   using T = typename CT<S>::T;
   optin_all<S>();
   const Tiles<S> t = pick_tiles(sp, ncomp);
@@ -878,14 +883,20 @@ int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S
   const T* twy = reinterpret_cast<const T*>(sp.twy);
   const T* twz = reinterpret_cast<const T*>(sp.twz);
   const int gz = (int)((nlines + 2 * t.ppb_z - 1) / (2 * t.ppb_z));
+  if (ev) cudaEventRecord(ev[0], st);
   k_fft_z_r2c<S><<<gz, 256, t.sm_z, st>>>(work, X, sp.pz, twz, nlines, sp.nh, t.ppb_z, ctrl);
+  if (ev) cudaEventRecord(ev[1], st);
   dim3 gy((sp.nh + t.tk_y - 1) / t.tk_y, ncomp * sp.nx);
   k_fft_y<-1, S><<<gy, 256, t.sm_y, st>>>(X, sp.py, twy, sp.nh, t.tk_y, ctrl);
+  if (ev) cudaEventRecord(ev[2], st);
   dim3 gx((sp.nh + t.tk_x - 1) / t.tk_x, sp.ny);
   k_fft_x<2, S><<<gx, 256, t.sm_x, st>>>(X, sp.px, twx, gp, sp.ny, sp.nh, t.tk_x, ncomp, ctrl);
+  if (ev) cudaEventRecord(ev[3], st);
   k_fft_y<1, S><<<gy, 256, t.sm_y, st>>>(X, sp.py, twy, sp.nh, t.tk_y, ctrl);
+  if (ev) cudaEventRecord(ev[4], st);
   const S scale = S(1.0 / ((double)sp.nx * sp.ny * sp.nz));
   k_fft_z_c2r<S><<<gz, 256, t.sm_z, st>>>(X, work, sp.pz, twz, nlines, sp.nh, t.ppb_z, scale, ctrl);
+  if (ev) cudaEventRecord(ev[5], st);
   return 5;
 }
 
@@ -1069,7 +1080,7 @@ int launch_green_batch(int n, const int32_t* kidx, const GreenParams<R>& gp, con
   template int launch_ref_medium<S>(const VoxelParams&, const FieldPtrs<S>&, double*, double*,   \
                                     cudaStream_t);                                               \
   template int launch_nr_update<S>(const VoxelParams&, const FieldPtrs<S>&, double*, IterCtrl*,  \
-                                   double*, cudaStream_t);                                       \
+                                   double*, cudaStream_t, cudaEvent_t*);                         \
   template int launch_post<S>(const PostParams&, const FieldPtrs<S>&, S*, cudaStream_t);         \
   template int launch_strain_rate<S>(const VoxelParams&, const FieldPtrs<S>&, S*, cudaStream_t); \
   template int launch_schmid_field<S>(long long, const S*, double*, cudaStream_t);               \
@@ -1078,7 +1089,7 @@ int launch_green_batch(int n, const int32_t* kidx, const GreenParams<R>& gp, con
   template int launch_fill<S>(S*, long long, double, cudaStream_t);                              \
   template int launch_crss_broadcast<S>(S*, long long, const double*, cudaStream_t);             \
   template int launch_spectral_iteration<S>(const Spectral<S>&, const GreenParams<S>&, S*,       \
-                                            const IterCtrl*, cudaStream_t, int);                 \
+                                            const IterCtrl*, cudaStream_t, int, cudaEvent_t*);   \
   template int launch_fft3d<S>(const Spectral<S>&, S*, int, int, cudaStream_t);                  \
   template size_t spectral_smem_optin<S>(int);                                                   \
   template int launch_green_batch<S>(int, const int32_t*, const GreenParams<S>&, const double*,  \

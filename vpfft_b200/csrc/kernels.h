@@ -74,9 +74,10 @@ int launch_init(const VoxelParams& p, const FieldPtrs<S>& f, IterCtrl* ctrl, cud
 template <typename S>
 int launch_ref_medium(const VoxelParams& p, const FieldPtrs<S>& f, double* partials,
                       double* out25, cudaStream_t st);
+// ev (optional): 2 events recorded after the NR kernel and after the finish kernel
 template <typename S>
 int launch_nr_update(const VoxelParams& p, const FieldPtrs<S>& f, double* partials,
-                     IterCtrl* ctrl, double* hist, cudaStream_t st);
+                     IterCtrl* ctrl, double* hist, cudaStream_t st, cudaEvent_t* ev = nullptr);
 template <typename S>
 int launch_post(const PostParams& p, const FieldPtrs<S>& f, S* crss_out, cudaStream_t st);
 template <typename S>
@@ -108,9 +109,11 @@ struct Spectral {
   void* X;          // 5 x nx x ny x nh complex R
 };
 // forward: work (P) -> X ; inverse: X -> work (d~, scaled by 1/N)
+// ev (optional): 6 events recorded before the first and after each of the 5 kernels
 template <typename S>
 int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S* work,
-                              const IterCtrl* ctrl, cudaStream_t st, int ncomp);
+                              const IterCtrl* ctrl, cudaStream_t st, int ncomp,
+                              cudaEvent_t* ev = nullptr);
 // forward-only / inverse-only transforms for testing (mode 0 = forward, 1 = inverse)
 template <typename S>
 int launch_fft3d(const Spectral<S>& sp, S* real, int ncomp, int mode, cudaStream_t st);

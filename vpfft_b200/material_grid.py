@@ -191,6 +191,18 @@ class MaterialGrid:
     def launch_count(self) -> int:
         return int(self._lib.vpfft_grid_launch_count(self._h))
 
+    def set_profiling(self, enabled: bool) -> None:
+        check(self._lib.vpfft_grid_set_profiling(self._h, int(bool(enabled))), self._h)
+
+    def phase_times(self) -> dict:
+        """{phase name: (total device ms, launches)} of the fixed-point loop."""
+        ms = np.zeros(capi.NUM_PHASES)
+        cnt = np.zeros(capi.NUM_PHASES, np.int64)
+        check(self._lib.vpfft_grid_phase_times(self._h, dptr(ms),
+                                               cnt.ctypes.data_as(C.POINTER(C.c_int64))), self._h)
+        return {self._lib.vpfft_phase_name(k).decode(): (float(ms[k]), int(cnt[k]))
+                for k in range(capi.NUM_PHASES)}
+
     def synchronize(self) -> None:
         check(self._lib.vpfft_grid_synchronize(self._h), self._h)
 
