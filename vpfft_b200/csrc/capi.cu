@@ -55,7 +55,8 @@ struct vpfft_grid {
   double* hist = nullptr;
   int hist_cap = 0;
   double L0[25] = {0};
-  double Linv[25] = {0};
+  double Linv[25] = {0};      // inverse(-L0): the Nyquist-plane operator
+  double L0inv_sym[15] = {0}; // symmetric part of L0^-1, packed (Newton step)
   double last_edot[5] = {0};
   long long launches = 0;
   // per-kernel device timing of the fixed-point loop (vpfft_grid_set_profiling)
@@ -157,6 +158,12 @@ void inverse5_host(const double* a, double* out) {
   }
 }
 
+}  // namespace
+
+void vpfft::inverse5_colmajor(const double* a, double* out) { inverse5_host(a, out); }
+
+namespace {
+
 MaterialParams mat_params(const vpfft_material& m) {
   MaterialParams p;
   for (int k = 0; k < kNS; ++k) {
@@ -198,6 +205,33 @@ VoxelParams voxel_params(vpfft_grid* g, const double edot[5]) {
                     edot[3] * edot[3] + edot[4] * edot[4];
   double imposed = 2.0 * std::pow(ee / g->mat.gamma_dot_base[0], (double)(1. / (float)min_n));
   p.imposed_max_rss = (2.0 < imposed) ? imposed : 2.0;
+  return p;
+}
+
+// Launch constants of the Newton kernels: the initialisation solve
+// (InitializeComputation, MaterialGrid.cpp:159-166) or the loop solve (909-911).
+NRParams nr_params(vpfft_grid* g, const double edot[5], bool init) {
+  VoxelParams v = voxel_params(g, edot);
+  NRParams p{};
+  p.n = g->n;
+  for (int c = 0; c < 5; ++c) p.edot[c] = edot[c];
+  for (int k = 0; k < 25; ++k) p.L0[k] = g->L0[k];
+  for (int k = 0; k < 15; ++k) p.L0inv[k] = g->L0inv_sym[k];
+  for (int q = 0; q < kNS; ++q) {
+    p.gdot[q] = g->mat.gamma_dot_base[q];
+    p.nexp[q] = g->mat.rate_sensitivity[q];
+    p.crss[q] = g->mat.crss[q];
+    p.icrss[q] = 1.0 / g->mat.crss[q];
+  }
+  if (init) {
+    p.eps = g->opt.init_nr_epsilon;
+    p.max_rss = v.imposed_max_rss;
+    p.max_iter = g->opt.init_nr_max_iter;
+  } else {
+    p.eps = g->opt.nr_epsilon;
+    p.max_rss = g->opt.nr_max_resolved;
+    p.max_iter = g->opt.nr_max_iter;
+  }
   return p;
 }
 
@@ -310,7 +344,7 @@ vpfft_status ensure_crss_array(vpfft_grid* g) {
 template <typename S>
 vpfft_status do_init(vpfft_grid* g, const double edot[5]) {
   if (!g->fields_set) return fail(g, VPFFT_ERR_NOT_INITIALIZED, "fields not set");
-  VoxelParams p = voxel_params(g, edot);
+  NRParams p = nr_params(g, edot, true);
   IterCtrl h{};
   h.n_voxels = (double)g->n;
   CK(g, cudaMemcpyAsync(g->ctrl, &h, sizeof(h), cudaMemcpyHostToDevice, g->stream));
@@ -348,6 +382,10 @@ vpfft_status do_ref_medium(vpfft_grid* g, double* L0_out) {
   double negL[25];
   for (int k = 0; k < 25; ++k) negL[k] = -g->L0[k];
   inverse5_host(negL, g->Linv);  // StrainRateEvolutionWithFFT, MaterialGrid.cpp:628-632
+  double inv[25];
+  inverse5_host(g->L0, inv);
+  for (int i = 0; i < 5; ++i)
+    for (int j = i; j < 5; ++j) g->L0inv_sym[sym5(i, j)] = 0.5 * (inv[j * 5 + i] + inv[i * 5 + j]);
   g->have_L0 = true;
   if (L0_out) std::memcpy(L0_out, g->L0, sizeof(g->L0));
   return VPFFT_OK;
@@ -374,7 +412,7 @@ vpfft_status do_fixed_point(vpfft_grid* g, const double edot[5], int max_iter, d
                           edot[3] * edot[3] + edot[4] * edot[4]);
   h.n_voxels = (double)g->n;
   CK(g, cudaMemcpyAsync(g->ctrl, &h, sizeof(h), cudaMemcpyHostToDevice, g->stream));
-  VoxelParams p = voxel_params(g, edot);
+  NRParams p = nr_params(g, edot, false);
   GreenParams<S> gp = green_params<S>(g->nx, g->ny, g->nz, g->h, g->L0, g->Linv);
   Spectral<S> sp = spectral<S>(g);
   FieldPtrs<S> f = fields<S>(g);

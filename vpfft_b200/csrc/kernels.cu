@@ -18,6 +18,7 @@
 #include <math.h>
 #include <stdint.h>
 
+#include "kernel_common.cuh"
 #include "kernels.h"
 
 namespace vpfft {
@@ -164,31 +165,6 @@ bool make_line_plan(int n, LinePlan* p) {
   return m == 1;
 }
 
-// Fixed-order block reduction of W doubles per thread; thread 0 of the block
-// writes the W sums to out.
-template <int W, int BLOCK>
-__device__ __forceinline__ void block_reduce_store(double (&acc)[W], double* out) {
-  __shared__ double sm[BLOCK / 32][W];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int k = 0; k < W; ++k) {
-    double v = acc[k];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-    if (lane == 0) sm[warp][k] = v;
-  }
-  __syncthreads();
-  if (warp == 0) {
-#pragma unroll
-    for (int k = 0; k < W; ++k) {
-      double v = lane < BLOCK / 32 ? sm[lane][k] : 0.0;
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-      if (lane == 0) out[k] = v;
-    }
-  }
-}
-
 // Neumaier (improved Kahan) accumulator; combined pairwise in a fixed tree.
 struct Neu {
   double s, c;
@@ -208,7 +184,6 @@ __device__ __forceinline__ Neu neu_merge(Neu a, Neu b) {
   return r;
 }
 
-constexpr int kFinishThreads = 256;
 
 // Column sums of partials[nparts][width] with compensated, fixed-order
 // summation; one block.
@@ -238,69 +213,10 @@ __global__ void k_column_sums(const double* partials, int nparts, int width, dou
   column_sums(partials, nparts, width, out);
 }
 
-template <typename S>
-__device__ __forceinline__ void load_R(const S* __restrict__ R, long long n, long long v,
-                                       double r[9]) {
-#pragma unroll
-  for (int k = 0; k < 9; ++k) r[k] = (double)R[k * n + v];
-}
-template <typename S>
-__device__ __forceinline__ void load_tau(const S* __restrict__ crss, const double* uni,
-                                         long long n, long long v, double tau[kNS]) {
-  if (crss) {
-#pragma unroll
-    for (int k = 0; k < kNS; ++k) tau[k] = (double)crss[k * n + v];
-  } else {
-#pragma unroll
-    for (int k = 0; k < kNS; ++k) tau[k] = uni[k];
-  }
-}
-template <typename S>
-__device__ __forceinline__ void load5(const S* __restrict__ f, long long n, long long v,
-                                      double x[5]) {
-#pragma unroll
-  for (int c = 0; c < 5; ++c) x[c] = (double)f[c * n + v];
-}
-template <typename S>
-__device__ __forceinline__ void store5(S* __restrict__ f, long long n, long long v,
-                                       const double x[5]) {
-#pragma unroll
-  for (int c = 0; c < 5; ++c) f[c * n + v] = (S)x[c];
-}
-
 // ============================================================== voxel phases
-constexpr int kVoxelBlock = 128;
 
 int nr_blocks(long long n) { return (int)((n + kVoxelBlock - 1) / kVoxelBlock); }
 int ref_medium_blocks(long long n) { return nr_blocks(n); }
-
-// InitializeComputation (MaterialGrid.cpp:153-210): Sachs guess, scaled to the
-// yield surface when MaxRSS > 1.1, unconstrained NR; lambda = P = sigma.
-template <typename S>
-__global__ void __launch_bounds__(kVoxelBlock) k_init(VoxelParams p, FieldPtrs<S> f, IterCtrl* ctrl) {
-  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= p.n) return;
-  const long long n = p.n;
-  double R[9], m[kNS][5], tau[kNS];
-  load_R(f.R, n, v, R);
-  schmid_from_R(R, m);
-  load_tau(f.crss, p.crss, n, v, tau);
-  double g[5];
-  sachs(m, tau, p.edot, g);
-  const double mx = max_rss(m, tau, g);
-  if (mx > 1.1) {
-#pragma unroll
-    for (int c = 0; c < 5; ++c) g[c] /= mx;
-  }
-  if (mx < 1e-10) atomicOr(&ctrl->status, kStatusMaxRssTiny);
-  // a zero strain rate makes the Sachs guess 0/0 (Solvers.cpp:241)
-  if (!isfinite(mx)) atomicOr(&ctrl->status, kStatusNonFinite);
-  int flag;
-  nr_unconstrained(m, tau, p.mat, p.edot, p.init_eps, p.imposed_max_rss, p.init_max_iter, g, &flag);
-  store5(f.sigma, n, v, g);
-  store5(f.lambda, n, v, g);
-  store5(f.work, n, v, g);
-}
 
 // BuildLinearRefMediumStiffness (MaterialGrid.cpp:219-282), per voxel:
 //   (sum_s m_s (x) m_s gdot0 |r_s|^(n-1) / tau_s)^-1, block partial sums of the
@@ -350,74 +266,6 @@ __global__ void __launch_bounds__(kVoxelBlock) k_ref_medium(VoxelParams p, Field
       for (int j = 0; j < 5; ++j) acc[j * 5 + i] = Mi[i][j];
   }
   block_reduce_store<25, kVoxelBlock>(acc, partials + (long long)blockIdx.x * 25);
-}
-
-// The per-voxel body of the fixed-point loop (MaterialGrid.cpp:946-1003):
-//   sigma /= MaxRSS(sigma); sigma = SolveConstrained(...); edot = Apply(sigma);
-//   P = sigma - L0 d~; lambda += L0 (Edot + d~ - edot);
-// and the block partials of sum sigma, sum edot, sum |sigma - lambda|,
-// sum |edot - Edot - d~| (lambda already updated).  `work` holds d~ on entry
-// and P on exit.
-template <typename S>
-__global__ void __launch_bounds__(kVoxelBlock) k_nr_update(VoxelParams p, FieldPtrs<S> f,
-                                                           double* partials, IterCtrl* ctrl) {
-  if (ctrl->done) return;
-  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  double acc[12];
-#pragma unroll
-  for (int k = 0; k < 12; ++k) acc[k] = 0.0;
-  if (v < p.n) {
-    const long long n = p.n;
-    double R[9], m[kNS][5], tau[kNS], s[5], lam[5], d[5];
-    load_R(f.R, n, v, R);
-    schmid_from_R(R, m);
-    load_tau(f.crss, p.crss, n, v, tau);
-    load5(f.sigma, n, v, s);
-    load5(f.lambda, n, v, lam);
-    load5(f.work, n, v, d);
-    if (f.dkeep) store5(f.dkeep, n, v, d);
-    const double mx = max_rss(m, tau, s);
-    if (mx < 1e-10) atomicOr(&ctrl->status, kStatusMaxRssTiny);
-#pragma unroll
-    for (int c = 0; c < 5; ++c) s[c] /= mx;
-    double rel;
-    int flag;
-    nr_constrained(m, tau, p.mat, p.edot, lam, d, p.L0, p.nr_eps, p.nr_max_rss, p.nr_max_iter, s,
-                   &rel, &flag);
-    if (flag != NR_OK) atomicAdd(&ctrl->nr_capped, 1ull);
-    double e[5];
-    apply_constitutive(m, tau, p.mat, s, e);
-    double P[5], T[5];
-#pragma unroll
-    for (int c = 0; c < 5; ++c) T[c] = p.edot[c] + d[c] - e[c];
-#pragma unroll
-    for (int i = 0; i < 5; ++i) {
-      double ld = 0.0, lt = 0.0;
-#pragma unroll
-      for (int j = 0; j < 5; ++j) {
-        ld += p.L0[j * 5 + i] * d[j];
-        lt += p.L0[j * 5 + i] * T[j];
-      }
-      P[i] = s[i] - ld;
-      lam[i] += lt;
-    }
-    store5(f.sigma, n, v, s);
-    store5(f.lambda, n, v, lam);
-    store5(f.work, n, v, P);
-    double es = 0.0, ee = 0.0;
-#pragma unroll
-    for (int c = 0; c < 5; ++c) {
-      acc[c] = s[c];
-      acc[5 + c] = e[c];
-      const double ds = s[c] - lam[c];
-      const double de = e[c] - p.edot[c] - d[c];
-      es += ds * ds;
-      ee += de * de;
-    }
-    acc[10] = sqrt(es);
-    acc[11] = sqrt(ee);
-  }
-  block_reduce_store<12, kVoxelBlock>(acc, partials + (long long)blockIdx.x * 12);
 }
 
 // Reductions and convergence test of one iteration (MaterialGrid.cpp:1009-1068).
@@ -585,26 +433,11 @@ __global__ void k_crss_broadcast(S* dst, long long n, Crss12 c) {
 static inline int grid1d(long long count, int block) { return (int)((count + block - 1) / block); }
 
 template <typename S>
-int launch_init(const VoxelParams& p, const FieldPtrs<S>& f, IterCtrl* ctrl, cudaStream_t st) {
-  k_init<S><<<nr_blocks(p.n), kVoxelBlock, 0, st>>>(p, f, ctrl);
-  return 1;
-}
-template <typename S>
 int launch_ref_medium(const VoxelParams& p, const FieldPtrs<S>& f, double* partials,
                       double* out25, cudaStream_t st) {
   const int nb = ref_medium_blocks(p.n);
   k_ref_medium<S><<<nb, kVoxelBlock, 0, st>>>(p, f, partials);
   k_column_sums<<<1, kFinishThreads, 0, st>>>(partials, nb, 25, out25);
-  return 2;
-}
-template <typename S>
-int launch_nr_update(const VoxelParams& p, const FieldPtrs<S>& f, double* partials,
-                     IterCtrl* ctrl, double* hist, cudaStream_t st, cudaEvent_t* ev) {
-  const int nb = nr_blocks(p.n);
-  k_nr_update<S><<<nb, kVoxelBlock, 0, st>>>(p, f, partials, ctrl);
-  if (ev) cudaEventRecord(ev[0], st);
-  k_iter_finish<<<1, kFinishThreads, 0, st>>>(partials, nb, ctrl, hist);
-  if (ev) cudaEventRecord(ev[1], st);
   return 2;
 }
 template <typename S>
@@ -946,40 +779,6 @@ struct Mat25 {
   double v[25];
 };
 
-__global__ void k_solvers_constrained(int n, const double* s0, const double* schmid,
-                                      const double* crss, MaterialParams mp, Vec5 edot,
-                                      const double* lambda, const double* dtilde, Mat25 L0,
-                                      double eps, double max_rss, int max_iter, double* out,
-                                      double* nr_err) {
-  const int v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= n) return;
-  double m[kNS][5], tau[kNS], s[5], lam[5], d[5];
-  load_schmid(schmid, v, m);
-  load_crss_v(crss, v, tau);
-  for (int c = 0; c < 5; ++c) {
-    s[c] = s0[v * 5 + c];
-    lam[c] = lambda[v * 5 + c];
-    d[c] = dtilde[v * 5 + c];
-  }
-  double rel;
-  int flag;
-  nr_constrained(m, tau, mp, edot.v, lam, d, L0.v, eps, max_rss, max_iter, s, &rel, &flag);
-  for (int c = 0; c < 5; ++c) out[v * 5 + c] = s[c];
-  if (nr_err) nr_err[v] = rel;
-}
-__global__ void k_solvers_unconstrained(int n, const double* s0, const double* schmid,
-                                        const double* crss, MaterialParams mp, Vec5 edot,
-                                        double eps, double max_rss, int max_iter, double* out) {
-  const int v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= n) return;
-  double m[kNS][5], tau[kNS], s[5];
-  load_schmid(schmid, v, m);
-  load_crss_v(crss, v, tau);
-  for (int c = 0; c < 5; ++c) s[c] = s0[v * 5 + c];
-  int flag;
-  nr_unconstrained(m, tau, mp, edot.v, eps, max_rss, max_iter, s, &flag);
-  for (int c = 0; c < 5; ++c) out[v * 5 + c] = s[c];
-}
 __global__ void k_solvers_apply(int n, const double* s_in, const double* schmid,
                                 const double* crss, MaterialParams mp, double* out) {
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1027,30 +826,6 @@ __global__ void k_green_batch(int n, const int32_t* kidx, GreenParams<R> gp, con
   }
 }
 
-int launch_solvers_constrained(int n, const double* s0, const double* schmid, const double* crss,
-                               const MaterialParams& mp, const double edot[5],
-                               const double* lambda, const double* dtilde, const double L0[25],
-                               double eps, double max_rss, int max_iter, double* out,
-                               double* nr_err, cudaStream_t st) {
-  Vec5 e;
-  Mat25 l;
-  for (int c = 0; c < 5; ++c) e.v[c] = edot[c];
-  for (int c = 0; c < 25; ++c) l.v[c] = L0[c];
-  k_solvers_constrained<<<grid1d(n, 128), 128, 0, st>>>(n, s0, schmid, crss, mp, e, lambda,
-                                                         dtilde, l, eps, max_rss, max_iter, out,
-                                                         nr_err);
-  return 1;
-}
-int launch_solvers_unconstrained(int n, const double* s0, const double* schmid,
-                                 const double* crss, const MaterialParams& mp,
-                                 const double edot[5], double eps, double max_rss, int max_iter,
-                                 double* out, cudaStream_t st) {
-  Vec5 e;
-  for (int c = 0; c < 5; ++c) e.v[c] = edot[c];
-  k_solvers_unconstrained<<<grid1d(n, 128), 128, 0, st>>>(n, s0, schmid, crss, mp, e, eps,
-                                                           max_rss, max_iter, out);
-  return 1;
-}
 int launch_solvers_apply(int n, const double* s, const double* schmid, const double* crss,
                          const MaterialParams& mp, double* out, cudaStream_t st) {
   k_solvers_apply<<<grid1d(n, 128), 128, 0, st>>>(n, s, schmid, crss, mp, out);
@@ -1076,11 +851,8 @@ int launch_green_batch(int n, const int32_t* kidx, const GreenParams<R>& gp, con
 
 // ============================================================== instantiations
 #define VPFFT_INST(S)                                                                            \
-  template int launch_init<S>(const VoxelParams&, const FieldPtrs<S>&, IterCtrl*, cudaStream_t); \
   template int launch_ref_medium<S>(const VoxelParams&, const FieldPtrs<S>&, double*, double*,   \
                                     cudaStream_t);                                               \
-  template int launch_nr_update<S>(const VoxelParams&, const FieldPtrs<S>&, double*, IterCtrl*,  \
-                                   double*, cudaStream_t, cudaEvent_t*);                         \
   template int launch_post<S>(const PostParams&, const FieldPtrs<S>&, S*, cudaStream_t);         \
   template int launch_strain_rate<S>(const VoxelParams&, const FieldPtrs<S>&, S*, cudaStream_t); \
   template int launch_schmid_field<S>(long long, const S*, double*, cudaStream_t);               \

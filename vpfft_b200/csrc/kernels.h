@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include "device_math.cuh"
+#include "nr_kernel.cuh"
 
 namespace vpfft {
 
@@ -70,14 +71,16 @@ struct FieldPtrs {
 
 // --- voxel phases (kernels.cu); each returns the number of kernels launched
 template <typename S>
-int launch_init(const VoxelParams& p, const FieldPtrs<S>& f, IterCtrl* ctrl, cudaStream_t st);
+int launch_init(const NRParams& p, const FieldPtrs<S>& f, IterCtrl* ctrl, cudaStream_t st);
 template <typename S>
 int launch_ref_medium(const VoxelParams& p, const FieldPtrs<S>& f, double* partials,
                       double* out25, cudaStream_t st);
 // ev (optional): 2 events recorded after the NR kernel and after the finish kernel
 template <typename S>
-int launch_nr_update(const VoxelParams& p, const FieldPtrs<S>& f, double* partials,
+int launch_nr_update(const NRParams& p, const FieldPtrs<S>& f, double* partials,
                      IterCtrl* ctrl, double* hist, cudaStream_t st, cudaEvent_t* ev = nullptr);
+// host LU inverse of a column-major 5x5 (capi.cu)
+void inverse5_colmajor(const double* a, double* out);
 template <typename S>
 int launch_post(const PostParams& p, const FieldPtrs<S>& f, S* crss_out, cudaStream_t st);
 template <typename S>

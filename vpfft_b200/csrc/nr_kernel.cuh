@@ -1,0 +1,383 @@
+// nr_kernel.cuh -- the per-voxel Newton-Raphson solves of the fixed-point loop
+// and of the initialisation, arranged for sm_100a.
+//
+// Layout per thread: the 12 rotated Schmid 5-vectors of the voxel being solved
+// live in shared memory (msm[(s*5 + c) * blockDim + tid], so a warp's loads are
+// conflict-free) instead of 120 registers; the Newton state, the accumulated
+// Jacobian and the 5x5 solve stay in registers.  One pass over the 12 systems
+// per Newton step computes the resolved shear r_s, the admissibility test, the
+// strain-rate sum S and the Jacobian sum K together.
+//
+// The constrained Newton step of the reference (Solvers.cpp:184-211)
+//     J d = R,  J = -I - L0 K,  R = (s - lambda) + L0 (S - Edot - d~)
+// is solved in its equivalent symmetric positive-definite form
+//     (L0^-1 + K) d = -y,  y = L0^-1 (s - lambda) + (S - Edot - d~)
+// (multiply by -L0^-1; L0 is an average of SPD matrices and K is PSD) with an
+// LDL^T factorisation, which needs no pivoting; the reference's full-pivot LU
+// and this give the same step up to rounding.  The unconstrained Newton of the
+// initialisation (Solvers.cpp:19-101) solves K d = -R the same way and falls
+// back to complete pivoting when K is singular (systems with r_s snapped to 0).
+#pragma once
+
+#include "device_math.cuh"
+
+namespace vpfft {
+
+// x^E for a compile-time E >= 0 by repeated squaring
+template <int E, typename T>
+__device__ __forceinline__ T cpow(T x) {
+  if constexpr (E == 0) {
+    return T(1);
+  } else if constexpr (E == 1) {
+    return x;
+  } else {
+    const T h = cpow<E / 2>(x);
+    if constexpr (E & 1)
+      return h * h * x;
+    else
+      return h * h;
+  }
+}
+template <typename T>
+__device__ __forceinline__ T ipow_t(T x, int e) {
+  T r = T(1), b = x;
+  while (e > 0) {
+    if (e & 1) r *= b;
+    b *= b;
+    e >>= 1;
+  }
+  return r;
+}
+// |r|^(n-1) with n known at compile time (NEXP > 0) or at run time (NEXP == 0)
+template <int NEXP, typename T>
+__device__ __forceinline__ T pow_nm1(T a, int n) {
+  if constexpr (NEXP > 0) {
+    return cpow<NEXP - 1>(a);
+  } else {
+    return n - 1 >= 0 ? ipow_t(a, n - 1) : T(1) / ipow_t(a, 1 - n);
+  }
+}
+template <int NEXP, typename T>
+__device__ __forceinline__ T pow_n(T a, int n) {
+  if constexpr (NEXP > 0) {
+    return cpow<NEXP>(a);
+  } else {
+    return ipow_t(a, n);
+  }
+}
+
+// Per-launch constants of the NR kernels.
+struct NRParams {
+  long long n;
+  double edot[5];
+  double L0[25];      // column-major
+  double L0inv[15];   // symmetric part of L0^-1, packed upper triangle row by row
+  double gdot[kNS];
+  int32_t nexp[kNS];
+  double crss[kNS];   // uniform CRSS (used when the per-voxel array is absent)
+  double icrss[kNS];  // 1 / crss
+  double eps;         // NR relative-step tolerance
+  double max_rss;     // admissibility cap of |r_s|
+  int32_t max_iter;
+  int32_t pad_;
+};
+
+// packed index of (i, j), i <= j, in a symmetric 5x5
+__host__ __device__ constexpr int sym5(int i, int j) {
+  return i <= j ? (i * (9 - i)) / 2 + j : (j * (9 - j)) / 2 + i;
+}
+
+// Rotated Schmid 5-vectors of one voxel into shared memory (see schmid_from_R).
+template <typename MS>
+__device__ __forceinline__ void schmid_to_smem(const double R[9], MS* msm, int bs) {
+#pragma unroll
+  for (int s = 0; s < kNS; ++s) {
+    double b[3], n[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      b[i] = R[3 * i + 0] * slip_b(s, 0) + R[3 * i + 1] * slip_b(s, 1) + R[3 * i + 2] * slip_b(s, 2);
+      n[i] = R[3 * i + 0] * slip_n(s, 0) + R[3 * i + 1] * slip_n(s, 1) + R[3 * i + 2] * slip_n(s, 2);
+    }
+    const double q00 = b[0] * n[0], q11 = b[1] * n[1], q22 = b[2] * n[2];
+    msm[(s * 5 + 0) * bs] = (MS)((q11 - q00) * VPFFT_INV_2SQRT3);
+    msm[(s * 5 + 1) * bs] = (MS)((2.0 * q22 - q00 - q11) * (1.0 / 6.0));
+    msm[(s * 5 + 2) * bs] = (MS)((b[1] * n[2] + b[2] * n[1]) * VPFFT_INV_2SQRT3);
+    msm[(s * 5 + 3) * bs] = (MS)((b[0] * n[2] + b[2] * n[0]) * VPFFT_INV_2SQRT3);
+    msm[(s * 5 + 4) * bs] = (MS)((b[0] * n[1] + b[1] * n[0]) * VPFFT_INV_2SQRT3);
+  }
+}
+
+template <typename MS>
+__device__ __forceinline__ void load_m(const MS* msm, int bs, int s, double m[5]) {
+#pragma unroll
+  for (int c = 0; c < 5; ++c) m[c] = (double)msm[(s * 5 + c) * bs];
+}
+
+// LDL^T solve of a symmetric positive-definite 5x5 A (packed upper) x = b.
+// Returns false when a pivot is not positive (A not numerically SPD).
+__device__ __forceinline__ bool ldlt5_solve(const double A[15], const double b[5], double x[5]) {
+  double L[5][5], d[5], id[5];
+  bool ok = true;
+#pragma unroll
+  for (int j = 0; j < 5; ++j) {
+    double dj = A[sym5(j, j)];
+#pragma unroll
+    for (int k = 0; k < j; ++k) dj -= L[j][k] * L[j][k] * d[k];
+    ok = ok && (dj > 0.0);
+    d[j] = dj;
+    id[j] = 1.0 / dj;
+#pragma unroll
+    for (int i = j + 1; i < 5; ++i) {
+      double a = A[sym5(j, i)];
+#pragma unroll
+      for (int k = 0; k < j; ++k) a -= L[i][k] * L[j][k] * d[k];
+      L[i][j] = a * id[j];
+    }
+  }
+  double z[5];
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    double a = b[i];
+#pragma unroll
+    for (int k = 0; k < i; ++k) a -= L[i][k] * z[k];
+    z[i] = a;
+  }
+#pragma unroll
+  for (int i = 4; i >= 0; --i) {
+    double a = z[i] * id[i];
+#pragma unroll
+    for (int k = i + 1; k < 5; ++k) a -= L[k][i] * x[k];
+    x[i] = a;
+  }
+  return ok;
+}
+
+// 1/CRSS of system q: per voxel from shared memory (stride bs) or uniform
+// from the launch parameters.
+template <bool kTauSmem, typename MS>
+__device__ __forceinline__ double itau_of(const MS* tsm, int bs, const NRParams& p, int q) {
+  if constexpr (kTauSmem)
+    return (double)tsm[q * bs];
+  else
+    return p.icrss[q];
+}
+
+// One pass over the systems: r_s, admissibility, S = sum m gdot r, K = sum n gdot/tau m m^T.
+// snap: set |r| < 1e-10 to 0 (the unconstrained solver does, Solvers.cpp:50-51).
+template <int NEXP, bool kSnap, bool kTauSmem, typename MS>
+__device__ __forceinline__ bool accumulate(const MS* msm, const MS* tsm, int bs,
+                                           const NRParams& p, const double s[5], double S[5],
+                                           double K[15]) {
+  bool adm = true;
+#pragma unroll
+  for (int c = 0; c < 5; ++c) S[c] = 0.0;
+#pragma unroll
+  for (int k = 0; k < 15; ++k) K[k] = 0.0;
+#pragma unroll 2
+  for (int q = 0; q < kNS; ++q) {
+    double m[5];
+    load_m(msm, bs, q, m);
+    const double it = itau_of<kTauSmem>(tsm, bs, p, q);
+    double r = (m[0] * s[0] + m[1] * s[1] + m[2] * s[2] + m[3] * s[3] + m[4] * s[4]) * it;
+    if (kSnap) r = fabs(r) < 1e-10 ? 0.0 : r;
+    adm = adm && !(fabs(r) > p.max_rss);
+    const int n = p.nexp[q];
+    // the constrained solver tests n != 1, the unconstrained n - 1 > 0 (Solvers.cpp:66,177)
+    const bool power = kSnap ? (n - 1 > 0) : (n != 1);
+    const double g = power ? p.gdot[q] * pow_nm1<NEXP>(fabs(r), n) : p.gdot[q];
+    const double gr = g * r;
+    const double w = (double)n * g * it;
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      S[i] += m[i] * gr;
+      const double mw = m[i] * w;
+#pragma unroll
+      for (int j = i; j < 5; ++j) K[sym5(i, j)] += mw * m[j];
+    }
+  }
+  return adm;
+}
+
+// SolveConstrainedConstitutiveEquations (Solvers.cpp:111-222).  ed = Edot + d~.
+// Returns the Newton steps taken; *capped when the iteration budget ran out.
+template <int NEXP, bool kTauSmem, typename MS>
+__device__ __forceinline__ int nr_constrained_smem(const MS* msm, const MS* tsm, int bs,
+                                                   const NRParams& p, const double lam[5],
+                                                   const double ed[5], double s_io[5],
+                                                   double* rel_out, bool* capped) {
+  double cur[5], saved[5], nw[5] = {-1.0, -3.0, -7.0, -9.0, -11.0};
+#pragma unroll
+  for (int c = 0; c < 5; ++c) cur[c] = saved[c] = s_io[c];
+  double rel = 1e5;
+  int remaining = p.max_iter, steps = 0;
+  *capped = false;
+  while (remaining > 0) {
+    double S[5], K[15];
+    // admissibility loop (Solvers.cpp:147-172): back off towards the saved
+    // state while some |r_s| exceeds the cap; every pass costs one iteration
+    for (;;) {
+      const bool adm = accumulate<NEXP, false, kTauSmem>(msm, tsm, bs, p, cur, S, K);
+      if (!adm) {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) cur[c] = saved[c] + (cur[c] - saved[c]) * 0.2;
+      }
+      remaining--;
+      if (remaining < 0) {
+        *capped = true;
+        *rel_out = rel;
+#pragma unroll
+        for (int c = 0; c < 5; ++c) s_io[c] = cur[c];
+        return steps;
+      }
+      if (adm) break;
+    }
+    // y = L0^-1 (cur - lambda) + (S - Edot - d~);  (L0^-1 + K) delta = -y
+    double dl[5], y[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) dl[c] = cur[c] - lam[c];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      double a = S[i] - ed[i];
+#pragma unroll
+      for (int j = 0; j < 5; ++j) a += p.L0inv[sym5(i, j)] * dl[j];
+      y[i] = -a;
+    }
+#pragma unroll
+    for (int k = 0; k < 15; ++k) K[k] += p.L0inv[k];
+    double delta[5];
+    ldlt5_solve(K, y, delta);
+    double dn = 0.0, an = 0.0;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      saved[c] = cur[c];
+      nw[c] = cur[c] + delta[c];
+      const double df = nw[c] - saved[c];
+      const double av = (nw[c] + saved[c]) * 0.5;
+      dn += df * df;
+      an += av * av;
+      cur[c] = nw[c];
+    }
+    rel = sqrt(dn) / sqrt(an);
+    steps++;
+    if (rel < p.eps) break;
+  }
+  *rel_out = rel;
+  *capped = !(rel < p.eps);
+#pragma unroll
+  for (int c = 0; c < 5; ++c) s_io[c] = nw[c];
+  return steps;
+}
+
+// Complete-pivoting fallback of the unconstrained step (singular K).
+static __device__ __noinline__ void solve_neg_K_fullpiv(const double K[15], const double res[5],
+                                                 double delta[5]) {
+  double A[5][5], b[5];
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    b[i] = res[i];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) A[i][j] = -K[sym5(i, j)];
+  }
+  solve5_fullpiv(A, b, delta);
+}
+
+// SolveConstitutiveEquations (Solvers.cpp:19-101): -K delta = R, R = S - Edot.
+template <int NEXP, bool kTauSmem, typename MS>
+__device__ __forceinline__ int nr_unconstrained_smem(const MS* msm, const MS* tsm, int bs,
+                                                     const NRParams& p, const double edot[5],
+                                                     double s_io[5], bool* capped) {
+  double cur[5], nw[5], saved[5];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) {
+    cur[c] = nw[c] = s_io[c];
+    saved[c] = 0.0;
+  }
+  int remaining = p.max_iter, steps = 0;
+  bool conv = false;
+  while (remaining > 0) {
+    double S[5], K[15];
+    for (;;) {
+      const bool adm = accumulate<NEXP, true, kTauSmem>(msm, tsm, bs, p, cur, S, K);
+      if (!adm) {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) cur[c] = saved[c] + (cur[c] - saved[c]) * 0.2;
+      }
+      remaining--;
+      if (remaining < 0) {  // the reference returns NewStressState here (Solvers.cpp:59-60)
+        *capped = true;
+#pragma unroll
+        for (int c = 0; c < 5; ++c) s_io[c] = nw[c];
+        return steps;
+      }
+      if (adm) break;
+    }
+    // J = -K, R = S - Edot:  K delta = -R
+    double res[5], mres[5], delta[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      res[c] = S[c] - edot[c];
+      mres[c] = -res[c];
+    }
+    if (!ldlt5_solve(K, mres, delta)) solve_neg_K_fullpiv(K, res, delta);
+    double dn = 0.0, sn = 0.0;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      saved[c] = cur[c];
+      nw[c] = cur[c] + delta[c];
+      const double sm = nw[c] + cur[c];
+      dn += delta[c] * delta[c];
+      sn += sm * sm;
+      cur[c] = nw[c];
+    }
+    const double rel = 2.0 * sqrt(dn) / sqrt(sn);
+    steps++;
+    if (rel < p.eps) {
+      conv = true;
+      break;
+    }
+  }
+  *capped = !conv;
+#pragma unroll
+  for (int c = 0; c < 5; ++c) s_io[c] = nw[c];
+  return steps;
+}
+
+// GetMaxRSS (MaterialGrid.h:550-566) and the Sachs bound (Solvers.cpp:234-240):
+// max_s |m_s . x| / tau_s
+template <bool kTauSmem, typename MS>
+__device__ __forceinline__ double max_resolved(const MS* msm, const MS* tsm, int bs,
+                                               const NRParams& p, const double x[5]) {
+  double mx = 0.0;
+#pragma unroll 4
+  for (int q = 0; q < kNS; ++q) {
+    double m[5];
+    load_m(msm, bs, q, m);
+    const double a =
+        fabs((m[0] * x[0] + m[1] * x[1] + m[2] * x[2] + m[3] * x[3] + m[4] * x[4]) *
+             itau_of<kTauSmem>(tsm, bs, p, q));
+    mx = (a < mx) ? mx : a;
+  }
+  return mx;
+}
+
+// ApplyConstitutiveEquations (Solvers.cpp:255-274)
+template <int NEXP, bool kTauSmem, typename MS>
+__device__ __forceinline__ void apply_smem(const MS* msm, const MS* tsm, int bs, const NRParams& p,
+                                           const double s[5], double e[5]) {
+#pragma unroll
+  for (int c = 0; c < 5; ++c) e[c] = 0.0;
+#pragma unroll 2
+  for (int q = 0; q < kNS; ++q) {
+    double m[5];
+    load_m(msm, bs, q, m);
+    const double r = (m[0] * s[0] + m[1] * s[1] + m[2] * s[2] + m[3] * s[3] + m[4] * s[4]) *
+                     itau_of<kTauSmem>(tsm, bs, p, q);
+    const int n = p.nexp[q];
+    const double g = n > 0 ? p.gdot[q] * pow_n<NEXP>(fabs(r), n) : p.gdot[q];
+    const double f = g * (double)sgn(r);
+#pragma unroll
+    for (int c = 0; c < 5; ++c) e[c] += m[c] * f;
+  }
+}
+
+}  // namespace vpfft

@@ -1,0 +1,332 @@
+// nr_update.cu -- the Newton-Raphson kernels of the initialisation and of the
+// fixed-point loop (see nr_kernel.cuh for the per-voxel arithmetic), their
+// launchers, and the batched Solvers entry points built on the same code.
+#include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+#include <tuple>
+
+#include "kernel_common.cuh"
+#include "nr_kernel.cuh"
+
+namespace vpfft {
+
+// Shared memory of the NR kernels per thread: 60 Schmid components, plus 12
+// reciprocal CRSS values when the CRSS is per voxel.
+template <typename MS>
+__host__ __device__ constexpr int nr_smem_per_thread(bool tau) {
+  return (60 + (tau ? 12 : 0)) * (int)sizeof(MS);
+}
+// Blocks per SM the NR kernels are compiled for: the FP64 Schmid tile
+// (61 KB per 128-thread block) fits three blocks in an SM's shared memory.
+template <typename MS>
+constexpr int nr_min_blocks() {
+  return sizeof(MS) == 8 ? 3 : 4;
+}
+
+template <bool kTauSmem, typename S, typename MS>
+__device__ __forceinline__ void voxel_schmid(const FieldPtrs<S>& f, long long n, long long v,
+                                             MS* msm, MS* tsm, int bs) {
+  double R[9];
+  load_R(f.R, n, v, R);
+  schmid_to_smem(R, msm, bs);
+  if constexpr (kTauSmem) {
+#pragma unroll
+    for (int q = 0; q < kNS; ++q) tsm[q * bs] = (MS)(1.0 / (double)f.crss[q * n + v]);
+  }
+}
+
+// InitializeComputation (MaterialGrid.cpp:153-210): Sachs guess, scaled to the
+// yield surface when MaxRSS > 1.1, unconstrained NR; lambda = P = sigma.
+// Persistent grid-stride loop over voxels.
+template <typename S, typename MS, int NEXP, bool kTauSmem>
+__global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
+    k_init(const __grid_constant__ NRParams p, const __grid_constant__ FieldPtrs<S> f,
+           IterCtrl* ctrl) {
+  extern __shared__ __align__(16) unsigned char nr_smem[];
+  const int bs = blockDim.x;
+  MS* msm = reinterpret_cast<MS*>(nr_smem) + threadIdx.x;
+  MS* tsm = msm + 60 * bs;
+  const long long n = p.n;
+  unsigned long long capped_count = 0;
+  int status = 0;
+  for (long long v = (long long)blockIdx.x * bs + threadIdx.x; v < n;
+       v += (long long)gridDim.x * bs) {
+    voxel_schmid<kTauSmem>(f, n, v, msm, tsm, bs);
+    const double mxs = max_resolved<kTauSmem>(msm, tsm, bs, p, p.edot);
+    double g[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) g[c] = p.edot[c] / mxs;
+    const double mx = max_resolved<kTauSmem>(msm, tsm, bs, p, g);
+    if (mx > 1.1) {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) g[c] /= mx;
+    }
+    if (mx < 1e-10) status |= kStatusMaxRssTiny;
+    // a zero strain rate makes the Sachs guess 0/0 (Solvers.cpp:241)
+    if (!isfinite(mx)) status |= kStatusNonFinite;
+    bool capped;
+    nr_unconstrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, p.edot, g, &capped);
+    capped_count += capped ? 1 : 0;
+    store5(f.sigma, n, v, g);
+    store5(f.lambda, n, v, g);
+    store5(f.work, n, v, g);
+  }
+  if (status) atomicOr(&ctrl->status, status);
+  if (capped_count) atomicAdd(&ctrl->nr_capped, capped_count);
+}
+
+// The per-voxel body of the fixed-point loop (MaterialGrid.cpp:946-1003):
+//   sigma /= MaxRSS(sigma); sigma = SolveConstrained(...); edot = Apply(sigma);
+//   P = sigma - L0 d~; lambda += L0 (Edot + d~ - edot);
+// and the block partials of sum sigma, sum edot, sum |sigma - lambda|,
+// sum |edot - Edot - d~| (lambda already updated).  `work` holds d~ on entry
+// and P on exit.  Persistent grid-stride loop: every thread solves many voxels
+// and the block reduces once, so the spread of Newton iteration counts between
+// voxels averages out instead of idling warps at a barrier.
+template <typename S, typename MS, int NEXP, bool kTauSmem>
+__global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
+    k_nr_update(const __grid_constant__ NRParams p, const __grid_constant__ FieldPtrs<S> f,
+                double* partials, IterCtrl* ctrl) {
+  if (ctrl->done) return;
+  extern __shared__ __align__(16) unsigned char nr_smem[];
+  const int bs = blockDim.x;
+  MS* msm = reinterpret_cast<MS*>(nr_smem) + threadIdx.x;
+  MS* tsm = msm + 60 * bs;
+  const long long n = p.n;
+  double acc[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) acc[k] = 0.0;
+  unsigned long long capped_count = 0;
+  int status = 0;
+  for (long long v = (long long)blockIdx.x * bs + threadIdx.x; v < n;
+       v += (long long)gridDim.x * bs) {
+    voxel_schmid<kTauSmem>(f, n, v, msm, tsm, bs);
+    double s[5], lam[5], d[5];
+    load5(f.sigma, n, v, s);
+    load5(f.lambda, n, v, lam);
+    load5(f.work, n, v, d);
+    if (f.dkeep) store5(f.dkeep, n, v, d);
+    const double mx = max_resolved<kTauSmem>(msm, tsm, bs, p, s);
+    if (mx < 1e-10) status |= kStatusMaxRssTiny;
+    double ed[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      s[c] /= mx;
+      ed[c] = p.edot[c] + d[c];
+    }
+    double rel;
+    bool capped;
+    nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, lam, ed, s, &rel, &capped);
+    capped_count += capped ? 1 : 0;
+    double e[5];
+    apply_smem<NEXP, kTauSmem>(msm, tsm, bs, p, s, e);
+    double P[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      double ld = 0.0, lt = 0.0;
+#pragma unroll
+      for (int j = 0; j < 5; ++j) {
+        ld += p.L0[j * 5 + i] * d[j];
+        lt += p.L0[j * 5 + i] * (ed[j] - e[j]);
+      }
+      P[i] = s[i] - ld;
+      lam[i] += lt;
+    }
+    store5(f.sigma, n, v, s);
+    store5(f.lambda, n, v, lam);
+    store5(f.work, n, v, P);
+    double es = 0.0, ee = 0.0;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      acc[c] += s[c];
+      acc[5 + c] += e[c];
+      const double ds = s[c] - lam[c];
+      const double de = e[c] - p.edot[c] - d[c];
+      es += ds * ds;
+      ee += de * de;
+    }
+    acc[10] += sqrt(es);
+    acc[11] += sqrt(ee);
+  }
+  if (status) atomicOr(&ctrl->status, status);
+  if (capped_count) atomicAdd(&ctrl->nr_capped, capped_count);
+  block_reduce_store<12, kVoxelBlock>(acc, partials + (long long)blockIdx.x * 12);
+}
+
+
+namespace {
+
+// Blocks of a persistent grid-stride launch: as many as are resident at once.
+int persistent_blocks(const void* kern, size_t smem, long long n) {
+  static std::mutex mu;
+  static std::map<std::tuple<const void*, size_t, int>, int> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int per_sm = 0, sms = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto key = std::make_tuple(kern, smem, dev);
+    auto it = cache.find(key);
+    if (it == cache.end()) {
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kVoxelBlock, smem);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      per_sm = per_sm < 1 ? 1 : per_sm;
+      it = cache.emplace(key, per_sm * sms).first;
+    }
+    per_sm = it->second;
+  }
+  const long long need = (n + kVoxelBlock - 1) / kVoxelBlock;
+  return (int)(need < per_sm ? (need < 1 ? 1 : need) : per_sm);
+}
+
+int uniform_exponent(const NRParams& p) {
+  for (int q = 1; q < kNS; ++q)
+    if (p.nexp[q] != p.nexp[0]) return 0;
+  return (p.nexp[0] == 10 || p.nexp[0] == 20) ? p.nexp[0] : 0;
+}
+
+template <typename S, int NEXP, bool TAU>
+int init_t(const NRParams& p, const FieldPtrs<S>& f, IterCtrl* ctrl, cudaStream_t st) {
+  auto kern = k_init<S, S, NEXP, TAU>;
+  const size_t smem = (size_t)kVoxelBlock * nr_smem_per_thread<S>(TAU);
+  const int nb = persistent_blocks((const void*)kern, smem, p.n);
+  kern<<<nb, kVoxelBlock, smem, st>>>(p, f, ctrl);
+  return 1;
+}
+
+template <typename S, int NEXP, bool TAU>
+int nr_t(const NRParams& p, const FieldPtrs<S>& f, double* partials, IterCtrl* ctrl, double* hist,
+         cudaStream_t st, cudaEvent_t* ev) {
+  auto kern = k_nr_update<S, S, NEXP, TAU>;
+  const size_t smem = (size_t)kVoxelBlock * nr_smem_per_thread<S>(TAU);
+  const int nb = persistent_blocks((const void*)kern, smem, p.n);
+  kern<<<nb, kVoxelBlock, smem, st>>>(p, f, partials, ctrl);
+  if (ev) cudaEventRecord(ev[0], st);
+  k_iter_finish<<<1, kFinishThreads, 0, st>>>(partials, nb, ctrl, hist);
+  if (ev) cudaEventRecord(ev[1], st);
+  return 2;
+}
+
+}  // namespace
+
+template <typename S>
+int launch_init(const NRParams& p, const FieldPtrs<S>& f, IterCtrl* ctrl, cudaStream_t st) {
+  const bool tau = f.crss != nullptr;
+  switch (uniform_exponent(p)) {
+    case 10: return tau ? init_t<S, 10, true>(p, f, ctrl, st) : init_t<S, 10, false>(p, f, ctrl, st);
+    case 20: return tau ? init_t<S, 20, true>(p, f, ctrl, st) : init_t<S, 20, false>(p, f, ctrl, st);
+    default: return tau ? init_t<S, 0, true>(p, f, ctrl, st) : init_t<S, 0, false>(p, f, ctrl, st);
+  }
+}
+
+template <typename S>
+int launch_nr_update(const NRParams& p, const FieldPtrs<S>& f, double* partials, IterCtrl* ctrl,
+                     double* hist, cudaStream_t st, cudaEvent_t* ev) {
+  const bool tau = f.crss != nullptr;
+  switch (uniform_exponent(p)) {
+    case 10:
+      return tau ? nr_t<S, 10, true>(p, f, partials, ctrl, hist, st, ev)
+                 : nr_t<S, 10, false>(p, f, partials, ctrl, hist, st, ev);
+    case 20:
+      return tau ? nr_t<S, 20, true>(p, f, partials, ctrl, hist, st, ev)
+                 : nr_t<S, 20, false>(p, f, partials, ctrl, hist, st, ev);
+    default:
+      return tau ? nr_t<S, 0, true>(p, f, partials, ctrl, hist, st, ev)
+                 : nr_t<S, 0, false>(p, f, partials, ctrl, hist, st, ev);
+  }
+}
+
+template int launch_init<double>(const NRParams&, const FieldPtrs<double>&, IterCtrl*, cudaStream_t);
+template int launch_init<float>(const NRParams&, const FieldPtrs<float>&, IterCtrl*, cudaStream_t);
+template int launch_nr_update<double>(const NRParams&, const FieldPtrs<double>&, double*,
+                                      IterCtrl*, double*, cudaStream_t, cudaEvent_t*);
+template int launch_nr_update<float>(const NRParams&, const FieldPtrs<float>&, double*, IterCtrl*,
+                                     double*, cudaStream_t, cudaEvent_t*);
+
+// ---------------------------------------------------------------- Solvers batch
+// One thread per voxel; the caller's Schmid tensors (n x 12 x 5) and CRSS
+// (n x 12) are staged into the same shared-memory layout the grid kernels use.
+template <bool kConstrained>
+__global__ void __launch_bounds__(kVoxelBlock, 3)
+    k_solvers_nr(const __grid_constant__ NRParams p, int n, const double* s0, const double* schmid,
+                 const double* crss, const double* lambda, const double* dtilde, double* out,
+                 double* nr_err) {
+  extern __shared__ __align__(16) unsigned char nr_smem[];
+  const int bs = blockDim.x;
+  double* msm = reinterpret_cast<double*>(nr_smem) + threadIdx.x;
+  double* tsm = msm + 60 * bs;
+  const int v = blockIdx.x * bs + threadIdx.x;
+  if (v >= n) return;
+  for (int k = 0; k < 60; ++k) msm[k * bs] = schmid[(long long)v * 60 + k];
+  for (int q = 0; q < kNS; ++q) tsm[q * bs] = 1.0 / crss[(long long)v * kNS + q];
+  double s[5];
+  for (int c = 0; c < 5; ++c) s[c] = s0[v * 5 + c];
+  bool capped;
+  if (kConstrained) {
+    double lam[5], ed[5], rel;
+    for (int c = 0; c < 5; ++c) {
+      lam[c] = lambda[v * 5 + c];
+      ed[c] = p.edot[c] + dtilde[v * 5 + c];
+    }
+    nr_constrained_smem<0, true>(msm, tsm, bs, p, lam, ed, s, &rel, &capped);
+    if (nr_err) nr_err[v] = rel;
+  } else {
+    nr_unconstrained_smem<0, true>(msm, tsm, bs, p, p.edot, s, &capped);
+  }
+  for (int c = 0; c < 5; ++c) out[v * 5 + c] = s[c];
+}
+
+static NRParams batch_params(const MaterialParams& mp, const double edot[5], const double* L0,
+                             double eps, double max_rss, int max_iter) {
+  NRParams p{};
+  for (int c = 0; c < 5; ++c) p.edot[c] = edot[c];
+  if (L0) {
+    for (int k = 0; k < 25; ++k) p.L0[k] = L0[k];
+    double inv[25];
+    inverse5_colmajor(L0, inv);
+    for (int i = 0; i < 5; ++i)
+      for (int j = i; j < 5; ++j) p.L0inv[sym5(i, j)] = 0.5 * (inv[j * 5 + i] + inv[i * 5 + j]);
+  }
+  for (int q = 0; q < kNS; ++q) {
+    p.gdot[q] = mp.gdot[q];
+    p.nexp[q] = mp.nexp[q];
+    p.crss[q] = 1.0;
+    p.icrss[q] = 1.0;
+  }
+  p.eps = eps;
+  p.max_rss = max_rss;
+  p.max_iter = max_iter;
+  return p;
+}
+
+int launch_solvers_constrained(int n, const double* s0, const double* schmid, const double* crss,
+                               const MaterialParams& mp, const double edot[5],
+                               const double* lambda, const double* dtilde, const double L0[25],
+                               double eps, double max_rss, int max_iter, double* out,
+                               double* nr_err, cudaStream_t st) {
+  NRParams p = batch_params(mp, edot, L0, eps, max_rss, max_iter);
+  p.n = n;
+  const size_t smem = (size_t)kVoxelBlock * 72 * sizeof(double);
+  cudaFuncSetAttribute(k_solvers_nr<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_solvers_nr<true><<<(n + kVoxelBlock - 1) / kVoxelBlock, kVoxelBlock, smem, st>>>(
+      p, n, s0, schmid, crss, lambda, dtilde, out, nr_err);
+  return 1;
+}
+
+int launch_solvers_unconstrained(int n, const double* s0, const double* schmid,
+                                 const double* crss, const MaterialParams& mp,
+                                 const double edot[5], double eps, double max_rss, int max_iter,
+                                 double* out, cudaStream_t st) {
+  NRParams p = batch_params(mp, edot, nullptr, eps, max_rss, max_iter);
+  p.n = n;
+  const size_t smem = (size_t)kVoxelBlock * 72 * sizeof(double);
+  cudaFuncSetAttribute(k_solvers_nr<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_solvers_nr<false><<<(n + kVoxelBlock - 1) / kVoxelBlock, kVoxelBlock, smem, st>>>(
+      p, n, s0, schmid, crss, nullptr, nullptr, out, nullptr);
+  return 1;
+}
+
+}  // namespace vpfft
