@@ -43,7 +43,8 @@ struct vpfft_grid {
   void* dkeep = nullptr;
   void* crss = nullptr;
   double* acc = nullptr;
-  void* X = nullptr;
+  void* X = nullptr;   // A: spectrum after the z pass
+  void* X2 = nullptr;  // B: spectrum after the y pass
   void* twx = nullptr;
   void* twy = nullptr;
   void* twz = nullptr;
@@ -266,6 +267,7 @@ Spectral<S> spectral(vpfft_grid* g) {
   sp.twy = g->twy;
   sp.twz = g->twz;
   sp.X = g->X;
+  sp.X2 = g->X2;
   return sp;
 }
 
@@ -283,8 +285,8 @@ vpfft_status upload_twiddles(vpfft_grid* g) {
 
 void free_grid_buffers(vpfft_grid* g) {
   void* ptrs[] = {g->R,   g->sigma, g->lambda, g->work,     g->dkeep, g->crss,
-                  g->acc, g->X,     g->twx,    g->twy,      g->twz,   g->partials,
-                  g->sum25, g->ctrl, g->hist, g->staging};
+                  g->acc, g->X,     g->X2,     g->twx,      g->twy,   g->twz,
+                  g->partials, g->sum25, g->ctrl, g->hist, g->staging};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (g->h_ctrl) cudaFreeHost(g->h_ctrl);
@@ -652,6 +654,7 @@ vpfft_status vpfft_grid_create(int nx, int ny, int nz, const vpfft_material* mat
   if (g->keep_d) CKC(cudaMalloc(&g->dkeep, es * n * 5));
   CKC(cudaMalloc(&g->acc, sizeof(double) * n));
   CKC(cudaMalloc(&g->X, 2 * es * 5 * (size_t)nx * ny * g->nh));
+  CKC(cudaMalloc(&g->X2, 2 * es * 5 * (size_t)nx * ny * g->nh));
   const size_t nparts = (size_t)std::max(nr_blocks(g->n), ref_medium_blocks(g->n));
   CKC(cudaMalloc(&g->partials, sizeof(double) * nparts * 25));
   CKC(cudaMalloc(&g->sum25, sizeof(double) * 25));
@@ -1088,29 +1091,57 @@ static vpfft_status fft_impl(int nx, int ny, int nz, int ncomp, const double* in
   make_line_plan(nx, &tmp.px);
   make_line_plan(ny, &tmp.py);
   make_line_plan(nz, &tmp.pz);
+  const int nh = tmp.nh;
   const long long n = (long long)nx * ny * nz;
-  const size_t nspec = (size_t)ncomp * nx * ny * tmp.nh;
+  const size_t nspec = (size_t)ncomp * nx * ny * nh;
   vpfft_status s = upload_twiddles<S>(&tmp);
-  DevBuf X, real, io;
+  DevBuf X, X2, real, io;
   if (s == VPFFT_OK) s = upload(X, nullptr, 2 * sizeof(S) * nspec);
+  if (s == VPFFT_OK) s = upload(X2, nullptr, 2 * sizeof(S) * nspec);
   if (s == VPFFT_OK) s = upload(real, nullptr, sizeof(S) * n * ncomp);
   const size_t in_count = mode == 0 ? (size_t)n * ncomp : 2 * nspec;
   const size_t out_count = mode == 0 ? 2 * nspec : (size_t)n * ncomp;
   if (s == VPFFT_OK) s = upload(io, nullptr, sizeof(double) * std::max(in_count, out_count));
+  // the device keeps the spectrum as B[c][kz][ky][x]; the API uses [c][x][y][kz]
+  auto b_index = [&](size_t c, size_t x, size_t y, size_t k) {
+    return 2 * (((c * nh + k) * ny + y) * nx + x);
+  };
+  auto api_index = [&](size_t c, size_t x, size_t y, size_t k) {
+    return 2 * (((c * nx + x) * ny + y) * nh + k);
+  };
+  std::vector<double> host(std::max(in_count, out_count));
   if (s == VPFFT_OK) {
-    cudaMemcpy(io.p, in, sizeof(double) * in_count, cudaMemcpyHostToDevice);
     Spectral<S> sp = spectral<S>(&tmp);
     sp.X = X.p;
+    sp.X2 = X2.p;
     if (mode == 0) {
+      cudaMemcpy(io.p, in, sizeof(double) * in_count, cudaMemcpyHostToDevice);
       launch_to_soa<S>((double*)io.p, (S*)real.p, (long long)in_count, 1, nullptr);
       launch_fft3d<S>(sp, (S*)real.p, ncomp, 0, nullptr);
-      launch_from_soa<S>((S*)X.p, (double*)io.p, (long long)out_count, 1, nullptr);
+      launch_from_soa<S>((S*)X2.p, (double*)io.p, (long long)out_count, 1, nullptr);
+      s = finish_batch(host.data(), io, sizeof(double) * out_count);
+      if (s == VPFFT_OK)
+        for (int c = 0; c < ncomp; ++c)
+          for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < ny; ++y)
+              for (int k = 0; k < nh; ++k) {
+                out[api_index(c, x, y, k)] = host[b_index(c, x, y, k)];
+                out[api_index(c, x, y, k) + 1] = host[b_index(c, x, y, k) + 1];
+              }
     } else {
-      launch_to_soa<S>((double*)io.p, (S*)X.p, (long long)in_count, 1, nullptr);
+      for (int c = 0; c < ncomp; ++c)
+        for (int x = 0; x < nx; ++x)
+          for (int y = 0; y < ny; ++y)
+            for (int k = 0; k < nh; ++k) {
+              host[b_index(c, x, y, k)] = in[api_index(c, x, y, k)];
+              host[b_index(c, x, y, k) + 1] = in[api_index(c, x, y, k) + 1];
+            }
+      cudaMemcpy(io.p, host.data(), sizeof(double) * in_count, cudaMemcpyHostToDevice);
+      launch_to_soa<S>((double*)io.p, (S*)X2.p, (long long)in_count, 1, nullptr);
       launch_fft3d<S>(sp, (S*)real.p, ncomp, 1, nullptr);
       launch_from_soa<S>((S*)real.p, (double*)io.p, (long long)out_count, 1, nullptr);
+      s = finish_batch(out, io, sizeof(double) * out_count);
     }
-    s = finish_batch(out, io, sizeof(double) * out_count);
   }
   if (tmp.twx) cudaFree(tmp.twx);
   if (tmp.twy) cudaFree(tmp.twy);

@@ -1,0 +1,522 @@
+// fft.cu -- the 3D real <-> half-complex transforms of the fixed-point loop,
+// with the Green operator fused into the x pass.
+//
+// The transform is done as five line passes, each of which reads its lines in
+// contiguous runs of at least 128 bytes and writes them in the layout the next
+// pass reads contiguously (the transpose happens in the shared-memory tile):
+//
+//   W[c][x][y][z]   real field (P before the forward transform, d~ after)
+//   A[c][x][kz][y]  after the z pass (kz in [0, nz/2])
+//   B[c][kz][ky][x] after the y pass; the x pass works in place on B
+//
+//   pass_z_r2c   W -> A   pairs of real z-lines packed as one complex line
+//   pass_y<-1>   A -> B
+//   pass_x_green B -> B   forward x FFT, dhat = -Gbar(k) phat, inverse x FFT
+//   pass_y<+1>   B -> A
+//   pass_z_c2r   A -> W   Hermitian extension, pairs unpacked, times 1/N
+//
+// Inside a tile every line is transformed by a shared-memory Stockham FFT
+// (radices 4, 2, 3, 5).  Line strides in shared memory are padded by one
+// element so that the transposing reads and writes are (nearly) bank-conflict
+// free.  No multicast or cluster features are used.
+#include <cuda_runtime.h>
+
+#include "kernel_common.cuh"
+#include "kernels.h"
+
+namespace vpfft {
+
+namespace {
+
+template <typename R>
+struct CX;
+template <>
+struct CX<float> {
+  using T = float2;
+};
+template <>
+struct CX<double> {
+  using T = double2;
+};
+
+template <typename T>
+__device__ __forceinline__ T add(T a, T b) {
+  return T{a.x + b.x, a.y + b.y};
+}
+template <typename T>
+__device__ __forceinline__ T sub(T a, T b) {
+  return T{a.x - b.x, a.y - b.y};
+}
+template <typename T, typename R>
+__device__ __forceinline__ T scl(T a, R s) {
+  return T{a.x * s, a.y * s};
+}
+template <int SIGN, typename T>
+__device__ __forceinline__ T tw_mul(T v, T w) {
+  if (SIGN < 0) return T{v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x};
+  return T{v.x * w.x + v.y * w.y, v.y * w.x - v.x * w.y};
+}
+template <int SIGN, typename T>
+__device__ __forceinline__ T mul_si(T z) {
+  if (SIGN < 0) return T{z.y, -z.x};
+  return T{-z.y, z.x};
+}
+
+// Stockham autosort FFT of nlines lines (line stride ls) of length pl.n in
+// shared memory; a and b are ping-pong buffers, the result buffer is returned.
+template <int SIGN, typename T>
+__device__ T* line_fft(T* a, T* b, const T* tw, const LinePlan& pl, int nlines, int ls) {
+  using R = decltype(T{}.x);
+  const int n = pl.n;
+  int Ns = 1;
+  for (int st = 0; st < pl.nrad; ++st) {
+    const int Rr = pl.rad[st];
+    const int nb = n / Rr;
+    const int total = nb * nlines;
+    const int tws = n / (Ns * Rr);
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+      const int line = t / nb;
+      const int j = t - line * nb;
+      const T* in = a + line * ls;
+      T* out = b + line * ls;
+      const int jm = j % Ns;
+      const int e = jm * tws;
+      const int od = (j - jm) * Rr + jm;
+      if (Rr == 4) {
+        T v0 = in[j], v1 = in[j + nb], v2 = in[j + 2 * nb], v3 = in[j + 3 * nb];
+        if (e) {
+          v1 = tw_mul<SIGN>(v1, tw[e]);
+          v2 = tw_mul<SIGN>(v2, tw[2 * e]);
+          v3 = tw_mul<SIGN>(v3, tw[3 * e]);
+        }
+        const T u0 = add(v0, v2), u1 = sub(v0, v2), u2 = add(v1, v3);
+        const T u3 = mul_si<SIGN>(sub(v1, v3));
+        out[od] = add(u0, u2);
+        out[od + Ns] = add(u1, u3);
+        out[od + 2 * Ns] = sub(u0, u2);
+        out[od + 3 * Ns] = sub(u1, u3);
+      } else if (Rr == 2) {
+        T v0 = in[j], v1 = in[j + nb];
+        if (e) v1 = tw_mul<SIGN>(v1, tw[e]);
+        out[od] = add(v0, v1);
+        out[od + Ns] = sub(v0, v1);
+      } else if (Rr == 3) {
+        T v0 = in[j], v1 = in[j + nb], v2 = in[j + 2 * nb];
+        if (e) {
+          v1 = tw_mul<SIGN>(v1, tw[e]);
+          v2 = tw_mul<SIGN>(v2, tw[2 * e]);
+        }
+        const T t1 = add(v1, v2);
+        const T t2 = sub(v0, scl(t1, R(0.5)));
+        const T t3 = mul_si<SIGN>(scl(sub(v1, v2), R(0.86602540378443864676)));
+        out[od] = add(v0, t1);
+        out[od + Ns] = add(t2, t3);
+        out[od + 2 * Ns] = sub(t2, t3);
+      } else {  // 5
+        T v0 = in[j], v1 = in[j + nb], v2 = in[j + 2 * nb], v3 = in[j + 3 * nb],
+          v4 = in[j + 4 * nb];
+        if (e) {
+          v1 = tw_mul<SIGN>(v1, tw[e]);
+          v2 = tw_mul<SIGN>(v2, tw[2 * e]);
+          v3 = tw_mul<SIGN>(v3, tw[3 * e]);
+          v4 = tw_mul<SIGN>(v4, tw[4 * e]);
+        }
+        const R c1 = R(0.30901699437494742410), c2 = R(-0.80901699437494742410);
+        const R s1 = R(0.95105651629515357212), s2 = R(0.58778525229247312917);
+        const T a1 = add(v1, v4), a2 = add(v2, v3), b1 = sub(v1, v4), b2 = sub(v2, v3);
+        const T p1 = add(v0, add(scl(a1, c1), scl(a2, c2)));
+        const T p2 = add(v0, add(scl(a1, c2), scl(a2, c1)));
+        const T q1 = mul_si<SIGN>(add(scl(b1, s1), scl(b2, s2)));
+        const T q2 = mul_si<SIGN>(sub(scl(b1, s2), scl(b2, s1)));
+        out[od] = add(v0, add(a1, a2));
+        out[od + Ns] = add(p1, q1);
+        out[od + 4 * Ns] = sub(p1, q1);
+        out[od + 2 * Ns] = add(p2, q2);
+        out[od + 3 * Ns] = sub(p2, q2);
+      }
+    }
+    __syncthreads();
+    T* tmp = a;
+    a = b;
+    b = tmp;
+    Ns *= Rr;
+  }
+  return a;
+}
+
+template <typename T>
+__device__ __forceinline__ void load_twiddles(T* tw, const T* twg, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = twg[i];
+}
+
+// Copy of nrows rows of len elements: warp w takes rows w, w + nwarps, ...;
+// lanes stride 32 along the row with kU independent loads in flight per lane
+// before the matching stores (global rows are contiguous: one coalesced
+// request per 32 elements, and enough bytes in flight to cover DRAM latency).
+constexpr int kU = 8;
+template <typename V, typename G, typename P>
+__device__ __forceinline__ void copy_rows(int nrows, int len, G get, P put) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int row = warp; row < nrows; row += nw) {
+    for (int c0 = lane; c0 < len; c0 += 32 * kU) {
+      V v[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int c = c0 + 32 * u;
+        if (c < len) v[u] = get(row, c);
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int c = c0 + 32 * u;
+        if (c < len) put(row, c, v[u]);
+      }
+    }
+  }
+}
+
+// Copy of a tile whose contiguous global rows are only W (compile-time)
+// elements long: element i is (row i / W, column i % W); kU loads in flight.
+template <int W, typename V, typename G, typename P>
+__device__ __forceinline__ void copy_short_rows(int nrows, G get, P put) {
+  const int total = nrows * W, bd = blockDim.x;
+  for (int base = threadIdx.x; base < total; base += kU * bd) {
+    V v[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const int i = base + u * bd;
+      if (i < total) v[u] = get(i / W, i % W);
+    }
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const int i = base + u * bd;
+      if (i < total) put(i / W, i % W, v[u]);
+    }
+  }
+}
+
+}  // namespace
+
+// Tile sizes: lines per block chosen so that global rows are >= 128 bytes.
+template <typename R>
+struct FftTiles {
+  static constexpr int kZ = 16;                        // real z-lines (y tile) per block
+  static constexpr int kY = sizeof(R) == 4 ? 16 : 8;   // y-lines (x tile) per block
+  static constexpr int kX = sizeof(R) == 4 ? 4 : 2;    // ky tile of the x pass (x 5 components)
+};
+constexpr int kFftThreads = 256;
+
+// ---------------------------------------------------------------- z, forward
+template <typename S>
+__global__ void __launch_bounds__(kFftThreads)
+    k_pass_z_r2c(const S* __restrict__ W, typename CX<S>::T* __restrict__ A, LinePlan pl,
+                 const typename CX<S>::T* __restrict__ twg, int nx, int ny, int nh,
+                 const IterCtrl* ctrl) {
+  using T = typename CX<S>::T;
+  if (ctrl && ctrl->done) return;
+  constexpr int TY = FftTiles<S>::kZ;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int nz = pl.n, ls = nz + 1;
+  T* tw = reinterpret_cast<T*>(smraw);
+  T* a = tw + nz;
+  T* b = a + (TY / 2) * ls;
+  load_twiddles(tw, twg, nz);
+  const int y0 = blockIdx.x * TY, x = blockIdx.y, c = blockIdx.z;
+  const int ty = min(TY, ny - y0);
+  const int npair = (ty + 1) / 2;
+  const S* src = W + ((long long)(c * nx + x) * ny + y0) * nz;
+  copy_rows<S>(
+      2 * npair, nz,
+      [&](int l, int z) { return l < ty ? src[(long long)l * nz + z] : S(0); },
+      [&](int l, int z, S v) { reinterpret_cast<S*>(&a[(l >> 1) * ls + z])[l & 1] = v; });
+  __syncthreads();
+  const T* r = line_fft<-1>(a, b, tw, pl, npair, ls);
+  T* dst = A + ((long long)(c * nx + x) * nh) * ny + y0;
+  copy_short_rows<TY, T>(
+      nh,
+      [&](int k, int l) {
+        const int p = l >> 1;
+        const T Z = r[p * ls + k];
+        const T Zm = r[p * ls + (k == 0 ? 0 : nz - k)];
+        T o;
+        if ((l & 1) == 0) {  // (Z + conj(Zm)) / 2
+          o.x = (Z.x + Zm.x) * S(0.5);
+          o.y = (Z.y - Zm.y) * S(0.5);
+        } else {             // (Z - conj(Zm)) / (2i)
+          o.x = (Z.y + Zm.y) * S(0.5);
+          o.y = (Zm.x - Z.x) * S(0.5);
+        }
+        return o;
+      },
+      [&](int k, int l, T v) {
+        if (l < ty) dst[(long long)k * ny + l] = v;
+      });
+}
+
+// ---------------------------------------------------------------- z, inverse
+template <typename S>
+__global__ void __launch_bounds__(kFftThreads)
+    k_pass_z_c2r(const typename CX<S>::T* __restrict__ A, S* __restrict__ W, LinePlan pl,
+                 const typename CX<S>::T* __restrict__ twg, int nx, int ny, int nh, S scale,
+                 const IterCtrl* ctrl) {
+  using T = typename CX<S>::T;
+  if (ctrl && ctrl->done) return;
+  constexpr int TY = FftTiles<S>::kZ;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int nz = pl.n, ls = nz + 1;
+  // a: (TY/2) packed lines; b: the tile's half spectra first (TY x (nh+1)),
+  // then the FFT's ping-pong buffer -- sized max of the two (see pass_smem)
+  T* tw = reinterpret_cast<T*>(smraw);
+  T* a = tw + nz;
+  T* b = a + (TY / 2) * ls;
+  load_twiddles(tw, twg, nz);
+  const int y0 = blockIdx.x * TY, x = blockIdx.y, c = blockIdx.z;
+  const int ty = min(TY, ny - y0);
+  const int npair = (ty + 1) / 2;
+  // half spectra of the tile into b: h[l][k]
+  const T* src = A + ((long long)(c * nx + x) * nh) * ny + y0;
+  const int hs = nh + 1;
+  copy_short_rows<TY, T>(
+      nh, [&](int k, int l) { return l < ty ? src[(long long)k * ny + l] : T{S(0), S(0)}; },
+      [&](int k, int l, T v) { b[l * hs + k] = v; });
+  __syncthreads();
+  // packed full lines: Z = A_even + i A_odd, Hermitian extension for k >= nh
+  for (int i = threadIdx.x; i < npair * nz; i += blockDim.x) {
+    const int p = i / nz, k = i - p * nz;
+    const bool cj = k >= nh;
+    const int kk = cj ? nz - k : k;
+    T Ae = b[(2 * p) * hs + kk];
+    T Ao = b[(2 * p + 1) * hs + kk];
+    if (cj) {
+      Ae.y = -Ae.y;
+      Ao.y = -Ao.y;
+    }
+    if (k == 0 || ((nz & 1) == 0 && k == nz / 2)) {
+      Ae.y = S(0);
+      Ao.y = S(0);
+    }
+    a[p * ls + k] = T{Ae.x - Ao.y, Ae.y + Ao.x};
+  }
+  __syncthreads();
+  const T* r = line_fft<1>(a, b, tw, pl, npair, ls);
+  S* dst = W + ((long long)(c * nx + x) * ny + y0) * nz;
+  copy_rows<S>(
+      ty, nz,
+      [&](int l, int z) {
+        const T Z = r[(l >> 1) * ls + z];
+        return ((l & 1) ? Z.y : Z.x) * scale;
+      },
+      [&](int l, int z, S v) { dst[(long long)l * nz + z] = v; });
+}
+
+// ---------------------------------------------------------------- y passes
+// Forward: A[c][x][kz][y] -> B[c][kz][ky][x]; inverse: B -> A.
+template <int SIGN, typename R>
+__global__ void __launch_bounds__(kFftThreads)
+    k_pass_y(const typename CX<R>::T* __restrict__ in, typename CX<R>::T* __restrict__ out,
+             LinePlan pl, const typename CX<R>::T* __restrict__ twg, int nx, int nh,
+             const IterCtrl* ctrl) {
+  using T = typename CX<R>::T;
+  if (ctrl && ctrl->done) return;
+  constexpr int TX = FftTiles<R>::kY;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int ny = pl.n, ls = ny + 1;
+  T* tw = reinterpret_cast<T*>(smraw);
+  T* a = tw + ny;
+  T* b = a + TX * ls;
+  load_twiddles(tw, twg, ny);
+  const int x0 = blockIdx.x * TX, kz = blockIdx.y, c = blockIdx.z;
+  const int tx = min(TX, nx - x0);
+  // A line (c, x, kz) starts at ((c*nx + x)*nh + kz)*ny; B row (c, kz, ky) at ((c*nh + kz)*ny + ky)*nx
+  const long long a_base = ((long long)(c * nx + x0) * nh + kz) * ny;
+  const long long a_xs = (long long)nh * ny;
+  const long long b_base = ((long long)(c * nh + kz) * ny) * nx + x0;
+  if (SIGN < 0) {
+    copy_rows<T>(
+        TX, ny, [&](int xl, int y) { return xl < tx ? in[a_base + xl * a_xs + y] : T{R(0), R(0)}; },
+        [&](int xl, int y, T v) { a[xl * ls + y] = v; });
+  } else {
+    copy_short_rows<TX, T>(
+        ny, [&](int y, int xl) { return xl < tx ? in[b_base + (long long)y * nx + xl] : T{R(0), R(0)}; },
+        [&](int y, int xl, T v) { a[xl * ls + y] = v; });
+  }
+  __syncthreads();
+  const T* r = line_fft<SIGN>(a, b, tw, pl, TX, ls);
+  if (SIGN < 0) {
+    copy_short_rows<TX, T>(
+        ny, [&](int y, int xl) { return r[xl * ls + y]; },
+        [&](int y, int xl, T v) {
+          if (xl < tx) out[b_base + (long long)y * nx + xl] = v;
+        });
+  } else {
+    copy_rows<T>(
+        tx, ny, [&](int xl, int y) { return r[xl * ls + y]; },
+        [&](int xl, int y, T v) { out[a_base + xl * a_xs + y] = v; });
+  }
+}
+
+// ---------------------------------------------------------------- x pass
+// In place on B[c][kz][ky][x]: MODE 0 forward, 1 inverse, 2 forward + Green + inverse.
+template <int MODE, typename R>
+__global__ void __launch_bounds__(kFftThreads, 2)
+    k_pass_x(typename CX<R>::T* __restrict__ B, LinePlan pl,
+             const typename CX<R>::T* __restrict__ twg, GreenParams<R> gp, int ny, int nh,
+             int ncomp, const IterCtrl* ctrl) {
+  using T = typename CX<R>::T;
+  if (ctrl && ctrl->done) return;
+  constexpr int TK = FftTiles<R>::kX;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int nx = pl.n, ls = nx + 1;
+  T* tw = reinterpret_cast<T*>(smraw);
+  T* a = tw + nx;
+  T* b = a + ncomp * TK * ls;
+  load_twiddles(tw, twg, nx);
+  const int ky0 = blockIdx.x * TK, kz = blockIdx.y;
+  const int tk = min(TK, ny - ky0);
+  const long long cs = (long long)nh * ny * nx;  // component stride
+  const long long base = ((long long)kz * ny + ky0) * nx;
+  const int nl = ncomp * TK;
+  copy_rows<T>(
+      nl, nx,
+      [&](int L, int xx) {
+        const int c = L / TK, kl = L - c * TK;
+        return kl < tk ? B[c * cs + base + (long long)kl * nx + xx] : T{R(0), R(0)};
+      },
+      [&](int L, int xx, T v) { a[L * ls + xx] = v; });
+  __syncthreads();
+  T* r = a;
+  T* o = b;
+  if (MODE != 1) {
+    r = line_fft<-1>(a, b, tw, pl, nl, ls);
+    o = (r == a) ? b : a;
+  }
+  if (MODE == 2) {
+    for (int i = threadIdx.x; i < TK * nx; i += blockDim.x) {
+      const int kl = i / nx, xx = i - kl * nx;
+      if (kl >= tk) continue;
+      R pre[5], pim[5];
+#pragma unroll
+      for (int c = 0; c < 5; ++c) {
+        const T z = r[(c * TK + kl) * ls + xx];
+        pre[c] = z.x;
+        pim[c] = z.y;
+      }
+      green_apply<R>(gp, xx, ky0 + kl, kz, pre, pim);
+#pragma unroll
+      for (int c = 0; c < 5; ++c) r[(c * TK + kl) * ls + xx] = T{pre[c], pim[c]};
+    }
+    __syncthreads();
+  }
+  if (MODE != 0) r = line_fft<1>(r, o, tw, pl, nl, ls);
+  copy_rows<T>(
+      nl, nx, [&](int L, int xx) { return r[L * ls + xx]; },
+      [&](int L, int xx, T v) {
+        const int c = L / TK, kl = L - c * TK;
+        if (kl < tk) B[c * cs + base + (long long)kl * nx + xx] = v;
+      });
+}
+
+// ---------------------------------------------------------------- launchers
+namespace {
+template <typename R>
+struct PassSmem {
+  size_t z_r2c, z_c2r, y, x;
+};
+template <typename R>
+PassSmem<R> pass_smem(const Spectral<R>& sp, int ncomp) {
+  using T = typename CX<R>::T;
+  PassSmem<R> s;
+  const int TY = FftTiles<R>::kZ, TX = FftTiles<R>::kY, TK = FftTiles<R>::kX;
+  const int lz = sp.nz + 1;
+  s.z_r2c = sizeof(T) * (sp.nz + 2 * (size_t)(TY / 2) * lz);
+  const size_t bsz = std::max((size_t)(TY / 2) * lz, (size_t)TY * (sp.nh + 1));
+  s.z_c2r = sizeof(T) * (sp.nz + (size_t)(TY / 2) * lz + bsz);
+  s.y = sizeof(T) * (sp.ny + 2 * (size_t)TX * (sp.ny + 1));
+  s.x = sizeof(T) * (sp.nx + 2 * (size_t)ncomp * TK * (sp.nx + 1));
+  return s;
+}
+template <typename R>
+void pass_optin() {
+  static bool done = false;  // attributes are per function and device-independent here
+  if (done) return;
+  const int s = 227 * 1024;
+  cudaFuncSetAttribute(k_pass_z_r2c<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  cudaFuncSetAttribute(k_pass_z_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  cudaFuncSetAttribute(k_pass_y<-1, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  cudaFuncSetAttribute(k_pass_y<1, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  cudaFuncSetAttribute(k_pass_x<0, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  cudaFuncSetAttribute(k_pass_x<1, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  cudaFuncSetAttribute(k_pass_x<2, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  done = true;
+}
+}  // namespace
+
+template <typename S>
+int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S* work,
+                              const IterCtrl* ctrl, cudaStream_t st, int ncomp,
+                              cudaEvent_t* ev) {
+  using T = typename CX<S>::T;
+  pass_optin<S>();
+  const PassSmem<S> sm = pass_smem(sp, ncomp);
+  T* A = reinterpret_cast<T*>(sp.X);
+  T* B = reinterpret_cast<T*>(sp.X2);
+  const T* twx = reinterpret_cast<const T*>(sp.twx);
+  const T* twy = reinterpret_cast<const T*>(sp.twy);
+  const T* twz = reinterpret_cast<const T*>(sp.twz);
+  const dim3 gz((sp.ny + FftTiles<S>::kZ - 1) / FftTiles<S>::kZ, sp.nx, ncomp);
+  const dim3 gy((sp.nx + FftTiles<S>::kY - 1) / FftTiles<S>::kY, sp.nh, ncomp);
+  const dim3 gx((sp.ny + FftTiles<S>::kX - 1) / FftTiles<S>::kX, sp.nh);
+  if (ev) cudaEventRecord(ev[0], st);
+  k_pass_z_r2c<S><<<gz, kFftThreads, sm.z_r2c, st>>>(work, A, sp.pz, twz, sp.nx, sp.ny, sp.nh, ctrl);
+  if (ev) cudaEventRecord(ev[1], st);
+  k_pass_y<-1, S><<<gy, kFftThreads, sm.y, st>>>(A, B, sp.py, twy, sp.nx, sp.nh, ctrl);
+  if (ev) cudaEventRecord(ev[2], st);
+  k_pass_x<2, S><<<gx, kFftThreads, sm.x, st>>>(B, sp.px, twx, gp, sp.ny, sp.nh, ncomp, ctrl);
+  if (ev) cudaEventRecord(ev[3], st);
+  k_pass_y<1, S><<<gy, kFftThreads, sm.y, st>>>(B, A, sp.py, twy, sp.nx, sp.nh, ctrl);
+  if (ev) cudaEventRecord(ev[4], st);
+  const S scale = S(1.0 / ((double)sp.nx * sp.ny * sp.nz));
+  k_pass_z_c2r<S><<<gz, kFftThreads, sm.z_c2r, st>>>(A, work, sp.pz, twz, sp.nx, sp.ny, sp.nh,
+                                                     scale, ctrl);
+  if (ev) cudaEventRecord(ev[5], st);
+  return 5;
+}
+
+template <typename S>
+int launch_fft3d(const Spectral<S>& sp, S* real, int ncomp, int mode, cudaStream_t st) {
+  using T = typename CX<S>::T;
+  pass_optin<S>();
+  const PassSmem<S> sm = pass_smem(sp, ncomp);
+  T* A = reinterpret_cast<T*>(sp.X);
+  T* B = reinterpret_cast<T*>(sp.X2);
+  const T* twx = reinterpret_cast<const T*>(sp.twx);
+  const T* twy = reinterpret_cast<const T*>(sp.twy);
+  const T* twz = reinterpret_cast<const T*>(sp.twz);
+  const dim3 gz((sp.ny + FftTiles<S>::kZ - 1) / FftTiles<S>::kZ, sp.nx, ncomp);
+  const dim3 gy((sp.nx + FftTiles<S>::kY - 1) / FftTiles<S>::kY, sp.nh, ncomp);
+  const dim3 gx((sp.ny + FftTiles<S>::kX - 1) / FftTiles<S>::kX, sp.nh);
+  GreenParams<S> gp{};
+  if (mode == 0) {
+    k_pass_z_r2c<S><<<gz, kFftThreads, sm.z_r2c, st>>>(real, A, sp.pz, twz, sp.nx, sp.ny, sp.nh,
+                                                       nullptr);
+    k_pass_y<-1, S><<<gy, kFftThreads, sm.y, st>>>(A, B, sp.py, twy, sp.nx, sp.nh, nullptr);
+    k_pass_x<0, S><<<gx, kFftThreads, sm.x, st>>>(B, sp.px, twx, gp, sp.ny, sp.nh, ncomp, nullptr);
+  } else {
+    k_pass_x<1, S><<<gx, kFftThreads, sm.x, st>>>(B, sp.px, twx, gp, sp.ny, sp.nh, ncomp, nullptr);
+    k_pass_y<1, S><<<gy, kFftThreads, sm.y, st>>>(B, A, sp.py, twy, sp.nx, sp.nh, nullptr);
+    const S scale = S(1.0 / ((double)sp.nx * sp.ny * sp.nz));
+    k_pass_z_c2r<S><<<gz, kFftThreads, sm.z_c2r, st>>>(A, real, sp.pz, twz, sp.nx, sp.ny, sp.nh,
+                                                       scale, nullptr);
+  }
+  return 3;
+}
+
+template int launch_spectral_iteration<double>(const Spectral<double>&, const GreenParams<double>&,
+                                               double*, const IterCtrl*, cudaStream_t, int,
+                                               cudaEvent_t*);
+template int launch_spectral_iteration<float>(const Spectral<float>&, const GreenParams<float>&,
+                                              float*, const IterCtrl*, cudaStream_t, int,
+                                              cudaEvent_t*);
+template int launch_fft3d<double>(const Spectral<double>&, double*, int, int, cudaStream_t);
+template int launch_fft3d<float>(const Spectral<float>&, float*, int, int, cudaStream_t);
+
+}  // namespace vpfft

@@ -23,128 +23,8 @@
 
 namespace vpfft {
 
-// ============================================================== helpers
-template <typename R>
-struct CT;
-template <>
-struct CT<float> {
-  using T = float2;
-};
-template <>
-struct CT<double> {
-  using T = double2;
-};
-
-template <typename T>
-__device__ __forceinline__ T cadd(T a, T b) {
-  return T{a.x + b.x, a.y + b.y};
-}
-template <typename T>
-__device__ __forceinline__ T csub(T a, T b) {
-  return T{a.x - b.x, a.y - b.y};
-}
-template <typename T, typename R>
-__device__ __forceinline__ T cscale(T a, R s) {
-  return T{a.x * s, a.y * s};
-}
-// v * w (SIGN < 0) or v * conj(w) (SIGN > 0); w = exp(-2 pi i e / n)
-template <int SIGN, typename T>
-__device__ __forceinline__ T twmul(T v, T w) {
-  if (SIGN < 0) return T{v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x};
-  return T{v.x * w.x + v.y * w.y, v.y * w.x - v.x * w.y};
-}
-// (SIGN * i) * z
-template <int SIGN, typename T>
-__device__ __forceinline__ T mul_si(T z) {
-  if (SIGN < 0) return T{z.y, -z.x};
-  return T{-z.y, z.x};
-}
-
-// Stockham autosort FFT of `nlines` lines of length pl.n held in shared
-// memory (line stride `stride`), ping-ponging between a and b; returns the
-// buffer holding the result in natural order.  Stage with radix R after
-// radices of product Ns: butterfly j takes in[j + r n/R] * W^(r (j mod Ns) n/(Ns R))
-// and writes out[(j - j mod Ns) R + j mod Ns + r Ns].
-template <int SIGN, typename T>
-__device__ T* stockham(T* a, T* b, const T* tw, const LinePlan& pl, int nlines, int stride) {
-  using R = decltype(T{}.x);
-  const int n = pl.n;
-  int Ns = 1;
-  for (int st = 0; st < pl.nrad; ++st) {
-    const int Rr = pl.rad[st];
-    const int nb = n / Rr;
-    const int total = nb * nlines;
-    const int tws = n / (Ns * Rr);
-    for (int t = threadIdx.x; t < total; t += blockDim.x) {
-      const int line = t / nb;
-      const int j = t - line * nb;
-      const T* in = a + line * stride;
-      T* out = b + line * stride;
-      const int jm = j % Ns;
-      const int e = jm * tws;
-      const int od = (j - jm) * Rr + jm;
-      if (Rr == 4) {
-        T v0 = in[j], v1 = in[j + nb], v2 = in[j + 2 * nb], v3 = in[j + 3 * nb];
-        if (e) {
-          v1 = twmul<SIGN>(v1, tw[e]);
-          v2 = twmul<SIGN>(v2, tw[2 * e]);
-          v3 = twmul<SIGN>(v3, tw[3 * e]);
-        }
-        const T u0 = cadd(v0, v2), u1 = csub(v0, v2), u2 = cadd(v1, v3);
-        const T u3 = mul_si<SIGN>(csub(v1, v3));
-        out[od] = cadd(u0, u2);
-        out[od + Ns] = cadd(u1, u3);
-        out[od + 2 * Ns] = csub(u0, u2);
-        out[od + 3 * Ns] = csub(u1, u3);
-      } else if (Rr == 2) {
-        T v0 = in[j], v1 = in[j + nb];
-        if (e) v1 = twmul<SIGN>(v1, tw[e]);
-        out[od] = cadd(v0, v1);
-        out[od + Ns] = csub(v0, v1);
-      } else if (Rr == 3) {
-        T v0 = in[j], v1 = in[j + nb], v2 = in[j + 2 * nb];
-        if (e) {
-          v1 = twmul<SIGN>(v1, tw[e]);
-          v2 = twmul<SIGN>(v2, tw[2 * e]);
-        }
-        const T t1 = cadd(v1, v2);
-        const T t2 = csub(v0, cscale(t1, R(0.5)));
-        const T t3 = mul_si<SIGN>(cscale(csub(v1, v2), R(0.86602540378443864676)));
-        out[od] = cadd(v0, t1);
-        out[od + Ns] = cadd(t2, t3);
-        out[od + 2 * Ns] = csub(t2, t3);
-      } else {  // radix 5
-        T v0 = in[j], v1 = in[j + nb], v2 = in[j + 2 * nb], v3 = in[j + 3 * nb],
-          v4 = in[j + 4 * nb];
-        if (e) {
-          v1 = twmul<SIGN>(v1, tw[e]);
-          v2 = twmul<SIGN>(v2, tw[2 * e]);
-          v3 = twmul<SIGN>(v3, tw[3 * e]);
-          v4 = twmul<SIGN>(v4, tw[4 * e]);
-        }
-        const R c1 = R(0.30901699437494742410), c2 = R(-0.80901699437494742410);
-        const R s1 = R(0.95105651629515357212), s2 = R(0.58778525229247312917);
-        const T a1 = cadd(v1, v4), a2 = cadd(v2, v3), b1 = csub(v1, v4), b2 = csub(v2, v3);
-        const T p1 = cadd(v0, cadd(cscale(a1, c1), cscale(a2, c2)));
-        const T p2 = cadd(v0, cadd(cscale(a1, c2), cscale(a2, c1)));
-        const T q1 = mul_si<SIGN>(cadd(cscale(b1, s1), cscale(b2, s2)));
-        const T q2 = mul_si<SIGN>(csub(cscale(b1, s2), cscale(b2, s1)));
-        out[od] = cadd(v0, cadd(a1, a2));
-        out[od + Ns] = cadd(p1, q1);
-        out[od + 4 * Ns] = csub(p1, q1);
-        out[od + 2 * Ns] = cadd(p2, q2);
-        out[od + 3 * Ns] = csub(p2, q2);
-      }
-    }
-    __syncthreads();
-    T* tmp = a;
-    a = b;
-    b = tmp;
-    Ns *= Rr;
-  }
-  return a;
-}
-
+// ============================================================== line plans
+// Radix-4 stages first, then 2, 3 and 5; returns false for other prime factors.
 bool make_line_plan(int n, LinePlan* p) {
   if (n < 1) return false;
   p->n = n;
@@ -478,289 +358,6 @@ int launch_crss_broadcast(S* dst, long long n, const double crss[kNS], cudaStrea
   return 1;
 }
 
-// ============================================================== spectral phase
-// Shared-memory budget per block for the line FFTs (dynamic, opted in).
-constexpr size_t kSmemBudget = 96 * 1024;
-
-// z: real lines of length nz, two packed per complex line.
-template <typename S>
-__global__ void __launch_bounds__(256) k_fft_z_r2c(const S* __restrict__ work,
-                                                   typename CT<S>::T* __restrict__ X, LinePlan pl,
-                                                   const typename CT<S>::T* __restrict__ twg,
-                                                   long long nlines, int nh, int ppb,
-                                                   const IterCtrl* ctrl) {
-  using T = typename CT<S>::T;
-  if (ctrl && ctrl->done) return;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  const int n = pl.n;
-  T* tw = reinterpret_cast<T*>(smraw);
-  T* a = tw + n;
-  T* b = a + ppb * n;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = twg[i];
-  const long long l0 = (long long)blockIdx.x * 2 * ppb;
-  for (int i = threadIdx.x; i < 2 * ppb * n; i += blockDim.x) {
-    const int l = i / n, z = i - l * n;
-    const long long g = l0 + l;
-    const S v = g < nlines ? work[g * n + z] : S(0);
-    S* dst = reinterpret_cast<S*>(&a[(l >> 1) * n + z]);
-    dst[l & 1] = v;
-  }
-  __syncthreads();
-  T* r = stockham<-1>(a, b, tw, pl, ppb, n);
-  for (int i = threadIdx.x; i < 2 * ppb * nh; i += blockDim.x) {
-    const int l = i / nh, k = i - l * nh;
-    const long long g = l0 + l;
-    if (g >= nlines) continue;
-    const int pr = l >> 1;
-    const T Z = r[pr * n + k];
-    const T Zm = r[pr * n + (k == 0 ? 0 : n - k)];
-    T o;
-    if ((l & 1) == 0) {  // (Z + conj(Zm)) / 2
-      o.x = (Z.x + Zm.x) * S(0.5);
-      o.y = (Z.y - Zm.y) * S(0.5);
-    } else {             // (Z - conj(Zm)) / (2i)
-      o.x = (Z.y + Zm.y) * S(0.5);
-      o.y = (Zm.x - Z.x) * S(0.5);
-    }
-    X[g * nh + k] = o;
-  }
-}
-
-template <typename S>
-__global__ void __launch_bounds__(256) k_fft_z_c2r(const typename CT<S>::T* __restrict__ X,
-                                                   S* __restrict__ work, LinePlan pl,
-                                                   const typename CT<S>::T* __restrict__ twg,
-                                                   long long nlines, int nh, int ppb, S scale,
-                                                   const IterCtrl* ctrl) {
-  using T = typename CT<S>::T;
-  if (ctrl && ctrl->done) return;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  const int n = pl.n;
-  T* tw = reinterpret_cast<T*>(smraw);
-  T* a = tw + n;
-  T* b = a + ppb * n;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = twg[i];
-  const long long l0 = (long long)blockIdx.x * 2 * ppb;
-  for (int i = threadIdx.x; i < ppb * n; i += blockDim.x) {
-    const int pr = i / n, k = i - pr * n;
-    const long long ga = l0 + 2 * pr, gb = ga + 1;
-    const bool cj = k >= nh;
-    const int kk = cj ? n - k : k;
-    T A = ga < nlines ? X[ga * nh + kk] : T{S(0), S(0)};
-    T B = gb < nlines ? X[gb * nh + kk] : T{S(0), S(0)};
-    if (cj) {
-      A.y = -A.y;
-      B.y = -B.y;
-    }
-    if (k == 0 || ((n & 1) == 0 && k == n / 2)) {
-      A.y = S(0);
-      B.y = S(0);
-    }
-    a[pr * n + k] = T{A.x - B.y, A.y + B.x};
-  }
-  __syncthreads();
-  T* r = stockham<1>(a, b, tw, pl, ppb, n);
-  for (int i = threadIdx.x; i < 2 * ppb * n; i += blockDim.x) {
-    const int l = i / n, z = i - l * n;
-    const long long g = l0 + l;
-    if (g >= nlines) continue;
-    const T Z = r[(l >> 1) * n + z];
-    work[g * n + z] = ((l & 1) ? Z.y : Z.x) * scale;
-  }
-}
-
-// y: complex lines at fixed (c, x) and a tile of tk consecutive kz.
-template <int SIGN, typename R>
-__global__ void __launch_bounds__(256) k_fft_y(typename CT<R>::T* __restrict__ X, LinePlan pl,
-                                               const typename CT<R>::T* __restrict__ twg, int nh,
-                                               int tk, const IterCtrl* ctrl) {
-  using T = typename CT<R>::T;
-  if (ctrl && ctrl->done) return;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  const int ny = pl.n;
-  T* tw = reinterpret_cast<T*>(smraw);
-  T* a = tw + ny;
-  T* b = a + tk * ny;
-  for (int i = threadIdx.x; i < ny; i += blockDim.x) tw[i] = twg[i];
-  const int k0 = blockIdx.x * tk;
-  const int kc = min(tk, nh - k0);
-  T* base = X + (long long)blockIdx.y * ny * nh + k0;
-  for (int y = threadIdx.x; y < ny; y += blockDim.x) {
-    const T* src = base + (long long)y * nh;
-    for (int kk = 0; kk < tk; ++kk) a[kk * ny + y] = kk < kc ? src[kk] : T{R(0), R(0)};
-  }
-  __syncthreads();
-  T* r = stockham<SIGN>(a, b, tw, pl, tk, ny);
-  for (int y = threadIdx.x; y < ny; y += blockDim.x) {
-    T* dst = base + (long long)y * nh;
-    for (int kk = 0; kk < kc; ++kk) dst[kk] = r[kk * ny + y];
-  }
-}
-
-// x: all 5 components of the lines at fixed (y, kz tile); MODE 0 forward,
-// 1 inverse, 2 forward + Green operator + inverse.
-template <int MODE, typename R>
-__global__ void __launch_bounds__(256) k_fft_x(typename CT<R>::T* __restrict__ X, LinePlan pl,
-                                               const typename CT<R>::T* __restrict__ twg,
-                                               GreenParams<R> gp, int ny, int nh, int tk,
-                                               int ncomp, const IterCtrl* ctrl) {
-  using T = typename CT<R>::T;
-  if (ctrl && ctrl->done) return;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  const int nx = pl.n;
-  T* tw = reinterpret_cast<T*>(smraw);
-  T* a = tw + nx;
-  T* b = a + ncomp * tk * nx;
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = twg[i];
-  const int y = blockIdx.y;
-  const int k0 = blockIdx.x * tk;
-  const int kc = min(tk, nh - k0);
-  const long long cstride = (long long)nx * ny * nh;  // component stride
-  const long long xstride = (long long)ny * nh;
-  T* base = X + (long long)y * nh + k0;
-  for (int i = threadIdx.x; i < ncomp * nx; i += blockDim.x) {
-    const int c = i / nx, x = i - c * nx;
-    const T* src = base + c * cstride + x * xstride;
-    for (int kk = 0; kk < tk; ++kk) a[(c * tk + kk) * nx + x] = kk < kc ? src[kk] : T{R(0), R(0)};
-  }
-  __syncthreads();
-  T* r = a;
-  T* o = b;
-  if (MODE != 1) {
-    r = stockham<-1>(a, b, tw, pl, ncomp * tk, nx);
-    o = (r == a) ? b : a;
-  }
-  if (MODE == 2) {
-    for (int i = threadIdx.x; i < nx * tk; i += blockDim.x) {
-      const int x = i / tk, kk = i - x * tk;
-      if (kk >= kc) continue;
-      R pre[5], pim[5];
-#pragma unroll
-      for (int c = 0; c < 5; ++c) {
-        const T z = r[(c * tk + kk) * nx + x];
-        pre[c] = z.x;
-        pim[c] = z.y;
-      }
-      green_apply<R>(gp, x, y, k0 + kk, pre, pim);
-#pragma unroll
-      for (int c = 0; c < 5; ++c) r[(c * tk + kk) * nx + x] = T{pre[c], pim[c]};
-    }
-    __syncthreads();
-  }
-  if (MODE != 0) r = stockham<1>(r, o, tw, pl, ncomp * tk, nx);
-  for (int i = threadIdx.x; i < ncomp * nx; i += blockDim.x) {
-    const int c = i / nx, x = i - c * nx;
-    T* dst = base + c * cstride + x * xstride;
-    for (int kk = 0; kk < kc; ++kk) dst[kk] = r[(c * tk + kk) * nx + x];
-  }
-}
-
-template <typename R>
-size_t spectral_smem_optin(int) {
-  return kSmemBudget;
-}
-
-namespace {
-template <typename R>
-struct Tiles {
-  int ppb_z, tk_y, tk_x;
-  size_t sm_z, sm_y, sm_x;
-};
-template <typename R>
-Tiles<R> pick_tiles(const Spectral<R>& sp, int ncomp) {
-  using T = typename CT<R>::T;
-  Tiles<R> t;
-  const size_t e = sizeof(T);
-  // z: tw + 2 * ppb * nz
-  t.ppb_z = (int)((kSmemBudget / e - sp.nz) / (2 * (size_t)sp.nz));
-  t.ppb_z = t.ppb_z < 1 ? 1 : (t.ppb_z > 16 ? 16 : t.ppb_z);
-  t.sm_z = e * (sp.nz + 2 * (size_t)t.ppb_z * sp.nz);
-  t.tk_y = (int)((kSmemBudget / e - sp.ny) / (2 * (size_t)sp.ny));
-  t.tk_y = t.tk_y < 1 ? 1 : (t.tk_y > 16 ? 16 : t.tk_y);
-  if (t.tk_y > sp.nh) t.tk_y = sp.nh;
-  t.sm_y = e * (sp.ny + 2 * (size_t)t.tk_y * sp.ny);
-  t.tk_x = (int)((kSmemBudget / e - sp.nx) / (2 * (size_t)ncomp * sp.nx));
-  t.tk_x = t.tk_x < 1 ? 1 : (t.tk_x > 8 ? 8 : t.tk_x);
-  if (t.tk_x > sp.nh) t.tk_x = sp.nh;
-  t.sm_x = e * (sp.nx + 2 * (size_t)ncomp * t.tk_x * sp.nx);
-  return t;
-}
-template <typename R>
-void optin_all() {
-  static bool done = false;
-  if (done) return;
-  // the tiles target kSmemBudget; the longest legal lines may need more, up to
-  // the 227 KB a block can have on sm_100
-  const int s = 227 * 1024;
-  cudaFuncSetAttribute(k_fft_z_r2c<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
-  cudaFuncSetAttribute(k_fft_z_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
-  cudaFuncSetAttribute(k_fft_y<-1, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
-  cudaFuncSetAttribute(k_fft_y<1, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
-  cudaFuncSetAttribute(k_fft_x<0, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
-  cudaFuncSetAttribute(k_fft_x<1, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
-  cudaFuncSetAttribute(k_fft_x<2, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
-  done = true;
-}
-}  // namespace
-
-template <typename S>
-int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S* work,
-                              const IterCtrl* ctrl, cudaStream_t st, int ncomp,
-                              cudaEvent_t* ev) {
-  using T = typename CT<S>::T;
-  optin_all<S>();
-  const Tiles<S> t = pick_tiles(sp, ncomp);
-  const long long nlines = (long long)ncomp * sp.nx * sp.ny;
-  T* X = reinterpret_cast<T*>(sp.X);
-  const T* twx = reinterpret_cast<const T*>(sp.twx);
-  const T* twy = reinterpret_cast<const T*>(sp.twy);
-  const T* twz = reinterpret_cast<const T*>(sp.twz);
-  const int gz = (int)((nlines + 2 * t.ppb_z - 1) / (2 * t.ppb_z));
-  if (ev) cudaEventRecord(ev[0], st);
-  k_fft_z_r2c<S><<<gz, 256, t.sm_z, st>>>(work, X, sp.pz, twz, nlines, sp.nh, t.ppb_z, ctrl);
-  if (ev) cudaEventRecord(ev[1], st);
-  dim3 gy((sp.nh + t.tk_y - 1) / t.tk_y, ncomp * sp.nx);
-  k_fft_y<-1, S><<<gy, 256, t.sm_y, st>>>(X, sp.py, twy, sp.nh, t.tk_y, ctrl);
-  if (ev) cudaEventRecord(ev[2], st);
-  dim3 gx((sp.nh + t.tk_x - 1) / t.tk_x, sp.ny);
-  k_fft_x<2, S><<<gx, 256, t.sm_x, st>>>(X, sp.px, twx, gp, sp.ny, sp.nh, t.tk_x, ncomp, ctrl);
-  if (ev) cudaEventRecord(ev[3], st);
-  k_fft_y<1, S><<<gy, 256, t.sm_y, st>>>(X, sp.py, twy, sp.nh, t.tk_y, ctrl);
-  if (ev) cudaEventRecord(ev[4], st);
-  const S scale = S(1.0 / ((double)sp.nx * sp.ny * sp.nz));
-  k_fft_z_c2r<S><<<gz, 256, t.sm_z, st>>>(X, work, sp.pz, twz, nlines, sp.nh, t.ppb_z, scale, ctrl);
-  if (ev) cudaEventRecord(ev[5], st);
-  return 5;
-}
-
-template <typename S>
-int launch_fft3d(const Spectral<S>& sp, S* real, int ncomp, int mode, cudaStream_t st) {
-  using T = typename CT<S>::T;
-  optin_all<S>();
-  const Tiles<S> t = pick_tiles(sp, ncomp);
-  const long long nlines = (long long)ncomp * sp.nx * sp.ny;
-  T* X = reinterpret_cast<T*>(sp.X);
-  const T* twx = reinterpret_cast<const T*>(sp.twx);
-  const T* twy = reinterpret_cast<const T*>(sp.twy);
-  const T* twz = reinterpret_cast<const T*>(sp.twz);
-  const int gz = (int)((nlines + 2 * t.ppb_z - 1) / (2 * t.ppb_z));
-  dim3 gy((sp.nh + t.tk_y - 1) / t.tk_y, ncomp * sp.nx);
-  dim3 gx((sp.nh + t.tk_x - 1) / t.tk_x, sp.ny);
-  GreenParams<S> gp{};
-  if (mode == 0) {
-    k_fft_z_r2c<S><<<gz, 256, t.sm_z, st>>>(real, X, sp.pz, twz, nlines, sp.nh, t.ppb_z, nullptr);
-    k_fft_y<-1, S><<<gy, 256, t.sm_y, st>>>(X, sp.py, twy, sp.nh, t.tk_y, nullptr);
-    k_fft_x<0, S><<<gx, 256, t.sm_x, st>>>(X, sp.px, twx, gp, sp.ny, sp.nh, t.tk_x, ncomp, nullptr);
-  } else {
-    k_fft_x<1, S><<<gx, 256, t.sm_x, st>>>(X, sp.px, twx, gp, sp.ny, sp.nh, t.tk_x, ncomp, nullptr);
-    k_fft_y<1, S><<<gy, 256, t.sm_y, st>>>(X, sp.py, twy, sp.nh, t.tk_y, nullptr);
-    const S scale = S(1.0 / ((double)sp.nx * sp.ny * sp.nz));
-    k_fft_z_c2r<S><<<gz, 256, t.sm_z, st>>>(X, real, sp.pz, twz, nlines, sp.nh, t.ppb_z, scale,
-                                            nullptr);
-  }
-  return 3;
-}
-
 // ============================================================== Solvers batch (testing)
 __device__ __forceinline__ void load_schmid(const double* schmid, int v, double m[kNS][5]) {
 #pragma unroll
@@ -860,10 +457,6 @@ int launch_green_batch(int n, const int32_t* kidx, const GreenParams<R>& gp, con
   template int launch_from_soa<S>(const S*, double*, long long, int, cudaStream_t);              \
   template int launch_fill<S>(S*, long long, double, cudaStream_t);                              \
   template int launch_crss_broadcast<S>(S*, long long, const double*, cudaStream_t);             \
-  template int launch_spectral_iteration<S>(const Spectral<S>&, const GreenParams<S>&, S*,       \
-                                            const IterCtrl*, cudaStream_t, int, cudaEvent_t*);   \
-  template int launch_fft3d<S>(const Spectral<S>&, S*, int, int, cudaStream_t);                  \
-  template size_t spectral_smem_optin<S>(int);                                                   \
   template int launch_green_batch<S>(int, const int32_t*, const GreenParams<S>&, const double*,  \
                                      double*, cudaStream_t);
 VPFFT_INST(double)

@@ -109,7 +109,8 @@ struct Spectral {
   const void* twx;  // twiddle tables exp(-2 pi i e / n), complex R
   const void* twy;
   const void* twz;
-  void* X;          // 5 x nx x ny x nh complex R
+  void* X;          // A[c][x][kz][y]: spectrum after the z pass (complex R)
+  void* X2;         // B[c][kz][ky][x]: spectrum after the y pass
 };
 // forward: work (P) -> X ; inverse: X -> work (d~, scaled by 1/N)
 // ev (optional): 6 events recorded before the first and after each of the 5 kernels
@@ -120,8 +121,6 @@ int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S
 // forward-only / inverse-only transforms for testing (mode 0 = forward, 1 = inverse)
 template <typename S>
 int launch_fft3d(const Spectral<S>& sp, S* real, int ncomp, int mode, cudaStream_t st);
-template <typename R>
-size_t spectral_smem_optin(int device);
 
 // --- batched solver entry points for testing (double, voxel-major) ---------
 int launch_solvers_constrained(int n, const double* s0, const double* schmid, const double* crss,

@@ -115,36 +115,37 @@ __device__ __forceinline__ void load_m(const MS* msm, int bs, int s, double m[5]
 
 // LDL^T solve of a symmetric positive-definite 5x5 A (packed upper) x = b.
 // Returns false when a pivot is not positive (A not numerically SPD).
-__device__ __forceinline__ bool ldlt5_solve(const double A[15], const double b[5], double x[5]) {
-  double L[5][5], d[5], id[5];
+template <typename T>
+__device__ __forceinline__ bool ldlt5_solve(const T A[15], const T b[5], T x[5]) {
+  T L[5][5], d[5], id[5];
   bool ok = true;
 #pragma unroll
   for (int j = 0; j < 5; ++j) {
-    double dj = A[sym5(j, j)];
+    T dj = A[sym5(j, j)];
 #pragma unroll
     for (int k = 0; k < j; ++k) dj -= L[j][k] * L[j][k] * d[k];
-    ok = ok && (dj > 0.0);
+    ok = ok && (dj > T(0));
     d[j] = dj;
-    id[j] = 1.0 / dj;
+    id[j] = T(1) / dj;
 #pragma unroll
     for (int i = j + 1; i < 5; ++i) {
-      double a = A[sym5(j, i)];
+      T a = A[sym5(j, i)];
 #pragma unroll
       for (int k = 0; k < j; ++k) a -= L[i][k] * L[j][k] * d[k];
       L[i][j] = a * id[j];
     }
   }
-  double z[5];
+  T z[5];
 #pragma unroll
   for (int i = 0; i < 5; ++i) {
-    double a = b[i];
+    T a = b[i];
 #pragma unroll
     for (int k = 0; k < i; ++k) a -= L[i][k] * z[k];
     z[i] = a;
   }
 #pragma unroll
   for (int i = 4; i >= 0; --i) {
-    double a = z[i] * id[i];
+    T a = z[i] * id[i];
 #pragma unroll
     for (int k = i + 1; k < 5; ++k) a -= L[k][i] * x[k];
     x[i] = a;
@@ -162,40 +163,92 @@ __device__ __forceinline__ double itau_of(const MS* tsm, int bs, const NRParams&
     return p.icrss[q];
 }
 
-// One pass over the systems: r_s, admissibility, S = sum m gdot r, K = sum n gdot/tau m m^T.
+// One pass over the systems: r_s, admissibility, S = sum m gdot r, K = sum n gdot/tau m m^T,
+// in arithmetic type T (double, or float for the predictor of the mixed path).
 // snap: set |r| < 1e-10 to 0 (the unconstrained solver does, Solvers.cpp:50-51).
-template <int NEXP, bool kSnap, bool kTauSmem, typename MS>
+template <int NEXP, bool kSnap, bool kTauSmem, typename T, typename MS>
 __device__ __forceinline__ bool accumulate(const MS* msm, const MS* tsm, int bs,
-                                           const NRParams& p, const double s[5], double S[5],
-                                           double K[15]) {
+                                           const NRParams& p, const T s[5], T S[5], T K[15]) {
   bool adm = true;
 #pragma unroll
-  for (int c = 0; c < 5; ++c) S[c] = 0.0;
+  for (int c = 0; c < 5; ++c) S[c] = T(0);
 #pragma unroll
-  for (int k = 0; k < 15; ++k) K[k] = 0.0;
+  for (int k = 0; k < 15; ++k) K[k] = T(0);
 #pragma unroll 2
   for (int q = 0; q < kNS; ++q) {
-    double m[5];
-    load_m(msm, bs, q, m);
-    const double it = itau_of<kTauSmem>(tsm, bs, p, q);
-    double r = (m[0] * s[0] + m[1] * s[1] + m[2] * s[2] + m[3] * s[3] + m[4] * s[4]) * it;
-    if (kSnap) r = fabs(r) < 1e-10 ? 0.0 : r;
-    adm = adm && !(fabs(r) > p.max_rss);
+    T m[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) m[c] = (T)msm[(q * 5 + c) * bs];
+    const T it = (T)itau_of<kTauSmem>(tsm, bs, p, q);
+    T r = (m[0] * s[0] + m[1] * s[1] + m[2] * s[2] + m[3] * s[3] + m[4] * s[4]) * it;
+    if (kSnap) r = fabs(r) < T(1e-10) ? T(0) : r;
+    adm = adm && !(fabs(r) > (T)p.max_rss);
     const int n = p.nexp[q];
     // the constrained solver tests n != 1, the unconstrained n - 1 > 0 (Solvers.cpp:66,177)
     const bool power = kSnap ? (n - 1 > 0) : (n != 1);
-    const double g = power ? p.gdot[q] * pow_nm1<NEXP>(fabs(r), n) : p.gdot[q];
-    const double gr = g * r;
-    const double w = (double)n * g * it;
+    const T g = power ? (T)p.gdot[q] * pow_nm1<NEXP>(fabs(r), n) : (T)p.gdot[q];
+    const T gr = g * r;
+    const T w = (T)n * g * it;
 #pragma unroll
     for (int i = 0; i < 5; ++i) {
       S[i] += m[i] * gr;
-      const double mw = m[i] * w;
+      const T mw = m[i] * w;
 #pragma unroll
       for (int j = i; j < 5; ++j) K[sym5(i, j)] += mw * m[j];
     }
   }
   return adm;
+}
+
+// Newton predictor of the constrained solve in FP32 (mixed precision only):
+// the reference's iteration and stopping rule in single precision.  Returns
+// true and the iterate in s_io when it converged with finite values; the
+// caller then takes the accepted step with FP64 residual and Jacobian.
+template <int NEXP, bool kTauSmem, typename MS>
+__device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, int bs,
+                                                const NRParams& p, const float L0i[15],
+                                                const double lam[5], const double ed[5],
+                                                double s_io[5], int max_steps) {
+  float cur[5], l32[5], e32[5];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) {
+    cur[c] = (float)s_io[c];
+    l32[c] = (float)lam[c];
+    e32[c] = (float)ed[c];
+  }
+  for (int it = 0; it < max_steps; ++it) {
+    float S[5], K[15];
+    if (!accumulate<NEXP, false, kTauSmem, float>(msm, tsm, bs, p, cur, S, K)) return false;
+    float y[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      float a = S[i] - e32[i];
+#pragma unroll
+      for (int j = 0; j < 5; ++j) a += L0i[sym5(i, j)] * (cur[j] - l32[j]);
+      y[i] = -a;
+    }
+#pragma unroll
+    for (int k = 0; k < 15; ++k) K[k] += L0i[k];
+    float delta[5];
+    if (!ldlt5_solve(K, y, delta)) return false;
+    float dn = 0.f, an = 0.f;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      const float nw = cur[c] + delta[c];
+      const float av = (nw + cur[c]) * 0.5f;
+      dn += delta[c] * delta[c];
+      an += av * av;
+      cur[c] = nw;
+    }
+    const float rel = sqrtf(dn) / sqrtf(an);
+    if (!isfinite(rel)) return false;
+    if (rel < (float)p.eps) {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) s_io[c] = (double)cur[c];
+      return true;
+    }
+  }
+  return false;
 }
 
 // SolveConstrainedConstitutiveEquations (Solvers.cpp:111-222).  ed = Edot + d~.
@@ -216,7 +269,7 @@ __device__ __forceinline__ int nr_constrained_smem(const MS* msm, const MS* tsm,
     // admissibility loop (Solvers.cpp:147-172): back off towards the saved
     // state while some |r_s| exceeds the cap; every pass costs one iteration
     for (;;) {
-      const bool adm = accumulate<NEXP, false, kTauSmem>(msm, tsm, bs, p, cur, S, K);
+      const bool adm = accumulate<NEXP, false, kTauSmem, double>(msm, tsm, bs, p, cur, S, K);
       if (!adm) {
 #pragma unroll
         for (int c = 0; c < 5; ++c) cur[c] = saved[c] + (cur[c] - saved[c]) * 0.2;
@@ -245,7 +298,7 @@ __device__ __forceinline__ int nr_constrained_smem(const MS* msm, const MS* tsm,
 #pragma unroll
     for (int k = 0; k < 15; ++k) K[k] += p.L0inv[k];
     double delta[5];
-    ldlt5_solve(K, y, delta);
+    ldlt5_solve<double>(K, y, delta);
     double dn = 0.0, an = 0.0;
 #pragma unroll
     for (int c = 0; c < 5; ++c) {
@@ -297,7 +350,7 @@ __device__ __forceinline__ int nr_unconstrained_smem(const MS* msm, const MS* ts
   while (remaining > 0) {
     double S[5], K[15];
     for (;;) {
-      const bool adm = accumulate<NEXP, true, kTauSmem>(msm, tsm, bs, p, cur, S, K);
+      const bool adm = accumulate<NEXP, true, kTauSmem, double>(msm, tsm, bs, p, cur, S, K);
       if (!adm) {
 #pragma unroll
         for (int c = 0; c < 5; ++c) cur[c] = saved[c] + (cur[c] - saved[c]) * 0.2;
@@ -318,7 +371,7 @@ __device__ __forceinline__ int nr_unconstrained_smem(const MS* msm, const MS* ts
       res[c] = S[c] - edot[c];
       mres[c] = -res[c];
     }
-    if (!ldlt5_solve(K, mres, delta)) solve_neg_K_fullpiv(K, res, delta);
+    if (!ldlt5_solve<double>(K, mres, delta)) solve_neg_K_fullpiv(K, res, delta);
     double dn = 0.0, sn = 0.0;
 #pragma unroll
     for (int c = 0; c < 5; ++c) {

@@ -118,6 +118,15 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
     }
     double rel;
     bool capped;
+    if constexpr (sizeof(S) == 4) {
+      // mixed precision: FP32 Newton predictor, then the FP64 solve from its
+      // iterate (normally one Newton step with FP64 residual and Jacobian);
+      // from the original start if the predictor failed
+      float L0i[15];
+#pragma unroll
+      for (int k = 0; k < 15; ++k) L0i[k] = (float)p.L0inv[k];
+      nr_predict_fp32<NEXP, kTauSmem>(msm, tsm, bs, p, L0i, lam, ed, s, 8);
+    }
     nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, lam, ed, s, &rel, &capped);
     capped_count += capped ? 1 : 0;
     double e[5];
