@@ -216,6 +216,24 @@ vpfft_status vpfft_solve_constrained_constitutive(int n, const double *stress0,
                                                   const double L0[25], double eps,
                                                   double max_rss, int max_iter,
                                                   double *stress_out, double *nr_error);
+/* The same constrained solve, with NO device memory allocation.  No
+ * counterpart in the reference.  For callers that cannot allocate: a
+ * macro-scale driver calling the point solve from inside its own Newton loop
+ * typically gives the device to its own memory pool, where a cudaMalloc can
+ * fail and every cudaFree synchronises the device.  The arrays are staged in
+ * a fixed device array of VPFFT_NOALLOC_MAX_POINTS points (2.9 MiB) that lives
+ * as long as the library; larger n returns VPFFT_ERR_UNSUPPORTED_SIZE.  The
+ * first call on each device looks up that array's address: make it before any
+ * stream capture begins.  Calls share the array, so they are serialised by a
+ * process-wide lock (overlapping calls would otherwise race on it).
+ * not_converged (may be NULL) gets the number of points whose NR error is not
+ * below eps. */
+#define VPFFT_NOALLOC_MAX_POINTS 4096
+vpfft_status vpfft_solve_constrained_constitutive_noalloc(
+    int n, const double *stress0, const double *schmid, const double *crss,
+    const vpfft_material *m, const double edot[5], const double *lambda, const double *dtilde,
+    const double L0[25], double eps, double max_rss, int max_iter, double *stress_out,
+    double *nr_error, int64_t *not_converged);
 /* ApplyConstitutiveEquations (Solvers.cpp:255-274) */
 vpfft_status vpfft_apply_constitutive(int n, const double *stress, const double *schmid,
                                       const double *crss, const vpfft_material *m,

@@ -45,6 +45,7 @@ FIELD_SCHMID = 8
 FIELD_WIDTH = {0: 5, 1: 5, 2: 9, 3: 12, 4: 1, 5: 5, 6: 5, 7: 5, 8: 60}
 
 NUM_PHASES = 7
+NOALLOC_MAX_POINTS = 4096
 
 
 class Material(C.Structure):
@@ -150,6 +151,9 @@ _PROTOS = {
     "vpfft_solve_constrained_constitutive": (C.c_int, [C.c_int, _D, _D, _D, C.POINTER(Material),
                                                        _D, _D, _D, _D, C.c_double, C.c_double,
                                                        C.c_int, _D, _D]),
+    "vpfft_solve_constrained_constitutive_noalloc": (
+        C.c_int, [C.c_int, _D, _D, _D, C.POINTER(Material), _D, _D, _D, _D, C.c_double,
+                  C.c_double, C.c_int, _D, _D, C.POINTER(C.c_int64)]),
     "vpfft_apply_constitutive": (C.c_int, [C.c_int, _D, _D, _D, C.POINTER(Material), _D]),
     "vpfft_solve_sachs": (C.c_int, [C.c_int, _D, _D, _D, _D]),
     "vpfft_schmid_tensors": (C.c_int, [C.c_int, _D, _D]),

@@ -163,6 +163,11 @@ void inverse5_host(const double* a, double* out) {
 
 void vpfft::inverse5_colmajor(const double* a, double* out) { inverse5_host(a, out); }
 
+// Library-level error slot (vpfft_last_error(NULL)) for entry points in other files.
+namespace vpfft {
+vpfft_status lib_fail(vpfft_status s, const std::string& msg) { return fail(nullptr, s, msg); }
+}  // namespace vpfft
+
 namespace {
 
 MaterialParams mat_params(const vpfft_material& m) {

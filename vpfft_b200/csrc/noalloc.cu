@@ -1,0 +1,158 @@
+// noalloc.cu -- vpfft_solve_constrained_constitutive_noalloc: the batched
+// constrained constitutive solve with no device memory allocation.
+//
+// Who needs it: a macro-scale driver (a finite-element code that calls the
+// crystal-plasticity point solve at every integration point of every global
+// Newton iteration) usually hands the whole device to its own memory pool,
+// so a cudaMalloc inside the call can fail, and each cudaFree synchronises
+// the device and stalls the driver's other streams.  This entry point stages
+// the caller's host arrays in a fixed device array that exists as long as the
+// library is loaded, so it calls neither cudaMalloc nor cudaFree nor any
+// library routine that allocates.
+//
+// Limits and rules:
+//  * at most VPFFT_NOALLOC_MAX_POINTS points per call (larger n is refused
+//    with VPFFT_ERR_UNSUPPORTED_SIZE; split the batch);
+//  * the first call on each device looks up the array's device address
+//    (cudaGetSymbolAddress, with that device current); make that first call
+//    before any stream capture begins;
+//  * there is one array per device per process, so two calls that overlapped
+//    in time would race on it: the entry point holds a process-wide lock for
+//    the whole call, and concurrent callers run one after another;
+//  * the array keeps the previous call's contents; the only value that must
+//    start at zero (the count of non-converged points) is cleared each call.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <mutex>
+#include <string>
+
+#include "../../include/vpfft_capi.h"
+#include "kernels.h"
+
+namespace vpfft {
+vpfft_status lib_fail(vpfft_status s, const std::string& msg);
+}
+
+namespace {
+
+constexpr int kMaxPoints = VPFFT_NOALLOC_MAX_POINTS;
+constexpr int kMaxDevices = 64;
+// doubles per point: stress0 5, schmid 60, crss 12, lambda 5, d~ 5, out 5, NR error 1
+constexpr long long kOffS0 = 0;
+constexpr long long kOffSchmid = kOffS0 + 5LL * kMaxPoints;
+constexpr long long kOffCrss = kOffSchmid + 60LL * kMaxPoints;
+constexpr long long kOffLambda = kOffCrss + 12LL * kMaxPoints;
+constexpr long long kOffDtilde = kOffLambda + 5LL * kMaxPoints;
+constexpr long long kOffOut = kOffDtilde + 5LL * kMaxPoints;
+constexpr long long kOffErr = kOffOut + 5LL * kMaxPoints;
+constexpr long long kOffCount = kOffErr + 1LL * kMaxPoints;  // one 64-bit counter
+constexpr long long kScratchDoubles = kOffCount + 32;       // counter + padding
+
+// 93 doubles x 4096 points + 256 bytes = 2.9 MiB per device.
+static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
+
+std::mutex g_noalloc_lock;
+double* g_scratch_ptr[kMaxDevices] = {nullptr};
+
+// Points whose final NR error is not below eps (or is NaN) -- the batch's
+// "not converged" count, accumulated into the scratch counter.
+__global__ void k_count_not_converged(const double* __restrict__ err, int n, double eps,
+                                      unsigned long long* count) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool bad = v < n && !(err[v] < eps);
+  const unsigned mask = __ballot_sync(0xffffffffu, bad);
+  if ((threadIdx.x & 31) == 0 && mask) atomicAdd(count, (unsigned long long)__popc(mask));
+}
+
+vpfft_status cuda_fail(cudaError_t e, const char* what) {
+  return vpfft::lib_fail(e == cudaErrorMemoryAllocation ? VPFFT_ERR_OUT_OF_MEMORY : VPFFT_ERR_CUDA,
+                         std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define NA_CK(call)                                   \
+  do {                                                \
+    cudaError_t e_ = (call);                          \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+// Device address of the scratch array on the current device (looked up once
+// per device; the caller holds g_noalloc_lock).
+vpfft_status scratch_for_current_device(double** out) {
+  int dev = -1;
+  NA_CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices)
+    return vpfft::lib_fail(VPFFT_ERR_UNSUPPORTED_SIZE, "device ordinal out of range");
+  if (!g_scratch_ptr[dev]) {
+    void* p = nullptr;
+    NA_CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_scratch_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_scratch_ptr[dev];
+  return VPFFT_OK;
+}
+
+}  // namespace
+
+extern "C" vpfft_status vpfft_solve_constrained_constitutive_noalloc(
+    int n, const double* s0, const double* schmid, const double* crss, const vpfft_material* m,
+    const double edot[5], const double* lambda, const double* dtilde, const double L0[25],
+    double eps, double max_rss, int max_iter, double* out, double* nr_error,
+    int64_t* not_converged) {
+  if (n < 0 || !s0 || !schmid || !crss || !m || !edot || !lambda || !dtilde || !L0 || !out)
+    return vpfft::lib_fail(VPFFT_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (n > kMaxPoints)
+    return vpfft::lib_fail(VPFFT_ERR_UNSUPPORTED_SIZE,
+                           "n = " + std::to_string(n) + " exceeds the no-allocation scratch of " +
+                               std::to_string(kMaxPoints) +
+                               " points; split the batch or call "
+                               "vpfft_solve_constrained_constitutive");
+  int cnt = 0;
+  if (cudaGetDeviceCount(&cnt) != cudaSuccess || cnt <= 0) {
+    cudaGetLastError();
+    return vpfft::lib_fail(VPFFT_ERR_NO_DEVICE,
+                           "no CUDA device available (vpfft_b200 has no CPU fallback)");
+  }
+  if (not_converged) *not_converged = 0;
+  if (n == 0) return VPFFT_OK;
+
+  std::lock_guard<std::mutex> lock(g_noalloc_lock);
+  double* base = nullptr;
+  if (vpfft_status s = scratch_for_current_device(&base)) return s;
+  double* d_s0 = base + kOffS0;
+  double* d_schmid = base + kOffSchmid;
+  double* d_crss = base + kOffCrss;
+  double* d_lambda = base + kOffLambda;
+  double* d_dtilde = base + kOffDtilde;
+  double* d_out = base + kOffOut;
+  double* d_err = base + kOffErr;
+  auto* d_count = reinterpret_cast<unsigned long long*>(base + kOffCount);
+
+  const size_t b5 = sizeof(double) * 5 * (size_t)n;
+  NA_CK(cudaMemcpy(d_s0, s0, b5, cudaMemcpyHostToDevice));
+  NA_CK(cudaMemcpy(d_schmid, schmid, sizeof(double) * 60 * (size_t)n, cudaMemcpyHostToDevice));
+  NA_CK(cudaMemcpy(d_crss, crss, sizeof(double) * 12 * (size_t)n, cudaMemcpyHostToDevice));
+  NA_CK(cudaMemcpy(d_lambda, lambda, b5, cudaMemcpyHostToDevice));
+  NA_CK(cudaMemcpy(d_dtilde, dtilde, b5, cudaMemcpyHostToDevice));
+  NA_CK(cudaMemset(d_count, 0, sizeof(unsigned long long)));
+
+  vpfft::MaterialParams mp;
+  for (int k = 0; k < vpfft::kNS; ++k) {
+    mp.gdot[k] = m->gamma_dot_base[k];
+    mp.nexp[k] = m->rate_sensitivity[k];
+  }
+  vpfft::launch_solvers_constrained(n, d_s0, d_schmid, d_crss, mp, edot, d_lambda, d_dtilde, L0,
+                                    eps, max_rss, max_iter, d_out, d_err, nullptr);
+  NA_CK(cudaGetLastError());
+  k_count_not_converged<<<(n + 255) / 256, 256>>>(d_err, n, eps, d_count);
+  NA_CK(cudaGetLastError());
+  NA_CK(cudaDeviceSynchronize());
+  NA_CK(cudaMemcpy(out, d_out, b5, cudaMemcpyDeviceToHost));
+  if (nr_error) NA_CK(cudaMemcpy(nr_error, d_err, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  if (not_converged) {
+    unsigned long long c = 0;
+    NA_CK(cudaMemcpy(&c, d_count, sizeof(c), cudaMemcpyDeviceToHost));
+    *not_converged = (int64_t)c;
+  }
+  return VPFFT_OK;
+}
