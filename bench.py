@@ -429,7 +429,11 @@ def main(argv=None):
         "bound": "hbm", "kernel": dom,
         "achieved": kernels[dom]["achieved_gbs"], "peak": hbm, "unit": "GB/s",
         "frac": kernels[dom]["achieved_gbs"] / hbm, "peak_kind": peak_kind,
-        "traffic": TRAFFIC_PER_LAUNCH.get((args.precision, args.grid, dom)),
+        "traffic": (TRAFFIC_PER_VOXEL[(args.precision, dom)] * N
+                    if (args.precision, dom) in TRAFFIC_PER_VOXEL else None),
+        "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at "
+                           "192^3, scaled by the voxel count"
+                           if (args.precision, dom) in TRAFFIC_PER_VOXEL else None),
         "alg_bytes_per_voxel": alg[dom],
         "iteration": {"alg_bytes_per_voxel": sum(alg.values()),
                       "achieved_gbs": it_bytes / (ms / args.steps * 1e-3) / 1e9,
@@ -495,9 +499,11 @@ def main(argv=None):
     return 0
 
 
-# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from the
-# ncu captures summarised under profiles/; None until captured.
-TRAFFIC_PER_LAUNCH: dict = {}
+# DRAM bytes per voxel of one launch (dram__bytes_read.sum + dram__bytes_write.sum
+# divided by the voxel count) from the ncu capture at 192^3 summarised in
+# profiles/k_nr_update_192cubed_mixed.md; the kernel's traffic is proportional to
+# the voxel count (it streams each voxel's fields once), so it scales to 256^3.
+TRAFFIC_PER_VOXEL: dict = {("mixed", "nr_update"): (682.147328e6 + 377.704704e6) / 192 ** 3}
 
 
 if __name__ == "__main__":
