@@ -198,7 +198,7 @@ def device_arm(args, R, edot, precision):
     avg = hist[-1, :5].copy()
     st = grid.last_stats
     res = dict(ms=ms, N=N, phases=phases, launches=launches, clocks=clk.summary(0), avg=avg,
-               iters=int(st.iterations), grid=grid)
+               iters=int(st.iterations), grid=grid, nr_capped=int(st.nr_not_converged))
     return res
 
 
@@ -467,14 +467,19 @@ def main(argv=None):
         s_d = f["grid"].Stress()
         e_m = main_grid.StrainRate()
         e_d = f["grid"].StrainRate()
+        rel_s = np.linalg.norm(s_m - s_d, axis=1) / np.linalg.norm(s_d, axis=1)
         line["fp64"] = {
             "value": v64, "unit": UNIT, "ms_per_step": ms64 / args.steps,
             "mixed_over_fp64": value / v64,
             "error_vs_fp64": {
                 "avg_stress_rel": float(np.linalg.norm(main_res["avg"] - f["avg"]) /
                                         np.linalg.norm(f["avg"])),
-                "stress_field_max_rel": float((np.linalg.norm(s_m - s_d, axis=1) /
-                                               np.linalg.norm(s_d, axis=1)).max()),
+                "stress_field_max_rel": float(rel_s.max()),
+                "stress_field_rel_p99": float(np.quantile(rel_s, 0.99)),
+                "stress_field_rel_p99_99": float(np.quantile(rel_s, 0.9999)),
+                "voxels_stress_rel_above_1e-3": int(np.count_nonzero(rel_s > 1e-3)),
+                "nr_not_converged_voxel_iters": {"mixed": int(main_res["nr_capped"]),
+                                               "fp64": int(f["nr_capped"])},
                 "strain_rate_field_rms_rel": float(np.sqrt(np.mean((e_m - e_d) ** 2)) /
                                                    np.sqrt(np.mean(e_d ** 2))),
                 "iterations": args.warmup + args.steps},

@@ -45,7 +45,8 @@ typedef enum {
   VPFFT_ERR_NOT_INITIALIZED = 8,  /* fields not set before a solve */
   VPFFT_ERR_IO = 9,               /* file could not be read or parsed */
   VPFFT_ERR_CANCELLED = 10,
-  VPFFT_ERR_TIMEOUT = 11
+  VPFFT_ERR_TIMEOUT = 11,
+  VPFFT_ERR_BUSY = 12             /* the grid has a request in flight in a batch */
 } vpfft_status;
 
 typedef enum {
@@ -275,6 +276,74 @@ vpfft_status vpfft_fixture_polycrystal(int nx, int ny, int nz, int n_grains, uin
 void vpfft_edot_from_matrix(const double L[9], double edot_out[5]);
 /* EigenRep::ToMatrixRep (LinearAlgebra.h:352-360) */
 void vpfft_matrix_from_edot(const double edot[5], double L_out[9]);
+
+/* ------------------------------------------------------------------ batches
+ * Many RVEs (grids of possibly different sizes) advanced together: every
+ * phase of an increment (initialisation, reference medium, the five FFT
+ * passes with the Green operator, the Newton-Raphson sweep, the reductions,
+ * the texture/hardening update) is ONE kernel launch over all RVEs in that
+ * phase, and the fixed-point iterations of a tick are replayed from a captured
+ * CUDA graph while the set of iterating RVEs is unchanged.  The reference has
+ * no counterpart (it solves one RVE per MPI job); each request is one
+ * RunSingleStrainStep (MaterialGrid.cpp:897-1084) on a caller-owned grid,
+ * whose fields and texture persist across requests.
+ *
+ * Continuous batching: vpfft_batch_step runs one tick -- requests that arrived
+ * since the last tick are admitted while a slot is free and their spectra fit
+ * the HBM budget (FIFO; a request waits while its grid has one in flight),
+ * newly admitted RVEs are initialised while the others iterate, converged RVEs
+ * get their post-increment update and are reported by vpfft_batch_poll.  A
+ * batch is bound to the device current at creation and is not thread-safe. */
+typedef struct vpfft_batch vpfft_batch;
+typedef struct {
+  int32_t max_slots;            /* RVEs in flight at once (default 256) */
+  int32_t iterations_per_tick;  /* fixed-point iterations enqueued per tick (default 8) */
+  int64_t hbm_budget_bytes;     /* device memory for in-flight spectra (default 8 GiB) */
+  int32_t use_graphs;           /* replay the tick's iterations from a CUDA graph (default 1) */
+  int32_t pad_;
+} vpfft_batch_options;
+typedef struct {
+  int64_t request_id;
+  int32_t status;               /* vpfft_status of the request */
+  int32_t iterations;           /* fixed-point iterations executed */
+  int32_t converged;
+  int32_t pad_;
+  double avg_stress[5];         /* <sigma> of the last iteration (the step's return value) */
+  double stress_error;          /* final delta_sigma */
+  double strain_rate_error;     /* final delta_eps */
+  int64_t nr_not_converged;     /* voxel-iterations whose NR hit its cap */
+  double seconds_queued;        /* submit -> admission */
+  double seconds_total;         /* submit -> completion (after the tick that finished it) */
+} vpfft_batch_result;
+typedef struct {
+  int64_t queued, active, completed;
+  int64_t ticks, graph_replays, kernel_launches;
+  int64_t arena_bytes_in_use, arena_bytes;
+  int64_t admissions_deferred_for_memory;  /* ticks at which the head request did not fit */
+} vpfft_batch_info;
+void vpfft_batch_options_default(vpfft_batch_options *o);
+vpfft_status vpfft_batch_create(vpfft_precision precision, const vpfft_material *material,
+                                const vpfft_solver_options *options,
+                                const vpfft_batch_options *batch_options, vpfft_batch **out);
+vpfft_status vpfft_batch_destroy(vpfft_batch *b);
+/* Queue one increment (RunSingleStrainStep) on grid g, which must have the
+ * batch's precision, material and solver options and its fields set.  The
+ * grid belongs to the batch until the request completes (other calls on it
+ * return VPFFT_ERR_BUSY). */
+vpfft_status vpfft_batch_submit(vpfft_batch *b, vpfft_grid *g, const double edot[5], int max_iter,
+                                double dt, double eps, int64_t *request_id);
+/* One tick; *pending (may be NULL) = queued + active requests afterwards. */
+vpfft_status vpfft_batch_step(vpfft_batch *b, int *pending);
+/* Ticks until every submitted request has completed. */
+vpfft_status vpfft_batch_run(vpfft_batch *b);
+/* Completed requests since the last poll, oldest first (at most cap). */
+vpfft_status vpfft_batch_poll(vpfft_batch *b, vpfft_batch_result *out, int cap, int *n_out);
+/* A queued request is dropped; an active one stops at the next tick with its
+ * grid as the last executed iteration left it (no texture/hardening update).
+ * Both complete with status VPFFT_ERR_CANCELLED. */
+vpfft_status vpfft_batch_cancel(vpfft_batch *b, int64_t request_id);
+vpfft_status vpfft_batch_get_info(const vpfft_batch *b, vpfft_batch_info *info);
+const char *vpfft_batch_last_error(const vpfft_batch *b);
 
 /* ------------------------------------------------------------------ config
  * Utilities::ConfigFile (Config.h:21-85, Config.cpp:11-300) with its defects

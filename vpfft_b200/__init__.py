@@ -9,6 +9,7 @@ from . import capi
 from .capi import Material, SolverOptions, Stats, VpfftError, device_count, load, material
 from .config import ConfigFile
 from .material_grid import MaterialGrid
+from .batch import Batch, BatchResult
 
 __all__ = ["capi", "Material", "SolverOptions", "Stats", "VpfftError", "device_count", "load",
-           "material", "MaterialGrid", "ConfigFile"]
+           "material", "MaterialGrid", "ConfigFile", "Batch", "BatchResult"]

@@ -29,6 +29,9 @@ ERR_MAX_RSS_TINY = 6
 ERR_NONFINITE = 7
 ERR_NOT_INITIALIZED = 8
 ERR_IO = 9
+ERR_CANCELLED = 10
+ERR_TIMEOUT = 11
+ERR_BUSY = 12
 
 PREC_FP64 = 0
 PREC_MIXED = 1
@@ -107,6 +110,38 @@ class Config(C.Structure):
     ]
 
 
+class BatchOptions(C.Structure):
+    _fields_ = [
+        ("max_slots", C.c_int32),
+        ("iterations_per_tick", C.c_int32),
+        ("hbm_budget_bytes", C.c_int64),
+        ("use_graphs", C.c_int32),
+        ("pad_", C.c_int32),
+    ]
+
+
+class BatchResult(C.Structure):
+    _fields_ = [
+        ("request_id", C.c_int64),
+        ("status", C.c_int32),
+        ("iterations", C.c_int32),
+        ("converged", C.c_int32),
+        ("pad_", C.c_int32),
+        ("avg_stress", C.c_double * 5),
+        ("stress_error", C.c_double),
+        ("strain_rate_error", C.c_double),
+        ("nr_not_converged", C.c_int64),
+        ("seconds_queued", C.c_double),
+        ("seconds_total", C.c_double),
+    ]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [(name, C.c_int64) for name in (
+        "queued", "active", "completed", "ticks", "graph_replays", "kernel_launches",
+        "arena_bytes_in_use", "arena_bytes", "admissions_deferred_for_memory")]
+
+
 STEP_CALLBACK = C.CFUNCTYPE(C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
                             C.c_void_p)
 
@@ -165,6 +200,18 @@ _PROTOS = {
                                             _I32]),
     "vpfft_edot_from_matrix": (None, [_D, _D]),
     "vpfft_matrix_from_edot": (None, [_D, _D]),
+    "vpfft_batch_options_default": (None, [C.POINTER(BatchOptions)]),
+    "vpfft_batch_create": (C.c_int, [C.c_int, C.POINTER(Material), C.POINTER(SolverOptions),
+                                     C.POINTER(BatchOptions), C.POINTER(_G)]),
+    "vpfft_batch_destroy": (C.c_int, [_G]),
+    "vpfft_batch_submit": (C.c_int, [_G, _G, _D, C.c_int, C.c_double, C.c_double,
+                                     C.POINTER(C.c_int64)]),
+    "vpfft_batch_step": (C.c_int, [_G, C.POINTER(C.c_int)]),
+    "vpfft_batch_run": (C.c_int, [_G]),
+    "vpfft_batch_poll": (C.c_int, [_G, C.POINTER(BatchResult), C.c_int, C.POINTER(C.c_int)]),
+    "vpfft_batch_cancel": (C.c_int, [_G, C.c_int64]),
+    "vpfft_batch_get_info": (C.c_int, [_G, C.POINTER(BatchInfo)]),
+    "vpfft_batch_last_error": (C.c_char_p, [_G]),
     "vpfft_config_read": (C.c_int, [C.c_char_p, C.POINTER(Config), C.c_char_p, C.c_size_t]),
 }
 

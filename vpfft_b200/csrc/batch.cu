@@ -1,0 +1,726 @@
+// batch.cu -- the batch engine: many RVEs (grids of different sizes) advanced
+// together, one kernel launch per phase over every RVE in that phase, with
+// continuous admission of new requests between ticks.
+//
+// A request is one increment (RunSingleStrainStep, MaterialGrid.cpp:897-1084)
+// on a caller-owned grid.  Its life in the batch:
+//   queued  -> admitted when a slot is free and its two spectrum buffers fit
+//              the HBM budget (first-fit in one arena allocated at creation);
+//   INIT    -> batched initialisation + reference medium; after the tick the
+//              host forms L0, inverse(-L0) and the Newton constants exactly as
+//              the single-grid path does;
+//   ITER    -> the tick's fixed-point iterations (five FFT passes with the
+//              Green operator, NR sweep, per-slot reductions), each kernel one
+//              launch over all iterating slots; a slot whose loop has finished
+//              lets its blocks return at once;
+//   done    -> batched texture/hardening update, result recorded, slot and
+//              arena space released.
+// The per-slot block counts of the persistent kernels equal the single-grid
+// launches', so every slot's sums are formed in the same order as when it is
+// solved alone.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "grid.h"
+
+using namespace vpfft;
+using namespace vpfft::grid_ops;
+
+namespace {
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+thread_local std::string g_batch_err;
+
+// First-fit allocator over [0, size) with 256-byte granules (host bookkeeping
+// of the device arena).
+class Arena {
+ public:
+  explicit Arena(size_t size = 0) : size_(size) {}
+  bool alloc(size_t bytes, size_t* off) {
+    bytes = (bytes + 255) & ~size_t(255);
+    size_t pos = 0;
+    for (auto it = used_.begin(); it != used_.end(); ++it) {
+      if (it->first - pos >= bytes) break;
+      pos = it->first + it->second;
+    }
+    if (pos + bytes > size_) return false;
+    used_[pos] = bytes;
+    in_use_ += bytes;
+    *off = pos;
+    return true;
+  }
+  void release(size_t off) {
+    auto it = used_.find(off);
+    if (it == used_.end()) return;
+    in_use_ -= it->second;
+    used_.erase(it);
+  }
+  size_t in_use() const { return in_use_; }
+  size_t size() const { return size_; }
+
+ private:
+  size_t size_;
+  size_t in_use_ = 0;
+  std::map<size_t, size_t> used_;  // offset -> bytes
+};
+
+enum Phase { kInit = 0, kIter = 1, kDone = 2 };
+
+struct Request {
+  int64_t id = 0;
+  vpfft_grid* g = nullptr;
+  double edot[5] = {0};
+  int max_iter = 100;
+  double dt = 0;
+  double eps = 0;
+  double t_submit = 0;
+  double t_admit = 0;
+  bool cancelled = false;
+};
+
+struct Active {
+  Request r;
+  int slot = -1;
+  size_t off = 0;  // arena offset of X (X2 follows)
+  Phase phase = kInit;
+  bool tau = false;  // per-voxel CRSS
+};
+
+// Host mirror of one device block list: slots and cumulative block counts.
+struct HostList {
+  std::vector<int> slot, prefix{0};
+  void clear() {
+    slot.clear();
+    prefix.assign(1, 0);
+  }
+  void add(int s, int blocks) {
+    slot.push_back(s);
+    prefix.push_back(prefix.back() + blocks);
+  }
+  int m() const { return (int)slot.size(); }
+  int blocks() const { return prefix.back(); }
+};
+
+// Device copy of a set of lists, packed into one buffer, staged through a
+// pinned host buffer (so the upload does not wait for the stream).
+struct DeviceLists {
+  int* d = nullptr;
+  int* h = nullptr;
+  int cap = 0;  // ints
+};
+
+}  // namespace
+
+struct vpfft_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  vpfft_precision prec = VPFFT_PREC_MIXED;
+  vpfft_material mat{};
+  vpfft_solver_options opt{};
+  vpfft_batch_options bopt{};
+  int nexp = 0;
+  // device memory
+  void* arena_base = nullptr;
+  Arena arena;
+  void* d_desc = nullptr;     // SlotDesc<S>[max_slots]
+  IterCtrl* d_ctrl = nullptr; // IterCtrl[max_slots]
+  double* d_sum25 = nullptr;  // 25 per slot
+  DeviceLists setup_lists, iter_lists;
+  // pinned host copies
+  IterCtrl* h_ctrl = nullptr;
+  double* h_sum25 = nullptr;
+  // bookkeeping
+  unsigned char* h_desc = nullptr;  // SlotDesc<S>[max_slots] host images (pinned)
+  std::vector<int> free_slots;
+  std::deque<Request> queue;
+  std::vector<Active> active;
+  std::deque<vpfft_batch_result> results;
+  int64_t next_id = 1;
+  int64_t ticks = 0, graph_replays = 0, launches = 0, completed = 0, deferred = 0;
+  // captured iteration chunk
+  uint64_t iter_generation = 1, graph_generation = 0, eager_generation = 0;
+  cudaGraphExec_t graph = nullptr;
+  std::string err;
+};
+
+namespace {
+
+vpfft_status bfail(vpfft_batch* b, vpfft_status s, const std::string& msg) {
+  if (b)
+    b->err = msg;
+  else
+    g_batch_err = msg;
+  return s;
+}
+
+#define BCK(b, call)                                                                       \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return bfail((b), e_ == cudaErrorMemoryAllocation ? VPFFT_ERR_OUT_OF_MEMORY          \
+                                                        : VPFFT_ERR_CUDA,                  \
+                   std::string(#call) + ": " + cudaGetErrorString(e_));                    \
+  } while (0)
+
+template <typename S>
+SlotDesc<S>* host_desc(vpfft_batch* b, int slot) {
+  return reinterpret_cast<SlotDesc<S>*>(b->h_desc) + slot;
+}
+template <typename S>
+SlotDesc<S>* dev_desc(vpfft_batch* b) {
+  return reinterpret_cast<SlotDesc<S>*>(b->d_desc);
+}
+
+// Uploads host lists into a device buffer; returns BatchLaunch views.
+vpfft_status upload_lists(vpfft_batch* b, DeviceLists& dl, const std::vector<HostList*>& lists,
+                          std::vector<BatchLaunch>& out) {
+  size_t need = 0;
+  for (const HostList* l : lists) need += l->slot.size() + l->prefix.size();
+  if ((int)need > dl.cap) {
+    BCK(b, cudaStreamSynchronize(b->stream));
+    if (dl.d) cudaFree(dl.d);
+    if (dl.h) cudaFreeHost(dl.h);
+    dl.d = nullptr;
+    dl.h = nullptr;
+    dl.cap = 0;
+    const int cap = (int)std::max<size_t>(need, 64) * 2;
+    BCK(b, cudaMalloc(&dl.d, sizeof(int) * cap));
+    BCK(b, cudaMallocHost(&dl.h, sizeof(int) * cap));
+    dl.cap = cap;
+  }
+  size_t pos = 0;
+  out.clear();
+  for (const HostList* l : lists) {
+    BatchLaunch bl;
+    bl.slot = dl.d + pos;
+    std::copy(l->slot.begin(), l->slot.end(), dl.h + pos);
+    pos += l->slot.size();
+    bl.prefix = dl.d + pos;
+    std::copy(l->prefix.begin(), l->prefix.end(), dl.h + pos);
+    pos += l->prefix.size();
+    bl.m = l->m();
+    bl.blocks = l->blocks();
+    out.push_back(bl);
+  }
+  if (pos)
+    BCK(b, cudaMemcpyAsync(dl.d, dl.h, sizeof(int) * pos, cudaMemcpyHostToDevice, b->stream));
+  return VPFFT_OK;
+}
+
+template <typename S>
+vpfft_status upload_desc(vpfft_batch* b, int slot) {
+  BCK(b, cudaMemcpyAsync(dev_desc<S>(b) + slot, host_desc<S>(b, slot), sizeof(SlotDesc<S>),
+                         cudaMemcpyHostToDevice, b->stream));
+  return VPFFT_OK;
+}
+
+vpfft_status upload_ctrl(vpfft_batch* b, int slot) {
+  BCK(b, cudaMemcpyAsync(b->d_ctrl + slot, b->h_ctrl + slot, sizeof(IterCtrl),
+                         cudaMemcpyHostToDevice, b->stream));
+  return VPFFT_OK;
+}
+
+void release(vpfft_batch* b, Active& a) {
+  b->arena.release(a.off);
+  b->free_slots.push_back(a.slot);
+  a.r.g->in_batch = false;
+}
+
+void record(vpfft_batch* b, const Active& a, vpfft_status st, double t_end) {
+  vpfft_batch_result r{};
+  r.request_id = a.r.id;
+  r.status = st;
+  const IterCtrl& c = b->h_ctrl[a.slot];
+  if (a.phase != kInit) {
+    r.iterations = c.iter;
+    r.converged = (c.last[10] <= a.r.eps && c.last[11] <= a.r.eps) ? 1 : 0;
+    for (int k = 0; k < 5; ++k) r.avg_stress[k] = c.last[k];
+    r.stress_error = c.last[10];
+    r.strain_rate_error = c.last[11];
+    r.nr_not_converged = (int64_t)c.nr_capped;
+  }
+  r.seconds_queued = a.r.t_admit - a.r.t_submit;
+  r.seconds_total = t_end - a.r.t_submit;
+  b->results.push_back(r);
+  b->completed++;
+}
+
+// Admission: FIFO over the queue; a request whose grid is busy waits without
+// blocking the others; the first request that does not fit the budget stops
+// admission for this tick.
+template <typename S>
+vpfft_status admit(vpfft_batch* b, std::vector<int>& admitted) {
+  for (auto it = b->queue.begin(); it != b->queue.end();) {
+    if (b->free_slots.empty()) break;
+    vpfft_grid* g = it->g;
+    if (g->in_batch) {
+      ++it;
+      continue;
+    }
+    const size_t spec = spectrum_bytes(g);
+    const size_t spec_al = (spec + 255) & ~size_t(255);
+    size_t off = 0;
+    if (!b->arena.alloc(2 * spec_al, &off)) {
+      b->deferred++;
+      break;
+    }
+    Active a;
+    a.r = *it;
+    a.r.t_admit = now_s();
+    a.off = off;
+    a.slot = b->free_slots.back();
+    b->free_slots.pop_back();
+    a.phase = kInit;
+    g->in_batch = true;
+    if (vpfft_status s = ensure_hist(g, a.r.max_iter)) {
+      release(b, a);
+      return bfail(b, s, g->err);
+    }
+    if (vpfft_status s = ensure_crss_array(g)) {
+      release(b, a);
+      return bfail(b, s, g->err);
+    }
+    a.tau = g->crss_per_voxel;
+    char* base = static_cast<char*>(b->arena_base) + off;
+    SlotDesc<S>& d = *host_desc<S>(b, a.slot);
+    d = SlotDesc<S>{};
+    d.nr_init = nr_params(g, a.r.edot, true);
+    d.vox = voxel_params(g, a.r.edot);
+    d.f = fields<S>(g);
+    d.sp = spectral<S>(g, base, base + spec_al);
+    d.crss_out = (S*)g->crss;
+    d.partials = g->partials;
+    d.sum25 = b->d_sum25 + 25 * (size_t)a.slot;
+    d.ctrl = b->d_ctrl + a.slot;
+    d.hist = g->hist;
+    d.init_blocks = nr_launch_blocks<S>(d.nr_init, a.tau, true);
+    IterCtrl& c = b->h_ctrl[a.slot];
+    c = IterCtrl{};
+    c.n_voxels = (double)g->n;
+    if (vpfft_status s = upload_ctrl(b, a.slot)) return s;
+    if (vpfft_status s = upload_desc<S>(b, a.slot)) return s;
+    for (int k = 0; k < 5; ++k) g->last_edot[k] = a.r.edot[k];
+    admitted.push_back((int)b->active.size());
+    b->active.push_back(a);
+    it = b->queue.erase(it);
+  }
+  return VPFFT_OK;
+}
+
+// After the INIT tick: L0 and the loop constants of an admitted slot.
+template <typename S>
+vpfft_status start_loop(vpfft_batch* b, Active& a) {
+  vpfft_grid* g = a.r.g;
+  SlotDesc<S>& d = *host_desc<S>(b, a.slot);
+  if (vpfft_status s = finish_ref_medium(g, b->h_sum25 + 25 * (size_t)a.slot)) return s;
+  d.nr = nr_params(g, a.r.edot, false);
+  d.gp = green_params<S>(g->nx, g->ny, g->nz, g->h, g->L0, g->Linv);
+  d.post = post_params(g, a.r.dt);
+  d.nr_blocks = nr_launch_blocks<S>(d.nr, a.tau, false);
+  b->h_ctrl[a.slot] = loop_ctrl(g, a.r.edot, a.r.max_iter, a.r.eps);
+  if (vpfft_status s = upload_ctrl(b, a.slot)) return s;
+  if (vpfft_status s = upload_desc<S>(b, a.slot)) return s;
+  a.phase = kIter;
+  b->iter_generation++;
+  return VPFFT_OK;
+}
+
+// The iteration lists of the slots in ITER phase.
+struct IterLists {
+  HostList z, y, x, nr[2], fin[2];
+  SpectralShape smax{};
+};
+
+template <typename S>
+void build_iter_lists(vpfft_batch* b, IterLists& L) {
+  L.smax = SpectralShape{};
+  for (const Active& a : b->active) {
+    if (a.phase != kIter) continue;
+    const SlotDesc<S>& d = *host_desc<S>(b, a.slot);
+    const SpectralShape sh = spectral_shape<S>(d.sp, 5);
+    L.z.add(a.slot, sh.blocks_z);
+    L.y.add(a.slot, sh.blocks_y);
+    L.x.add(a.slot, sh.blocks_x);
+    L.nr[a.tau].add(a.slot, d.nr_blocks);
+    L.fin[a.tau].add(a.slot, 1);
+    L.smax.smem_z_r2c = std::max(L.smax.smem_z_r2c, sh.smem_z_r2c);
+    L.smax.smem_z_c2r = std::max(L.smax.smem_z_c2r, sh.smem_z_c2r);
+    L.smax.smem_y = std::max(L.smax.smem_y, sh.smem_y);
+    L.smax.smem_x = std::max(L.smax.smem_x, sh.smem_x);
+  }
+}
+
+template <typename S>
+int enqueue_iterations(vpfft_batch* b, const std::vector<BatchLaunch>& bl, const IterLists& L,
+                       int iters) {
+  int n = 0;
+  for (int it = 0; it < iters; ++it) {
+    n += launch_spectral_batch<S>(dev_desc<S>(b), bl[0], bl[1], bl[2], L.smax, b->stream);
+    for (int t = 0; t < 2; ++t)
+      n += launch_nr_update_batch<S>(dev_desc<S>(b), bl[3 + t], bl[5 + t], b->nexp, t == 1,
+                                     b->stream);
+  }
+  return n;
+}
+
+// The tick's iterations.  While the set of iterating slots stays the same the
+// launches are replayed from a CUDA graph: the first chunk of a new set runs
+// eagerly (it also sets the kernels' shared-memory attributes), the second is
+// captured and launched, later ones replay it.
+template <typename S>
+vpfft_status run_iterations(vpfft_batch* b) {
+  IterLists L;
+  build_iter_lists<S>(b, L);
+  if (L.z.m() == 0) return VPFFT_OK;
+  const int iters = std::max(1, b->bopt.iterations_per_tick);
+  if (b->bopt.use_graphs && b->graph && b->graph_generation == b->iter_generation) {
+    BCK(b, cudaGraphLaunch(b->graph, b->stream));
+    b->graph_replays++;
+    return VPFFT_OK;
+  }
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  std::vector<HostList*> lists = {&L.z, &L.y, &L.x, &L.nr[0], &L.nr[1], &L.fin[0], &L.fin[1]};
+  std::vector<BatchLaunch> bl;
+  if (vpfft_status s = upload_lists(b, b->iter_lists, lists, bl)) return s;
+  if (b->bopt.use_graphs && b->eager_generation == b->iter_generation) {
+    cudaGraph_t graph = nullptr;
+    BCK(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    const int n = enqueue_iterations<S>(b, bl, L, iters);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+    if (e != cudaSuccess)
+      return bfail(b, VPFFT_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&b->graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess)
+      return bfail(b, VPFFT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    b->graph_generation = b->iter_generation;
+    BCK(b, cudaGraphLaunch(b->graph, b->stream));
+    b->graph_replays++;
+    b->launches += n;
+    return VPFFT_OK;
+  }
+  b->launches += enqueue_iterations<S>(b, bl, L, iters);
+  b->eager_generation = b->iter_generation;
+  BCK(b, cudaGetLastError());
+  return VPFFT_OK;
+}
+
+template <typename S>
+vpfft_status tick(vpfft_batch* b) {
+  BCK(b, cudaSetDevice(b->device));
+  b->ticks++;
+  // cancelled requests still queued complete at once
+  for (auto it = b->queue.begin(); it != b->queue.end();) {
+    if (it->cancelled) {
+      Active a;
+      a.r = *it;
+      a.slot = -1;
+      vpfft_batch_result r{};
+      r.request_id = it->id;
+      r.status = VPFFT_ERR_CANCELLED;
+      r.seconds_total = now_s() - it->t_submit;
+      b->results.push_back(r);
+      b->completed++;
+      it = b->queue.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  // cancelled active requests leave before any work of this tick
+  for (size_t i = 0; i < b->active.size();) {
+    Active& a = b->active[i];
+    if (a.r.cancelled) {
+      record(b, a, VPFFT_ERR_CANCELLED, now_s());
+      if (a.phase == kIter) b->iter_generation++;
+      release(b, a);
+      b->active.erase(b->active.begin() + i);
+    } else {
+      ++i;
+    }
+  }
+  // 1. admission and the initialisation of the new slots
+  std::vector<int> admitted;
+  if (vpfft_status s = admit<S>(b, admitted)) return s;
+  if (!admitted.empty()) {
+    HostList init[2], rm, rms;
+    for (int idx : admitted) {
+      const Active& a = b->active[idx];
+      const SlotDesc<S>& d = *host_desc<S>(b, a.slot);
+      init[a.tau].add(a.slot, d.init_blocks);
+      rm.add(a.slot, (int)((d.vox.n + 127) / 128));
+      rms.add(a.slot, 1);
+    }
+    std::vector<BatchLaunch> bl;
+    if (vpfft_status s = upload_lists(b, b->setup_lists, {&init[0], &init[1], &rm, &rms}, bl))
+      return s;
+    for (int t = 0; t < 2; ++t)
+      b->launches += launch_init_batch<S>(dev_desc<S>(b), bl[t], b->nexp, t == 1, b->stream);
+    b->launches += launch_ref_medium_batch<S>(dev_desc<S>(b), bl[2], bl[3], b->stream);
+    BCK(b, cudaGetLastError());
+  }
+  // 2. the iterations of the slots already iterating
+  if (vpfft_status s = run_iterations<S>(b)) return s;
+  // 3. read back control blocks and reference-medium sums
+  const int ms = b->bopt.max_slots;
+  BCK(b, cudaMemcpyAsync(b->h_ctrl, b->d_ctrl, sizeof(IterCtrl) * ms, cudaMemcpyDeviceToHost,
+                         b->stream));
+  BCK(b, cudaMemcpyAsync(b->h_sum25, b->d_sum25, sizeof(double) * 25 * ms,
+                         cudaMemcpyDeviceToHost, b->stream));
+  BCK(b, cudaStreamSynchronize(b->stream));
+  const double t_now = now_s();
+  // 4. finished loops: post-increment update (one launch) and results
+  HostList post;
+  std::vector<size_t> finishing;
+  for (size_t i = 0; i < b->active.size(); ++i) {
+    Active& a = b->active[i];
+    const IterCtrl& c = b->h_ctrl[a.slot];
+    if (a.phase != kIter || !c.done) continue;
+    if (c.status & (kStatusNonFinite | kStatusMaxRssTiny)) continue;  // no post on error
+    post.add(a.slot, (int)((a.r.g->n + 127) / 128));
+    finishing.push_back(i);
+  }
+  if (post.m()) {
+    std::vector<BatchLaunch> bl;
+    if (vpfft_status s = upload_lists(b, b->setup_lists, {&post}, bl)) return s;
+    b->launches += launch_post_batch<S>(dev_desc<S>(b), bl[0], b->stream);
+    BCK(b, cudaGetLastError());
+    BCK(b, cudaStreamSynchronize(b->stream));
+  }
+  // 5. phase transitions
+  const double t_end = now_s();
+  std::vector<Active> keep;
+  keep.reserve(b->active.size());
+  for (Active& a : b->active) {
+    const IterCtrl& c = b->h_ctrl[a.slot];
+    if (a.phase == kInit) {
+      vpfft_status st = VPFFT_OK;
+      if (c.status & kStatusNonFinite) st = VPFFT_ERR_NONFINITE;
+      else if (c.status & kStatusMaxRssTiny) st = VPFFT_ERR_MAX_RSS_TINY;
+      if (st == VPFFT_OK) st = start_loop<S>(b, a);
+      if (st != VPFFT_OK) {
+        record(b, a, st, t_now);
+        release(b, a);
+        continue;
+      }
+      keep.push_back(a);
+    } else if (a.phase == kIter && c.done) {
+      vpfft_status st = VPFFT_OK;
+      if (c.status & kStatusNonFinite) st = VPFFT_ERR_NONFINITE;
+      else if (c.status & kStatusMaxRssTiny) st = VPFFT_ERR_MAX_RSS_TINY;
+      if (st == VPFFT_OK) finish_post(a.r.g, a.r.edot, a.r.dt);
+      record(b, a, st, t_end);
+      b->iter_generation++;
+      release(b, a);
+    } else {
+      keep.push_back(a);
+    }
+  }
+  b->active.swap(keep);
+  return VPFFT_OK;
+}
+
+void free_batch(vpfft_batch* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  void* ptrs[] = {b->arena_base, b->d_desc, b->d_ctrl, b->d_sum25, b->setup_lists.d,
+                  b->iter_lists.d};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  void* hptrs[] = {b->h_ctrl, b->h_sum25, b->h_desc, b->setup_lists.h, b->iter_lists.h};
+  for (void* p : hptrs)
+    if (p) cudaFreeHost(p);
+  if (b->stream) cudaStreamDestroy(b->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+void vpfft_batch_options_default(vpfft_batch_options* o) {
+  if (!o) return;
+  o->max_slots = 256;
+  o->iterations_per_tick = 8;
+  o->hbm_budget_bytes = 8LL << 30;
+  o->use_graphs = 1;
+  o->pad_ = 0;
+}
+
+vpfft_status vpfft_batch_create(vpfft_precision precision, const vpfft_material* material,
+                                const vpfft_solver_options* options,
+                                const vpfft_batch_options* bopt, vpfft_batch** out) {
+  if (!out) return bfail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "out is NULL");
+  *out = nullptr;
+  if (precision != VPFFT_PREC_FP64 && precision != VPFFT_PREC_MIXED)
+    return bfail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "unknown precision");
+  int cnt = 0;
+  if (cudaGetDeviceCount(&cnt) != cudaSuccess || cnt <= 0) {
+    cudaGetLastError();
+    return bfail(nullptr, VPFFT_ERR_NO_DEVICE,
+                 "no CUDA device available (vpfft_b200 has no CPU fallback)");
+  }
+  vpfft_batch* b = new vpfft_batch();
+  b->prec = precision;
+  if (material)
+    b->mat = *material;
+  else
+    vpfft_material_default(&b->mat);
+  if (options)
+    b->opt = *options;
+  else
+    vpfft_solver_options_default(&b->opt);
+  if (bopt)
+    b->bopt = *bopt;
+  else
+    vpfft_batch_options_default(&b->bopt);
+  if (b->bopt.max_slots < 1 || b->bopt.max_slots > 65536 || b->bopt.hbm_budget_bytes < 0) {
+    delete b;
+    return bfail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "bad batch options");
+  }
+  {
+    NRParams p{};
+    for (int q = 0; q < kNS; ++q) p.nexp[q] = b->mat.rate_sensitivity[q];
+    b->nexp = uniform_exponent(p);
+  }
+  cudaGetDevice(&b->device);
+  auto bail = [&](cudaError_t e, const char* what) {
+    g_batch_err = std::string(what) + ": " + cudaGetErrorString(e);
+    free_batch(b);
+    delete b;
+    return e == cudaErrorMemoryAllocation ? VPFFT_ERR_OUT_OF_MEMORY : VPFFT_ERR_CUDA;
+  };
+  const int ms = b->bopt.max_slots;
+  const size_t desc_bytes = precision == VPFFT_PREC_FP64 ? sizeof(SlotDesc<double>)
+                                                         : sizeof(SlotDesc<float>);
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return bail(e, "stream");
+  if (b->bopt.hbm_budget_bytes > 0 &&
+      (e = cudaMalloc(&b->arena_base, (size_t)b->bopt.hbm_budget_bytes)) != cudaSuccess)
+    return bail(e, "arena");
+  b->arena = Arena((size_t)b->bopt.hbm_budget_bytes);
+  if ((e = cudaMalloc(&b->d_desc, desc_bytes * ms)) != cudaSuccess) return bail(e, "descriptors");
+  if ((e = cudaMalloc(&b->d_ctrl, sizeof(IterCtrl) * ms)) != cudaSuccess) return bail(e, "ctrl");
+  if ((e = cudaMalloc(&b->d_sum25, sizeof(double) * 25 * ms)) != cudaSuccess) return bail(e, "sums");
+  if ((e = cudaMallocHost(&b->h_ctrl, sizeof(IterCtrl) * ms)) != cudaSuccess) return bail(e, "pinned");
+  if ((e = cudaMallocHost(&b->h_sum25, sizeof(double) * 25 * ms)) != cudaSuccess)
+    return bail(e, "pinned");
+  std::memset(b->h_ctrl, 0, sizeof(IterCtrl) * ms);
+  if ((e = cudaMemset(b->d_ctrl, 0, sizeof(IterCtrl) * ms)) != cudaSuccess) return bail(e, "ctrl");
+  if ((e = cudaMallocHost(&b->h_desc, desc_bytes * ms)) != cudaSuccess) return bail(e, "pinned");
+  std::memset(b->h_desc, 0, desc_bytes * ms);
+  for (int s = ms - 1; s >= 0; --s) b->free_slots.push_back(s);
+  *out = b;
+  return VPFFT_OK;
+}
+
+vpfft_status vpfft_batch_destroy(vpfft_batch* b) {
+  if (!b) return VPFFT_OK;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (Active& a : b->active) a.r.g->in_batch = false;
+  free_batch(b);
+  delete b;
+  return VPFFT_OK;
+}
+
+vpfft_status vpfft_batch_submit(vpfft_batch* b, vpfft_grid* g, const double edot[5], int max_iter,
+                                double dt, double eps, int64_t* id) {
+  if (!b || !g || !edot) return bfail(b, VPFFT_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (g->prec != b->prec) return bfail(b, VPFFT_ERR_INVALID_ARGUMENT, "grid precision differs from the batch's");
+  if (g->device != b->device) return bfail(b, VPFFT_ERR_INVALID_ARGUMENT, "grid lives on another device");
+  if (std::memcmp(&g->mat, &b->mat, sizeof(vpfft_material)) != 0 ||
+      std::memcmp(&g->opt, &b->opt, sizeof(vpfft_solver_options)) != 0)
+    return bfail(b, VPFFT_ERR_INVALID_ARGUMENT, "grid material or solver options differ from the batch's");
+  if (!g->fields_set) return bfail(b, VPFFT_ERR_NOT_INITIALIZED, "grid fields not set");
+  if (max_iter < 1) return bfail(b, VPFFT_ERR_INVALID_ARGUMENT, "max_iter must be >= 1");
+  const size_t need = 2 * ((spectrum_bytes(g) + 255) & ~size_t(255));
+  if (need > b->arena.size())
+    return bfail(b, VPFFT_ERR_OUT_OF_MEMORY, "the grid's spectra exceed the batch's HBM budget");
+  Request r;
+  r.id = b->next_id++;
+  r.g = g;
+  std::memcpy(r.edot, edot, sizeof(r.edot));
+  r.max_iter = max_iter;
+  r.dt = dt;
+  r.eps = eps;
+  r.t_submit = now_s();
+  b->queue.push_back(r);
+  if (id) *id = r.id;
+  return VPFFT_OK;
+}
+
+vpfft_status vpfft_batch_step(vpfft_batch* b, int* pending) {
+  if (!b) return bfail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "NULL batch");
+  vpfft_status s = b->prec == VPFFT_PREC_FP64 ? tick<double>(b) : tick<float>(b);
+  if (pending) *pending = (int)(b->queue.size() + b->active.size());
+  return s;
+}
+
+vpfft_status vpfft_batch_run(vpfft_batch* b) {
+  if (!b) return bfail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "NULL batch");
+  int pending = 1;
+  while (pending > 0) {
+    vpfft_status s = vpfft_batch_step(b, &pending);
+    if (s != VPFFT_OK) return s;
+  }
+  return VPFFT_OK;
+}
+
+vpfft_status vpfft_batch_poll(vpfft_batch* b, vpfft_batch_result* out, int cap, int* n_out) {
+  if (!b || (!out && cap > 0)) return bfail(b, VPFFT_ERR_INVALID_ARGUMENT, "NULL argument");
+  int n = 0;
+  while (n < cap && !b->results.empty()) {
+    out[n++] = b->results.front();
+    b->results.pop_front();
+  }
+  if (n_out) *n_out = n;
+  return VPFFT_OK;
+}
+
+vpfft_status vpfft_batch_cancel(vpfft_batch* b, int64_t id) {
+  if (!b) return bfail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "NULL batch");
+  for (Request& r : b->queue)
+    if (r.id == id) {
+      r.cancelled = true;
+      return VPFFT_OK;
+    }
+  for (Active& a : b->active)
+    if (a.r.id == id) {
+      a.r.cancelled = true;
+      return VPFFT_OK;
+    }
+  return bfail(b, VPFFT_ERR_INVALID_ARGUMENT, "no such pending request");
+}
+
+vpfft_status vpfft_batch_get_info(const vpfft_batch* b, vpfft_batch_info* info) {
+  if (!b || !info) return VPFFT_ERR_INVALID_ARGUMENT;
+  info->queued = (int64_t)b->queue.size();
+  info->active = (int64_t)b->active.size();
+  info->completed = b->completed;
+  info->ticks = b->ticks;
+  info->graph_replays = b->graph_replays;
+  info->kernel_launches = b->launches;
+  info->arena_bytes_in_use = (int64_t)b->arena.in_use();
+  info->arena_bytes = (int64_t)b->arena.size();
+  info->admissions_deferred_for_memory = b->deferred;
+  return VPFFT_OK;
+}
+
+const char* vpfft_batch_last_error(const vpfft_batch* b) {
+  return b ? b->err.c_str() : g_batch_err.c_str();
+}
+
+}  // extern "C"

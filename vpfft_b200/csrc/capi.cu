@@ -16,57 +16,10 @@
 #include <string>
 #include <vector>
 
-#include "../../include/vpfft_capi.h"
-#include "kernels.h"
+#include "grid.h"
 
 using namespace vpfft;
-
-struct vpfft_grid {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  int nx = 0, ny = 0, nz = 0, nh = 0;
-  long long n = 0;
-  vpfft_precision prec = VPFFT_PREC_FP64;
-  vpfft_material mat{};
-  vpfft_solver_options opt{};
-  double h[3] = {1, 1, 1};
-  bool fields_set = false;
-  bool crss_per_voxel = false;
-  bool keep_d = false;
-  bool have_L0 = false;
-  LinePlan px{}, py{}, pz{};
-  // device storage (element type = double for FP64, float for MIXED)
-  void* R = nullptr;
-  void* sigma = nullptr;
-  void* lambda = nullptr;
-  void* work = nullptr;
-  void* dkeep = nullptr;
-  void* crss = nullptr;
-  double* acc = nullptr;
-  void* X = nullptr;   // A: spectrum after the z pass
-  void* X2 = nullptr;  // B: spectrum after the y pass
-  void* twx = nullptr;
-  void* twy = nullptr;
-  void* twz = nullptr;
-  double* partials = nullptr;
-  double* sum25 = nullptr;
-  double* staging = nullptr;  // voxel-major FP64 copy of one host field (N x 12 max)
-  IterCtrl* ctrl = nullptr;
-  IterCtrl* h_ctrl = nullptr;  // pinned
-  double* hist = nullptr;
-  int hist_cap = 0;
-  double L0[25] = {0};
-  double Linv[25] = {0};      // inverse(-L0): the Nyquist-plane operator
-  double L0inv_sym[15] = {0}; // symmetric part of L0^-1, packed (Newton step)
-  double last_edot[5] = {0};
-  long long launches = 0;
-  // per-kernel device timing of the fixed-point loop (vpfft_grid_set_profiling)
-  bool profile = false;
-  std::vector<cudaEvent_t> ev;
-  double phase_ms[VPFFT_NUM_PHASES] = {0};
-  int64_t phase_n[VPFFT_NUM_PHASES] = {0};
-  std::string err;
-};
+using namespace vpfft::grid_ops;
 
 namespace {
 
@@ -93,6 +46,10 @@ vpfft_status fail(vpfft_grid* g, vpfft_status s, const std::string& msg) {
   } while (0)
 
 #define CKL(g) CK(g, cudaGetLastError())
+
+vpfft_status busy(vpfft_grid* g) {
+  return fail(g, VPFFT_ERR_BUSY, "the grid has a request in flight in a batch");
+}
 
 vpfft_status need_device(vpfft_grid* g) {
   int cnt = 0;
@@ -170,29 +127,12 @@ vpfft_status lib_fail(vpfft_status s, const std::string& msg) { return fail(null
 
 namespace {
 
-MaterialParams mat_params(const vpfft_material& m) {
-  MaterialParams p;
-  for (int k = 0; k < kNS; ++k) {
-    p.gdot[k] = m.gamma_dot_base[k];
-    p.nexp[k] = m.rate_sensitivity[k];
-  }
-  return p;
-}
+}  // namespace
 
-template <typename S>
-FieldPtrs<S> fields(vpfft_grid* g) {
-  FieldPtrs<S> f;
-  f.R = (S*)g->R;
-  f.sigma = (S*)g->sigma;
-  f.lambda = (S*)g->lambda;
-  f.work = (S*)g->work;
-  f.dkeep = g->keep_d ? (S*)g->dkeep : nullptr;
-  f.crss = g->crss_per_voxel ? (S*)g->crss : nullptr;
-  f.acc = g->acc;
-  return f;
-}
+namespace vpfft {
+namespace grid_ops {
 
-VoxelParams voxel_params(vpfft_grid* g, const double edot[5]) {
+VoxelParams voxel_params(const vpfft_grid* g, const double edot[5]) {
   VoxelParams p{};
   p.n = g->n;
   for (int c = 0; c < 5; ++c) p.edot[c] = edot[c];
@@ -216,7 +156,7 @@ VoxelParams voxel_params(vpfft_grid* g, const double edot[5]) {
 
 // Launch constants of the Newton kernels: the initialisation solve
 // (InitializeComputation, MaterialGrid.cpp:159-166) or the loop solve (909-911).
-NRParams nr_params(vpfft_grid* g, const double edot[5], bool init) {
+NRParams nr_params(const vpfft_grid* g, const double edot[5], bool init) {
   VoxelParams v = voxel_params(g, edot);
   NRParams p{};
   p.n = g->n;
@@ -241,39 +181,100 @@ NRParams nr_params(vpfft_grid* g, const double edot[5], bool init) {
   return p;
 }
 
-template <typename S>
-GreenParams<S> green_params(int nx, int ny, int nz, const double h[3], const double* L0,
-                            const double* Linv) {
-  GreenParams<S> gp{};
-  gp.nx = nx;
-  gp.ny = ny;
-  gp.nz = nz;
-  gp.inv_len[0] = (S)(1.0 / (nx * h[0]));
-  gp.inv_len[1] = (S)(1.0 / (ny * h[1]));
-  gp.inv_len[2] = (S)(1.0 / (nz * h[2]));
-  for (int k = 0; k < 25; ++k) {
-    gp.L0[k] = (S)L0[k];
-    gp.Linv[k] = (S)Linv[k];
+PostParams post_params(const vpfft_grid* g, double dt) {
+  PostParams p{};
+  p.n = g->n;
+  p.dt = dt;
+  p.mat = mat_params(g->mat);
+  for (int k = 0; k < kNS; ++k) {
+    p.crss[k] = g->mat.crss[k];
+    p.tau0[k] = g->mat.tau0[k];
+    p.tau1[k] = g->mat.tau1[k];
+    p.theta0[k] = g->mat.theta0[k];
+    p.theta1[k] = g->mat.theta1[k];
   }
-  return gp;
+  for (int k = 0; k < kNS * kNS; ++k) p.H[k] = g->mat.hardening[k];
+  return p;
 }
 
-template <typename S>
-Spectral<S> spectral(vpfft_grid* g) {
-  Spectral<S> sp;
-  sp.nx = g->nx;
-  sp.ny = g->ny;
-  sp.nz = g->nz;
-  sp.nh = g->nh;
-  sp.px = g->px;
-  sp.py = g->py;
-  sp.pz = g->pz;
-  sp.twx = g->twx;
-  sp.twy = g->twy;
-  sp.twz = g->twz;
-  sp.X = g->X;
-  sp.X2 = g->X2;
-  return sp;
+vpfft_status grid_fail(vpfft_grid* g, vpfft_status s, const std::string& msg) {
+  return fail(g, s, msg);
+}
+
+vpfft_status finish_ref_medium(vpfft_grid* g, const double sums[25]) {
+  const double N = (double)g->n;
+  for (int k = 0; k < 25; ++k) {
+    double m = sums[k] / N;                        // mean of the per-voxel inverses (H4)
+    double tmp = m * (double)g->nx;                // * DimXLocal   (MaterialGrid.cpp:262)
+    m = tmp / (double)g->nx;                       // / DimX        (269)
+    g->L0[k] = std::fabs(m) < 1e-10 ? 0.0 : m;     // NormalizeValues (LinearAlgebra.h:605-613)
+  }
+  for (int k = 0; k < 25; ++k)
+    if (!std::isfinite(g->L0[k]))
+      return fail(g, VPFFT_ERR_NONFINITE, "reference medium is not finite (singular voxel compliance)");
+  double negL[25];
+  for (int k = 0; k < 25; ++k) negL[k] = -g->L0[k];
+  inverse5_host(negL, g->Linv);  // StrainRateEvolutionWithFFT, MaterialGrid.cpp:628-632
+  double inv[25];
+  inverse5_host(g->L0, inv);
+  for (int i = 0; i < 5; ++i)
+    for (int j = i; j < 5; ++j) g->L0inv_sym[sym5(i, j)] = 0.5 * (inv[j * 5 + i] + inv[i * 5 + j]);
+  g->have_L0 = true;
+  return VPFFT_OK;
+}
+
+void finish_post(vpfft_grid* g, const double edot[5], double dt) {
+  g->crss_per_voxel = true;
+  // UpdateVoxelLength (MaterialGrid.cpp:1190-1196) with Edot as a 3x3 matrix
+  double E[9];
+  vpfft_matrix_from_edot(edot, E);
+  g->h[0] *= (1.0 + E[0] * dt);
+  g->h[1] *= (1.0 + E[4] * dt);
+  g->h[2] *= (1.0 + E[8] * dt);
+}
+
+// like the reference's do { } while (StepsTaken < NumMaxIterations && ...)
+// (MaterialGrid.cpp:930-1068), at least one iteration always runs
+IterCtrl loop_ctrl(const vpfft_grid* g, const double edot[5], int max_iter, double eps) {
+  IterCtrl h{};
+  h.iter = 0;
+  h.done = 0;
+  h.max_iter = max_iter;
+  h.eps = eps;
+  h.edot_norm = std::sqrt(edot[0] * edot[0] + edot[1] * edot[1] + edot[2] * edot[2] +
+                          edot[3] * edot[3] + edot[4] * edot[4]);
+  h.n_voxels = (double)g->n;
+  return h;
+}
+
+vpfft_status ensure_hist(vpfft_grid* g, int max_iter) {
+  if (std::max(max_iter, 1) > g->hist_cap) {
+    if (g->hist) cudaFree(g->hist);
+    g->hist = nullptr;
+    CK(g, cudaMalloc(&g->hist, sizeof(double) * 12 * (size_t)std::max(max_iter, 1)));
+    g->hist_cap = std::max(max_iter, 1);
+  }
+  return VPFFT_OK;
+}
+
+vpfft_status ensure_crss_array(vpfft_grid* g) {
+  const size_t es = g->prec == VPFFT_PREC_FP64 ? sizeof(double) : sizeof(float);
+  if (!g->crss) CK(g, cudaMalloc(&g->crss, es * (size_t)g->n * kNS));
+  return VPFFT_OK;
+}
+
+}  // namespace grid_ops
+}  // namespace vpfft
+
+namespace {
+
+// The spectrum buffers of the single-grid path: allocated on first use and
+// kept (a grid solved only through a batch never allocates them).
+vpfft_status ensure_spectrum(vpfft_grid* g) {
+  const size_t b = spectrum_bytes(g);
+  if (!g->X) CK(g, cudaMalloc(&g->X, b));
+  if (!g->X2) CK(g, cudaMalloc(&g->X2, b));
+  return VPFFT_OK;
 }
 
 template <typename S>
@@ -341,11 +342,6 @@ vpfft_status from_device_field(vpfft_grid* g, const S* src, int width, double* h
   return VPFFT_OK;
 }
 
-template <typename S>
-vpfft_status ensure_crss_array(vpfft_grid* g) {
-  if (!g->crss) CK(g, cudaMalloc(&g->crss, sizeof(S) * (size_t)g->n * kNS));
-  return VPFFT_OK;
-}
 
 // ---------------------------------------------------------------- phases
 template <typename S>
@@ -376,24 +372,7 @@ vpfft_status do_ref_medium(vpfft_grid* g, double* L0_out) {
   double sums[25];
   CK(g, cudaMemcpyAsync(sums, g->sum25, sizeof(sums), cudaMemcpyDeviceToHost, g->stream));
   CK(g, cudaStreamSynchronize(g->stream));
-  const double N = (double)g->n;
-  for (int k = 0; k < 25; ++k) {
-    double m = sums[k] / N;                        // mean of the per-voxel inverses (H4)
-    double tmp = m * (double)g->nx;                // * DimXLocal   (MaterialGrid.cpp:262)
-    m = tmp / (double)g->nx;                       // / DimX        (269)
-    g->L0[k] = std::fabs(m) < 1e-10 ? 0.0 : m;     // NormalizeValues (LinearAlgebra.h:605-613)
-  }
-  for (int k = 0; k < 25; ++k)
-    if (!std::isfinite(g->L0[k]))
-      return fail(g, VPFFT_ERR_NONFINITE, "reference medium is not finite (singular voxel compliance)");
-  double negL[25];
-  for (int k = 0; k < 25; ++k) negL[k] = -g->L0[k];
-  inverse5_host(negL, g->Linv);  // StrainRateEvolutionWithFFT, MaterialGrid.cpp:628-632
-  double inv[25];
-  inverse5_host(g->L0, inv);
-  for (int i = 0; i < 5; ++i)
-    for (int j = i; j < 5; ++j) g->L0inv_sym[sym5(i, j)] = 0.5 * (inv[j * 5 + i] + inv[i * 5 + j]);
-  g->have_L0 = true;
+  if (vpfft_status r = finish_ref_medium(g, sums)) return r;
   if (L0_out) std::memcpy(L0_out, g->L0, sizeof(g->L0));
   return VPFFT_OK;
 }
@@ -402,26 +381,13 @@ template <typename S>
 vpfft_status do_fixed_point(vpfft_grid* g, const double edot[5], int max_iter, double eps,
                             double* history, vpfft_stats* st) {
   if (!g->have_L0) return fail(g, VPFFT_ERR_NOT_INITIALIZED, "reference medium not built");
-  if (std::max(max_iter, 1) > g->hist_cap) {
-    if (g->hist) cudaFree(g->hist);
-    g->hist = nullptr;
-    CK(g, cudaMalloc(&g->hist, sizeof(double) * 12 * (size_t)std::max(max_iter, 1)));
-    g->hist_cap = std::max(max_iter, 1);
-  }
-  // like the reference's do { } while (StepsTaken < NumMaxIterations && ...)
-  // (MaterialGrid.cpp:930-1068), at least one iteration always runs
-  IterCtrl h{};
-  h.iter = 0;
-  h.done = 0;
-  h.max_iter = max_iter;
-  h.eps = eps;
-  h.edot_norm = std::sqrt(edot[0] * edot[0] + edot[1] * edot[1] + edot[2] * edot[2] +
-                          edot[3] * edot[3] + edot[4] * edot[4]);
-  h.n_voxels = (double)g->n;
+  if (vpfft_status r = ensure_hist(g, max_iter)) return r;
+  if (vpfft_status r = ensure_spectrum(g)) return r;
+  IterCtrl h = loop_ctrl(g, edot, max_iter, eps);
   CK(g, cudaMemcpyAsync(g->ctrl, &h, sizeof(h), cudaMemcpyHostToDevice, g->stream));
   NRParams p = nr_params(g, edot, false);
   GreenParams<S> gp = green_params<S>(g->nx, g->ny, g->nz, g->h, g->L0, g->Linv);
-  Spectral<S> sp = spectral<S>(g);
+  Spectral<S> sp = spectral<S>(g, g->X, g->X2);
   FieldPtrs<S> f = fields<S>(g);
   const int batch = g->n >= (1LL << 21) ? 4 : 16;
   constexpr int kEv = 8;  // events per iteration when profiling
@@ -480,29 +446,12 @@ vpfft_status do_fixed_point(vpfft_grid* g, const double edot[5], int max_iter, d
 
 template <typename S>
 vpfft_status do_post(vpfft_grid* g, const double edot[5], double dt) {
-  vpfft_status s = ensure_crss_array<S>(g);
+  vpfft_status s = ensure_crss_array(g);
   if (s != VPFFT_OK) return s;
-  PostParams p{};
-  p.n = g->n;
-  p.dt = dt;
-  p.mat = mat_params(g->mat);
-  for (int k = 0; k < kNS; ++k) {
-    p.crss[k] = g->mat.crss[k];
-    p.tau0[k] = g->mat.tau0[k];
-    p.tau1[k] = g->mat.tau1[k];
-    p.theta0[k] = g->mat.theta0[k];
-    p.theta1[k] = g->mat.theta1[k];
-  }
-  for (int k = 0; k < kNS * kNS; ++k) p.H[k] = g->mat.hardening[k];
+  PostParams p = post_params(g, dt);
   g->launches += launch_post<S>(p, fields<S>(g), (S*)g->crss, g->stream);
   CKL(g);
-  g->crss_per_voxel = true;
-  // UpdateVoxelLength (MaterialGrid.cpp:1190-1196) with Edot as a 3x3 matrix
-  double E[9];
-  vpfft_matrix_from_edot(edot, E);
-  g->h[0] *= (1.0 + E[0] * dt);
-  g->h[1] *= (1.0 + E[4] * dt);
-  g->h[2] *= (1.0 + E[8] * dt);
+  finish_post(g, edot, dt);
   CK(g, cudaStreamSynchronize(g->stream));
   return VPFFT_OK;
 }
@@ -561,6 +510,7 @@ const char* vpfft_status_string(vpfft_status s) {
     case VPFFT_ERR_IO: return "I/O or parse error";
     case VPFFT_ERR_CANCELLED: return "cancelled";
     case VPFFT_ERR_TIMEOUT: return "timeout";
+    case VPFFT_ERR_BUSY: return "grid busy in a batch";
   }
   return "unknown status";
 }
@@ -658,8 +608,6 @@ vpfft_status vpfft_grid_create(int nx, int ny, int nz, const vpfft_material* mat
   CKC(cudaMalloc(&g->work, es * n * 5));
   if (g->keep_d) CKC(cudaMalloc(&g->dkeep, es * n * 5));
   CKC(cudaMalloc(&g->acc, sizeof(double) * n));
-  CKC(cudaMalloc(&g->X, 2 * es * 5 * (size_t)nx * ny * g->nh));
-  CKC(cudaMalloc(&g->X2, 2 * es * 5 * (size_t)nx * ny * g->nh));
   const size_t nparts = (size_t)std::max(nr_blocks(g->n), ref_medium_blocks(g->n));
   CKC(cudaMalloc(&g->partials, sizeof(double) * nparts * 25));
   CKC(cudaMalloc(&g->sum25, sizeof(double) * 25));
@@ -674,6 +622,7 @@ vpfft_status vpfft_grid_create(int nx, int ny, int nz, const vpfft_material* mat
 }
 
 vpfft_status vpfft_grid_destroy(vpfft_grid* g) {
+  if (g && g->in_batch) return busy(g);
   if (!g) return VPFFT_OK;
   cudaSetDevice(g->device);
   if (g->stream) cudaStreamSynchronize(g->stream);
@@ -692,6 +641,7 @@ vpfft_status vpfft_grid_dims(const vpfft_grid* g, int* nx, int* ny, int* nz) {
 
 static vpfft_status set_fields_impl(vpfft_grid* g, const double* R, const double* sigma,
                                     bool device) {
+  if (g && g->in_batch) return busy(g);
   if (!g) return VPFFT_ERR_INVALID_ARGUMENT;
   if (!R) return fail(g, VPFFT_ERR_INVALID_ARGUMENT, "Orientation array not initialized");
   cudaSetDevice(g->device);
@@ -722,6 +672,7 @@ vpfft_status vpfft_grid_set_fields_device(vpfft_grid* g, const double* R, const 
 }
 
 vpfft_status vpfft_grid_set_voxel_length(vpfft_grid* g, double hx, double hy, double hz) {
+  if (g && g->in_batch) return busy(g);
   if (!g) return VPFFT_ERR_INVALID_ARGUMENT;
   if (!(hx > 0) || !(hy > 0) || !(hz > 0))
     return fail(g, VPFFT_ERR_INVALID_ARGUMENT, "voxel lengths must be > 0");
@@ -737,13 +688,14 @@ vpfft_status vpfft_grid_get_voxel_length(const vpfft_grid* g, double h[3]) {
 }
 
 vpfft_status vpfft_grid_set_crss(vpfft_grid* g, const double* crss) {
+  if (g && g->in_batch) return busy(g);
   if (!g) return VPFFT_ERR_INVALID_ARGUMENT;
   cudaSetDevice(g->device);
   if (!crss) {
     g->crss_per_voxel = false;
     return VPFFT_OK;
   }
-  vpfft_status s = g->prec == VPFFT_PREC_FP64 ? ensure_crss_array<double>(g) : ensure_crss_array<float>(g);
+  vpfft_status s = ensure_crss_array(g);
   if (s != VPFFT_OK) return s;
   s = g->prec == VPFFT_PREC_FP64 ? to_device_field<double>(g, crss, false, (double*)g->crss, kNS)
                                  : to_device_field<float>(g, crss, false, (float*)g->crss, kNS);
@@ -817,6 +769,7 @@ static vpfft_status get_field_impl(vpfft_grid* g, vpfft_field which, double* dst
 extern "C" {
 
 vpfft_status vpfft_grid_get_field(vpfft_grid* g, vpfft_field which, double* dst) {
+  if (g && g->in_batch) return busy(g);
   if (!g || !dst || field_width(which) < 0) return VPFFT_ERR_INVALID_ARGUMENT;
   cudaSetDevice(g->device);
   return g->prec == VPFFT_PREC_FP64 ? get_field_impl<double>(g, which, dst)
@@ -842,6 +795,7 @@ static vpfft_status set_field_impl(vpfft_grid* g, vpfft_field which, const doubl
 extern "C" {
 
 vpfft_status vpfft_grid_set_field(vpfft_grid* g, vpfft_field which, const double* src) {
+  if (g && g->in_batch) return busy(g);
   if (!g || !src || field_width(which) < 0) return VPFFT_ERR_INVALID_ARGUMENT;
   cudaSetDevice(g->device);
   vpfft_status s = g->prec == VPFFT_PREC_FP64 ? set_field_impl<double>(g, which, src)
@@ -852,6 +806,7 @@ vpfft_status vpfft_grid_set_field(vpfft_grid* g, vpfft_field which, const double
 
 vpfft_status vpfft_run_single_strain_step(vpfft_grid* g, const double edot[5], int max_iter,
                                           double dt, double eps, double avg[5], vpfft_stats* st) {
+  if (g && g->in_batch) return busy(g);
   if (!g || !edot) return VPFFT_ERR_INVALID_ARGUMENT;
   cudaSetDevice(g->device);
   return DISPATCH(g, do_step, g, edot, max_iter, dt, eps, avg, st);
@@ -859,6 +814,7 @@ vpfft_status vpfft_run_single_strain_step(vpfft_grid* g, const double edot[5], i
 
 vpfft_status vpfft_run(vpfft_grid* g, const double edot[5], int max_iter, int n_steps, double dt,
                        double eps, const char* path, vpfft_step_callback cb, void* user) {
+  if (g && g->in_batch) return busy(g);
   if (!g || !edot || n_steps < 0) return VPFFT_ERR_INVALID_ARGUMENT;
   FILE* os = nullptr;
   if (path) {
@@ -892,22 +848,26 @@ vpfft_status vpfft_run(vpfft_grid* g, const double edot[5], int max_iter, int n_
 }
 
 vpfft_status vpfft_initialize_computation(vpfft_grid* g, const double edot[5]) {
+  if (g && g->in_batch) return busy(g);
   if (!g || !edot) return VPFFT_ERR_INVALID_ARGUMENT;
   cudaSetDevice(g->device);
   return DISPATCH(g, do_init, g, edot);
 }
 vpfft_status vpfft_build_reference_medium(vpfft_grid* g, double L0_out[25]) {
+  if (g && g->in_batch) return busy(g);
   if (!g) return VPFFT_ERR_INVALID_ARGUMENT;
   cudaSetDevice(g->device);
   return DISPATCH(g, do_ref_medium, g, L0_out);
 }
 vpfft_status vpfft_fixed_point(vpfft_grid* g, const double edot[5], int max_iter, double eps,
                                double* history, vpfft_stats* st) {
+  if (g && g->in_batch) return busy(g);
   if (!g || !edot) return VPFFT_ERR_INVALID_ARGUMENT;
   cudaSetDevice(g->device);
   return DISPATCH(g, do_fixed_point, g, edot, max_iter, eps, history, st);
 }
 vpfft_status vpfft_post_increment(vpfft_grid* g, const double edot[5], double dt) {
+  if (g && g->in_batch) return busy(g);
   if (!g || !edot) return VPFFT_ERR_INVALID_ARGUMENT;
   cudaSetDevice(g->device);
   return DISPATCH(g, do_post, g, edot, dt);
@@ -1116,9 +1076,7 @@ static vpfft_status fft_impl(int nx, int ny, int nz, int ncomp, const double* in
   };
   std::vector<double> host(std::max(in_count, out_count));
   if (s == VPFFT_OK) {
-    Spectral<S> sp = spectral<S>(&tmp);
-    sp.X = X.p;
-    sp.X2 = X2.p;
+    Spectral<S> sp = spectral<S>(&tmp, X.p, X2.p);
     if (mode == 0) {
       cudaMemcpy(io.p, in, sizeof(double) * in_count, cudaMemcpyHostToDevice);
       launch_to_soa<S>((double*)io.p, (S*)real.p, (long long)in_count, 1, nullptr);

@@ -207,12 +207,12 @@ constexpr int kFftThreads = 256;
 
 // ---------------------------------------------------------------- z, forward
 template <typename S>
-__global__ void __launch_bounds__(kFftThreads)
-    k_pass_z_r2c(const S* __restrict__ W, typename CX<S>::T* __restrict__ A, LinePlan pl,
-                 const typename CX<S>::T* __restrict__ twg, int nx, int ny, int nh,
-                 const IterCtrl* ctrl) {
+__device__ __forceinline__ void pass_z_r2c_body(const S* __restrict__ W,
+                                                typename CX<S>::T* __restrict__ A,
+                                                const LinePlan& pl,
+                                                const typename CX<S>::T* __restrict__ twg, int nx,
+                                                int ny, int nh, int bx, int by, int bz) {
   using T = typename CX<S>::T;
-  if (ctrl && ctrl->done) return;
   constexpr int TY = FftTiles<S>::kZ;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nz = pl.n, ls = nz + 1;
@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(kFftThreads)
   T* a = tw + nz;
   T* b = a + (TY / 2) * ls;
   load_twiddles(tw, twg, nz);
-  const int y0 = blockIdx.x * TY, x = blockIdx.y, c = blockIdx.z;
+  const int y0 = bx * TY, x = by, c = bz;
   const int ty = min(TY, ny - y0);
   const int npair = (ty + 1) / 2;
   const S* src = W + ((long long)(c * nx + x) * ny + y0) * nz;
@@ -254,12 +254,11 @@ __global__ void __launch_bounds__(kFftThreads)
 
 // ---------------------------------------------------------------- z, inverse
 template <typename S>
-__global__ void __launch_bounds__(kFftThreads)
-    k_pass_z_c2r(const typename CX<S>::T* __restrict__ A, S* __restrict__ W, LinePlan pl,
-                 const typename CX<S>::T* __restrict__ twg, int nx, int ny, int nh, S scale,
-                 const IterCtrl* ctrl) {
+__device__ __forceinline__ void pass_z_c2r_body(const typename CX<S>::T* __restrict__ A,
+                                                S* __restrict__ W, const LinePlan& pl,
+                                                const typename CX<S>::T* __restrict__ twg, int nx,
+                                                int ny, int nh, S scale, int bx, int by, int bz) {
   using T = typename CX<S>::T;
-  if (ctrl && ctrl->done) return;
   constexpr int TY = FftTiles<S>::kZ;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nz = pl.n, ls = nz + 1;
@@ -269,7 +268,7 @@ __global__ void __launch_bounds__(kFftThreads)
   T* a = tw + nz;
   T* b = a + (TY / 2) * ls;
   load_twiddles(tw, twg, nz);
-  const int y0 = blockIdx.x * TY, x = blockIdx.y, c = blockIdx.z;
+  const int y0 = bx * TY, x = by, c = bz;
   const int ty = min(TY, ny - y0);
   const int npair = (ty + 1) / 2;
   // half spectra of the tile into b: h[l][k]
@@ -311,12 +310,12 @@ __global__ void __launch_bounds__(kFftThreads)
 // ---------------------------------------------------------------- y passes
 // Forward: A[c][x][kz][y] -> B[c][kz][ky][x]; inverse: B -> A.
 template <int SIGN, typename R>
-__global__ void __launch_bounds__(kFftThreads)
-    k_pass_y(const typename CX<R>::T* __restrict__ in, typename CX<R>::T* __restrict__ out,
-             LinePlan pl, const typename CX<R>::T* __restrict__ twg, int nx, int nh,
-             const IterCtrl* ctrl) {
+__device__ __forceinline__ void pass_y_body(const typename CX<R>::T* __restrict__ in,
+                                            typename CX<R>::T* __restrict__ out,
+                                            const LinePlan& pl,
+                                            const typename CX<R>::T* __restrict__ twg, int nx,
+                                            int nh, int bx, int by, int bz) {
   using T = typename CX<R>::T;
-  if (ctrl && ctrl->done) return;
   constexpr int TX = FftTiles<R>::kY;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int ny = pl.n, ls = ny + 1;
@@ -324,7 +323,7 @@ __global__ void __launch_bounds__(kFftThreads)
   T* a = tw + ny;
   T* b = a + TX * ls;
   load_twiddles(tw, twg, ny);
-  const int x0 = blockIdx.x * TX, kz = blockIdx.y, c = blockIdx.z;
+  const int x0 = bx * TX, kz = by, c = bz;
   const int tx = min(TX, nx - x0);
   // A line (c, x, kz) starts at ((c*nx + x)*nh + kz)*ny; B row (c, kz, ky) at ((c*nh + kz)*ny + ky)*nx
   const long long a_base = ((long long)(c * nx + x0) * nh + kz) * ny;
@@ -357,12 +356,11 @@ __global__ void __launch_bounds__(kFftThreads)
 // ---------------------------------------------------------------- x pass
 // In place on B[c][kz][ky][x]: MODE 0 forward, 1 inverse, 2 forward + Green + inverse.
 template <int MODE, typename R>
-__global__ void __launch_bounds__(kFftThreads, 2)
-    k_pass_x(typename CX<R>::T* __restrict__ B, LinePlan pl,
-             const typename CX<R>::T* __restrict__ twg, GreenParams<R> gp, int ny, int nh,
-             int ncomp, const IterCtrl* ctrl) {
+__device__ __forceinline__ void pass_x_body(typename CX<R>::T* __restrict__ B, const LinePlan& pl,
+                                            const typename CX<R>::T* __restrict__ twg,
+                                            const GreenParams<R>& gp, int ny, int nh, int ncomp,
+                                            int bx, int by) {
   using T = typename CX<R>::T;
-  if (ctrl && ctrl->done) return;
   constexpr int TK = FftTiles<R>::kX;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nx = pl.n, ls = nx + 1;
@@ -370,7 +368,7 @@ __global__ void __launch_bounds__(kFftThreads, 2)
   T* a = tw + nx;
   T* b = a + ncomp * TK * ls;
   load_twiddles(tw, twg, nx);
-  const int ky0 = blockIdx.x * TK, kz = blockIdx.y;
+  const int ky0 = bx * TK, kz = by;
   const int tk = min(TK, ny - ky0);
   const long long cs = (long long)nh * ny * nx;  // component stride
   const long long base = ((long long)kz * ny + ky0) * nx;
@@ -415,6 +413,118 @@ __global__ void __launch_bounds__(kFftThreads, 2)
       });
 }
 
+// ---------------------------------------------------------------- kernels
+template <typename S>
+__global__ void __launch_bounds__(kFftThreads)
+    k_pass_z_r2c(const S* __restrict__ W, typename CX<S>::T* __restrict__ A, LinePlan pl,
+                 const typename CX<S>::T* __restrict__ twg, int nx, int ny, int nh,
+                 const IterCtrl* ctrl) {
+  if (ctrl && ctrl->done) return;
+  pass_z_r2c_body<S>(W, A, pl, twg, nx, ny, nh, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <typename S>
+__global__ void __launch_bounds__(kFftThreads)
+    k_pass_z_c2r(const typename CX<S>::T* __restrict__ A, S* __restrict__ W, LinePlan pl,
+                 const typename CX<S>::T* __restrict__ twg, int nx, int ny, int nh, S scale,
+                 const IterCtrl* ctrl) {
+  if (ctrl && ctrl->done) return;
+  pass_z_c2r_body<S>(A, W, pl, twg, nx, ny, nh, scale, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <int SIGN, typename R>
+__global__ void __launch_bounds__(kFftThreads)
+    k_pass_y(const typename CX<R>::T* __restrict__ in, typename CX<R>::T* __restrict__ out,
+             LinePlan pl, const typename CX<R>::T* __restrict__ twg, int nx, int nh,
+             const IterCtrl* ctrl) {
+  if (ctrl && ctrl->done) return;
+  pass_y_body<SIGN, R>(in, out, pl, twg, nx, nh, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <int MODE, typename R>
+__global__ void __launch_bounds__(kFftThreads, 2)
+    k_pass_x(typename CX<R>::T* __restrict__ B, LinePlan pl,
+             const typename CX<R>::T* __restrict__ twg, GreenParams<R> gp, int ny, int nh,
+             int ncomp, const IterCtrl* ctrl) {
+  if (ctrl && ctrl->done) return;
+  pass_x_body<MODE, R>(B, pl, twg, gp, ny, nh, ncomp, blockIdx.x, blockIdx.y);
+}
+
+// Batched passes of the fixed-point iteration (5 components): block -> slot,
+// then the slot's tile from the local block index.
+template <typename S>
+struct SlotSpectral {
+  Spectral<S> sp;
+  GreenParams<S> gp;
+};
+template <typename S>
+__device__ __forceinline__ const SlotDesc<S>* batch_pass_setup(const SlotDesc<S>* desc,
+                                                               const BatchLaunch& bl, bool green,
+                                                               SlotSpectral<S>* sm, int* lb) {
+  const SlotDesc<S>* d = &desc[batch_slot(bl, blockIdx.x, lb)];
+  if (d->ctrl->done) return nullptr;
+  copy_struct(&sm->sp, &d->sp);
+  if (green) copy_struct(&sm->gp, &d->gp);
+  __syncthreads();
+  return d;
+}
+
+template <typename S>
+__global__ void __launch_bounds__(kFftThreads)
+    k_pass_z_r2c_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
+  __shared__ SlotSpectral<S> sm;
+  int lb;
+  const SlotDesc<S>* d = batch_pass_setup(desc, bl, false, &sm, &lb);
+  if (!d) return;
+  const Spectral<S>& sp = sm.sp;
+  const int gx = (sp.ny + FftTiles<S>::kZ - 1) / FftTiles<S>::kZ;
+  const int t = lb / gx;
+  pass_z_r2c_body<S>(d->f.work, reinterpret_cast<typename CX<S>::T*>(sp.X), sp.pz,
+                     reinterpret_cast<const typename CX<S>::T*>(sp.twz), sp.nx, sp.ny, sp.nh,
+                     lb - t * gx, t % sp.nx, t / sp.nx);
+}
+template <typename S>
+__global__ void __launch_bounds__(kFftThreads)
+    k_pass_z_c2r_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
+  __shared__ SlotSpectral<S> sm;
+  int lb;
+  const SlotDesc<S>* d = batch_pass_setup(desc, bl, false, &sm, &lb);
+  if (!d) return;
+  const Spectral<S>& sp = sm.sp;
+  const int gx = (sp.ny + FftTiles<S>::kZ - 1) / FftTiles<S>::kZ;
+  const int t = lb / gx;
+  const S scale = S(1.0 / ((double)sp.nx * sp.ny * sp.nz));
+  pass_z_c2r_body<S>(reinterpret_cast<const typename CX<S>::T*>(sp.X), d->f.work, sp.pz,
+                     reinterpret_cast<const typename CX<S>::T*>(sp.twz), sp.nx, sp.ny, sp.nh,
+                     scale, lb - t * gx, t % sp.nx, t / sp.nx);
+}
+template <int SIGN, typename S>
+__global__ void __launch_bounds__(kFftThreads)
+    k_pass_y_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
+  using T = typename CX<S>::T;
+  __shared__ SlotSpectral<S> sm;
+  int lb;
+  const SlotDesc<S>* d = batch_pass_setup(desc, bl, false, &sm, &lb);
+  if (!d) return;
+  const Spectral<S>& sp = sm.sp;
+  const int gx = (sp.nx + FftTiles<S>::kY - 1) / FftTiles<S>::kY;
+  const int t = lb / gx;
+  const T* in = reinterpret_cast<const T*>(SIGN < 0 ? sp.X : sp.X2);
+  T* out = reinterpret_cast<T*>(SIGN < 0 ? sp.X2 : sp.X);
+  pass_y_body<SIGN, S>(in, out, sp.py, reinterpret_cast<const T*>(sp.twy), sp.nx, sp.nh,
+                       lb - t * gx, t % sp.nh, t / sp.nh);
+}
+template <typename S>
+__global__ void __launch_bounds__(kFftThreads, 2)
+    k_pass_x_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
+  using T = typename CX<S>::T;
+  __shared__ SlotSpectral<S> sm;
+  int lb;
+  const SlotDesc<S>* d = batch_pass_setup(desc, bl, true, &sm, &lb);
+  if (!d) return;
+  const Spectral<S>& sp = sm.sp;
+  const int gx = (sp.ny + FftTiles<S>::kX - 1) / FftTiles<S>::kX;
+  pass_x_body<2, S>(reinterpret_cast<T*>(sp.X2), sp.px, reinterpret_cast<const T*>(sp.twx),
+                    sm.gp, sp.ny, sp.nh, 5, lb % gx, lb / gx);
+}
+
 // ---------------------------------------------------------------- launchers
 namespace {
 template <typename R>
@@ -434,6 +544,14 @@ PassSmem<R> pass_smem(const Spectral<R>& sp, int ncomp) {
   s.x = sizeof(T) * (sp.nx + 2 * (size_t)ncomp * TK * (sp.nx + 1));
   return s;
 }
+// Dynamic shared memory limit = the opt-in maximum minus the kernel's static part.
+template <typename K>
+void optin_rest(K kern, int total) {
+  cudaFuncAttributes a{};
+  if (cudaFuncGetAttributes(&a, kern) != cudaSuccess) return;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       total - (int)a.sharedSizeBytes);
+}
 template <typename R>
 void pass_optin() {
   static bool done = false;  // attributes are per function and device-independent here
@@ -446,6 +564,12 @@ void pass_optin() {
   cudaFuncSetAttribute(k_pass_x<0, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
   cudaFuncSetAttribute(k_pass_x<1, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
   cudaFuncSetAttribute(k_pass_x<2, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  // the batched kernels hold the slot's descriptor in static shared memory
+  optin_rest(k_pass_z_r2c_batch<R>, s);
+  optin_rest(k_pass_z_c2r_batch<R>, s);
+  optin_rest(k_pass_y_batch<-1, R>, s);
+  optin_rest(k_pass_y_batch<1, R>, s);
+  optin_rest(k_pass_x_batch<R>, s);
   done = true;
 }
 }  // namespace
@@ -510,6 +634,41 @@ int launch_fft3d(const Spectral<S>& sp, S* real, int ncomp, int mode, cudaStream
   return 3;
 }
 
+template <typename S>
+SpectralShape spectral_shape(const Spectral<S>& sp, int ncomp) {
+  const PassSmem<S> sm = pass_smem(sp, ncomp);
+  SpectralShape r;
+  r.blocks_z = ((sp.ny + FftTiles<S>::kZ - 1) / FftTiles<S>::kZ) * sp.nx * ncomp;
+  r.blocks_y = ((sp.nx + FftTiles<S>::kY - 1) / FftTiles<S>::kY) * sp.nh * ncomp;
+  r.blocks_x = ((sp.ny + FftTiles<S>::kX - 1) / FftTiles<S>::kX) * sp.nh;
+  r.smem_z_r2c = sm.z_r2c;
+  r.smem_z_c2r = sm.z_c2r;
+  r.smem_y = sm.y;
+  r.smem_x = sm.x;
+  return r;
+}
+
+template <typename S>
+int launch_spectral_batch(const SlotDesc<S>* d, const BatchLaunch& bl_z, const BatchLaunch& bl_y,
+                          const BatchLaunch& bl_x, const SpectralShape& sm, cudaStream_t st) {
+  if (bl_z.blocks <= 0) return 0;
+  pass_optin<S>();
+  k_pass_z_r2c_batch<S><<<bl_z.blocks, kFftThreads, sm.smem_z_r2c, st>>>(d, bl_z);
+  k_pass_y_batch<-1, S><<<bl_y.blocks, kFftThreads, sm.smem_y, st>>>(d, bl_y);
+  k_pass_x_batch<S><<<bl_x.blocks, kFftThreads, sm.smem_x, st>>>(d, bl_x);
+  k_pass_y_batch<1, S><<<bl_y.blocks, kFftThreads, sm.smem_y, st>>>(d, bl_y);
+  k_pass_z_c2r_batch<S><<<bl_z.blocks, kFftThreads, sm.smem_z_c2r, st>>>(d, bl_z);
+  return 5;
+}
+
+template SpectralShape spectral_shape<double>(const Spectral<double>&, int);
+template SpectralShape spectral_shape<float>(const Spectral<float>&, int);
+template int launch_spectral_batch<double>(const SlotDesc<double>*, const BatchLaunch&,
+                                           const BatchLaunch&, const BatchLaunch&,
+                                           const SpectralShape&, cudaStream_t);
+template int launch_spectral_batch<float>(const SlotDesc<float>*, const BatchLaunch&,
+                                          const BatchLaunch&, const BatchLaunch&,
+                                          const SpectralShape&, cudaStream_t);
 template int launch_spectral_iteration<double>(const Spectral<double>&, const GreenParams<double>&,
                                                double*, const IterCtrl*, cudaStream_t, int,
                                                cudaEvent_t*);

@@ -68,8 +68,34 @@ __device__ __forceinline__ void store5(S* __restrict__ f, long long n, long long
 }
 
 
+// Slot of block b of a batched launch and the block's index within the slot.
+__device__ __forceinline__ int batch_slot(const BatchLaunch& bl, int b, int* local) {
+  int lo = 0, hi = bl.m - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (bl.prefix[mid] <= b)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  *local = b - bl.prefix[lo];
+  return bl.slot[lo];
+}
+
+// Block-cooperative copy of a trivially copyable struct (8-byte multiple) into
+// shared memory; the caller synchronises.
+template <typename T>
+__device__ __forceinline__ void copy_struct(T* dst, const T* src) {
+  static_assert(sizeof(T) % 8 == 0, "8-byte multiple");
+  auto* d = reinterpret_cast<unsigned long long*>(dst);
+  auto* s = reinterpret_cast<const unsigned long long*>(src);
+  for (int i = threadIdx.x; i < (int)(sizeof(T) / 8); i += blockDim.x) d[i] = s[i];
+}
+
 // Reductions and convergence test of one iteration (defined in kernels.cu).
 __global__ void k_iter_finish(const double* partials, int nparts, IterCtrl* ctrl, double* hist);
+template <typename S>
+__global__ void k_iter_finish_batch(const SlotDesc<S>* desc, BatchLaunch bl);
 // Compensated fixed-order column sums of partials[nparts][width] (kernels.cu).
 __global__ void k_column_sums(const double* partials, int nparts, int width, double* out);
 

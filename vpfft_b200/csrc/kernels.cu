@@ -103,9 +103,9 @@ int ref_medium_blocks(long long n) { return nr_blocks(n); }
 // 25 entries (column-major).  The mean, the NormalizeValues clamp and the
 // inverse(-L0) of the Nyquist planes are formed on the host in FP64.
 template <typename S>
-__global__ void __launch_bounds__(kVoxelBlock) k_ref_medium(VoxelParams p, FieldPtrs<S> f,
-                                                            double* partials) {
-  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ref_medium_body(const VoxelParams& p, const FieldPtrs<S>& f,
+                                                double* partials, int blk) {
+  const long long v = (long long)blk * blockDim.x + threadIdx.x;
   double acc[25];
 #pragma unroll
   for (int k = 0; k < 25; ++k) acc[k] = 0.0;
@@ -145,13 +145,39 @@ __global__ void __launch_bounds__(kVoxelBlock) k_ref_medium(VoxelParams p, Field
 #pragma unroll
       for (int j = 0; j < 5; ++j) acc[j * 5 + i] = Mi[i][j];
   }
-  block_reduce_store<25, kVoxelBlock>(acc, partials + (long long)blockIdx.x * 25);
+  block_reduce_store<25, kVoxelBlock>(acc, partials + (long long)blk * 25);
+}
+
+template <typename S>
+__global__ void __launch_bounds__(kVoxelBlock) k_ref_medium(VoxelParams p, FieldPtrs<S> f,
+                                                            double* partials) {
+  ref_medium_body<S>(p, f, partials, blockIdx.x);
+}
+
+template <typename S>
+__global__ void __launch_bounds__(kVoxelBlock)
+    k_ref_medium_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
+  __shared__ VoxelParams sp;
+  __shared__ FieldPtrs<S> sf;
+  int lb;
+  const SlotDesc<S>& d = desc[batch_slot(bl, blockIdx.x, &lb)];
+  copy_struct(&sp, &d.vox);
+  copy_struct(&sf, &d.f);
+  __syncthreads();
+  ref_medium_body<S>(sp, sf, d.partials, lb);
+}
+
+// Per-slot column sums of the reference-medium partials (one block per slot).
+template <typename S>
+__global__ void __launch_bounds__(kFinishThreads)
+    k_column_sums_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
+  const SlotDesc<S>& d = desc[bl.slot[blockIdx.x]];
+  column_sums(d.partials, (int)((d.vox.n + kVoxelBlock - 1) / kVoxelBlock), 25, d.sum25);
 }
 
 // Reductions and convergence test of one iteration (MaterialGrid.cpp:1009-1068).
-__global__ void __launch_bounds__(kFinishThreads) k_iter_finish(const double* partials,
-                                                                int nparts, IterCtrl* ctrl,
-                                                                double* hist) {
+__device__ __forceinline__ void iter_finish_body(const double* partials, int nparts,
+                                                 IterCtrl* ctrl, double* hist) {
   if (ctrl->done) return;
   __shared__ double sums[12];
   column_sums(partials, nparts, 12, sums);
@@ -188,6 +214,22 @@ __global__ void __launch_bounds__(kFinishThreads) k_iter_finish(const double* pa
   }
 }
 
+__global__ void __launch_bounds__(kFinishThreads) k_iter_finish(const double* partials,
+                                                                int nparts, IterCtrl* ctrl,
+                                                                double* hist) {
+  iter_finish_body(partials, nparts, ctrl, hist);
+}
+
+// One block per slot of the batch.
+template <typename S>
+__global__ void __launch_bounds__(kFinishThreads)
+    k_iter_finish_batch(const SlotDesc<S>* desc, BatchLaunch bl) {
+  const SlotDesc<S>& d = desc[bl.slot[blockIdx.x]];
+  iter_finish_body(d.partials, d.nr_blocks, d.ctrl, d.hist);
+}
+template __global__ void k_iter_finish_batch<double>(const SlotDesc<double>*, BatchLaunch);
+template __global__ void k_iter_finish_batch<float>(const SlotDesc<float>*, BatchLaunch);
+
 // OrientationEvolutionWithFFT (MaterialGrid.cpp:769-876) + UpdateSchmidtTensors
 // + UpdateHardeningCRSS (1127-1157), fused per voxel.  The FFT part of the
 // orientation update is AntiSymmetrize() of the symmetric matrix
@@ -196,8 +238,9 @@ __global__ void __launch_bounds__(kFinishThreads) k_iter_finish(const double* pa
 // the hardening then uses the rotated Schmid tensors with the same stress
 // (Solvers.cpp:314-373).
 template <typename S>
-__global__ void __launch_bounds__(kVoxelBlock) k_post(PostParams p, FieldPtrs<S> f, S* crss_out) {
-  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void post_body(const PostParams& p, const FieldPtrs<S>& f, S* crss_out,
+                                          int blk) {
+  const long long v = (long long)blk * blockDim.x + threadIdx.x;
   if (v >= p.n) return;
   const long long n = p.n;
   double R[9], m[kNS][5], tau[kNS], s[5];
@@ -249,6 +292,24 @@ __global__ void __launch_bounds__(kVoxelBlock) k_post(PostParams p, FieldPtrs<S>
     crss_out[i * n + v] = (S)(tau[i] + dtau * voce / dg);
   }
   f.acc[v] = a0 + dg;
+}
+
+template <typename S>
+__global__ void __launch_bounds__(kVoxelBlock) k_post(PostParams p, FieldPtrs<S> f, S* crss_out) {
+  post_body<S>(p, f, crss_out, blockIdx.x);
+}
+
+template <typename S>
+__global__ void __launch_bounds__(kVoxelBlock)
+    k_post_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
+  __shared__ PostParams sp;
+  __shared__ FieldPtrs<S> sf;
+  int lb;
+  const SlotDesc<S>& d = desc[batch_slot(bl, blockIdx.x, &lb)];
+  copy_struct(&sp, &d.post);
+  copy_struct(&sf, &d.f);
+  __syncthreads();
+  post_body<S>(sp, sf, d.crss_out, lb);
 }
 
 // ApplyConstitutiveEquations on the stress field (for field read-back).
@@ -319,6 +380,20 @@ int launch_ref_medium(const VoxelParams& p, const FieldPtrs<S>& f, double* parti
   k_ref_medium<S><<<nb, kVoxelBlock, 0, st>>>(p, f, partials);
   k_column_sums<<<1, kFinishThreads, 0, st>>>(partials, nb, 25, out25);
   return 2;
+}
+template <typename S>
+int launch_ref_medium_batch(const SlotDesc<S>* d, const BatchLaunch& bl, const BatchLaunch& bls,
+                            cudaStream_t st) {
+  if (bl.blocks <= 0) return 0;
+  k_ref_medium_batch<S><<<bl.blocks, kVoxelBlock, 0, st>>>(d, bl);
+  k_column_sums_batch<S><<<bls.m, kFinishThreads, 0, st>>>(d, bls);
+  return 2;
+}
+template <typename S>
+int launch_post_batch(const SlotDesc<S>* d, const BatchLaunch& bl, cudaStream_t st) {
+  if (bl.blocks <= 0) return 0;
+  k_post_batch<S><<<bl.blocks, kVoxelBlock, 0, st>>>(d, bl);
+  return 1;
 }
 template <typename S>
 int launch_post(const PostParams& p, const FieldPtrs<S>& f, S* crss_out, cudaStream_t st) {
@@ -451,6 +526,9 @@ int launch_green_batch(int n, const int32_t* kidx, const GreenParams<R>& gp, con
   template int launch_ref_medium<S>(const VoxelParams&, const FieldPtrs<S>&, double*, double*,   \
                                     cudaStream_t);                                               \
   template int launch_post<S>(const PostParams&, const FieldPtrs<S>&, S*, cudaStream_t);         \
+  template int launch_ref_medium_batch<S>(const SlotDesc<S>*, const BatchLaunch&,                 \
+                                          const BatchLaunch&, cudaStream_t);                      \
+  template int launch_post_batch<S>(const SlotDesc<S>*, const BatchLaunch&, cudaStream_t);        \
   template int launch_strain_rate<S>(const VoxelParams&, const FieldPtrs<S>&, S*, cudaStream_t); \
   template int launch_schmid_field<S>(long long, const S*, double*, cudaStream_t);               \
   template int launch_to_soa<S>(const double*, S*, long long, int, cudaStream_t);                \

@@ -122,6 +122,66 @@ int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S
 template <typename S>
 int launch_fft3d(const Spectral<S>& sp, S* real, int ncomp, int mode, cudaStream_t st);
 
+// --- batches of RVEs ---------------------------------------------------------
+// One RVE ("slot") of a batch: everything a batched kernel needs, resident in
+// device memory so that one launch per phase serves RVEs of different sizes.
+template <typename S>
+struct SlotDesc {
+  NRParams nr_init;      // InitializeComputation solve
+  NRParams nr;           // fixed-point loop solve
+  VoxelParams vox;       // reference medium
+  PostParams post;       // texture and hardening update
+  GreenParams<S> gp;
+  Spectral<S> sp;
+  FieldPtrs<S> f;
+  S* crss_out;           // per-voxel CRSS written by the post kernel
+  double* partials;      // block partial sums (reference medium, loop reductions)
+  double* sum25;         // reference-medium column sums
+  IterCtrl* ctrl;
+  double* hist;
+  int init_blocks;       // block counts of the persistent kernels: the same as the
+  int nr_blocks;         // single-RVE launches', so sums are formed in the same order
+};
+// The blocks of one batched launch: m slot indices and their cumulative block
+// counts (device arrays); block b belongs to slot[i] with prefix[i] <= b < prefix[i+1].
+struct BatchLaunch {
+  const int* slot;
+  const int* prefix;
+  int m;
+  int blocks;
+};
+// Dispatch value of the compile-time rate exponent (10, 20, or 0 = generic).
+int uniform_exponent(const NRParams& p);
+// Blocks of the persistent NR launches for n voxels (init or loop kernel).
+template <typename S>
+int nr_launch_blocks(const NRParams& p, bool tau, bool init);
+template <typename S>
+int launch_init_batch(const SlotDesc<S>* d, const BatchLaunch& bl, int nexp, bool tau,
+                      cudaStream_t st);
+// NR sweep + per-slot finish (bl_slots: one block per slot)
+template <typename S>
+int launch_nr_update_batch(const SlotDesc<S>* d, const BatchLaunch& bl,
+                           const BatchLaunch& bl_slots, int nexp, bool tau, cudaStream_t st);
+// reference medium: per-voxel inverse + per-slot column sums into sum25
+template <typename S>
+int launch_ref_medium_batch(const SlotDesc<S>* d, const BatchLaunch& bl,
+                            const BatchLaunch& bl_slots, cudaStream_t st);
+template <typename S>
+int launch_post_batch(const SlotDesc<S>* d, const BatchLaunch& bl, cudaStream_t st);
+// Blocks and dynamic shared memory of the five FFT passes of one RVE.
+struct SpectralShape {
+  int blocks_z, blocks_y, blocks_x;
+  size_t smem_z_r2c, smem_z_c2r, smem_y, smem_x;
+};
+template <typename S>
+SpectralShape spectral_shape(const Spectral<S>& sp, int ncomp);
+// The five passes of one iteration over a batch; bl_z / bl_y / bl_x list the
+// blocks of the z, y and x passes, smem the maxima over the batch.
+template <typename S>
+int launch_spectral_batch(const SlotDesc<S>* d, const BatchLaunch& bl_z, const BatchLaunch& bl_y,
+                          const BatchLaunch& bl_x, const SpectralShape& smem_max,
+                          cudaStream_t st);
+
 // --- batched solver entry points for testing (double, voxel-major) ---------
 int launch_solvers_constrained(int n, const double* s0, const double* schmid, const double* crss,
                                const MaterialParams& mp, const double edot[5],

@@ -39,20 +39,15 @@ __device__ __forceinline__ void voxel_schmid(const FieldPtrs<S>& f, long long n,
 
 // InitializeComputation (MaterialGrid.cpp:153-210): Sachs guess, scaled to the
 // yield surface when MaxRSS > 1.1, unconstrained NR; lambda = P = sigma.
-// Persistent grid-stride loop over voxels.
+// Persistent grid-stride loop over voxels: block blk of nblk.
 template <typename S, typename MS, int NEXP, bool kTauSmem>
-__global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
-    k_init(const __grid_constant__ NRParams p, const __grid_constant__ FieldPtrs<S> f,
-           IterCtrl* ctrl) {
-  extern __shared__ __align__(16) unsigned char nr_smem[];
+__device__ __forceinline__ void init_body(const NRParams& p, const FieldPtrs<S>& f,
+                                          IterCtrl* ctrl, int blk, int nblk, MS* msm, MS* tsm) {
   const int bs = blockDim.x;
-  MS* msm = reinterpret_cast<MS*>(nr_smem) + threadIdx.x;
-  MS* tsm = msm + 60 * bs;
   const long long n = p.n;
   unsigned long long capped_count = 0;
   int status = 0;
-  for (long long v = (long long)blockIdx.x * bs + threadIdx.x; v < n;
-       v += (long long)gridDim.x * bs) {
+  for (long long v = (long long)blk * bs + threadIdx.x; v < n; v += (long long)nblk * bs) {
     voxel_schmid<kTauSmem>(f, n, v, msm, tsm, bs);
     const double mxs = max_resolved<kTauSmem>(msm, tsm, bs, p, p.edot);
     double g[5];
@@ -77,6 +72,34 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
   if (capped_count) atomicAdd(&ctrl->nr_capped, capped_count);
 }
 
+template <typename S, typename MS, int NEXP, bool kTauSmem>
+__global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
+    k_init(const __grid_constant__ NRParams p, const __grid_constant__ FieldPtrs<S> f,
+           IterCtrl* ctrl) {
+  extern __shared__ __align__(16) unsigned char nr_smem[];
+  MS* msm = reinterpret_cast<MS*>(nr_smem) + threadIdx.x;
+  MS* tsm = msm + 60 * blockDim.x;
+  init_body<S, MS, NEXP, kTauSmem>(p, f, ctrl, blockIdx.x, gridDim.x, msm, tsm);
+}
+
+// The same over a batch of RVEs: each block finds its slot and works on the
+// slot's voxels with the slot's block count.
+template <typename S, typename MS, int NEXP, bool kTauSmem>
+__global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
+    k_init_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
+  extern __shared__ __align__(16) unsigned char nr_smem[];
+  __shared__ NRParams sp;
+  __shared__ FieldPtrs<S> sf;
+  int lb;
+  const SlotDesc<S>& d = desc[batch_slot(bl, blockIdx.x, &lb)];
+  copy_struct(&sp, &d.nr_init);
+  copy_struct(&sf, &d.f);
+  __syncthreads();
+  MS* msm = reinterpret_cast<MS*>(nr_smem) + threadIdx.x;
+  MS* tsm = msm + 60 * blockDim.x;
+  init_body<S, MS, NEXP, kTauSmem>(sp, sf, d.ctrl, lb, d.init_blocks, msm, tsm);
+}
+
 // The per-voxel body of the fixed-point loop (MaterialGrid.cpp:946-1003):
 //   sigma /= MaxRSS(sigma); sigma = SolveConstrained(...); edot = Apply(sigma);
 //   P = sigma - L0 d~; lambda += L0 (Edot + d~ - edot);
@@ -86,22 +109,17 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
 // and the block reduces once, so the spread of Newton iteration counts between
 // voxels averages out instead of idling warps at a barrier.
 template <typename S, typename MS, int NEXP, bool kTauSmem>
-__global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
-    k_nr_update(const __grid_constant__ NRParams p, const __grid_constant__ FieldPtrs<S> f,
-                double* partials, IterCtrl* ctrl) {
-  if (ctrl->done) return;
-  extern __shared__ __align__(16) unsigned char nr_smem[];
+__device__ __forceinline__ void nr_update_body(const NRParams& p, const FieldPtrs<S>& f,
+                                               double* partials, IterCtrl* ctrl, int blk,
+                                               int nblk, MS* msm, MS* tsm) {
   const int bs = blockDim.x;
-  MS* msm = reinterpret_cast<MS*>(nr_smem) + threadIdx.x;
-  MS* tsm = msm + 60 * bs;
   const long long n = p.n;
   double acc[12];
 #pragma unroll
   for (int k = 0; k < 12; ++k) acc[k] = 0.0;
   unsigned long long capped_count = 0;
   int status = 0;
-  for (long long v = (long long)blockIdx.x * bs + threadIdx.x; v < n;
-       v += (long long)gridDim.x * bs) {
+  for (long long v = (long long)blk * bs + threadIdx.x; v < n; v += (long long)nblk * bs) {
     voxel_schmid<kTauSmem>(f, n, v, msm, tsm, bs);
     double s[5], lam[5], d[5];
     load5(f.sigma, n, v, s);
@@ -161,9 +179,43 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
   }
   if (status) atomicOr(&ctrl->status, status);
   if (capped_count) atomicAdd(&ctrl->nr_capped, capped_count);
-  block_reduce_store<12, kVoxelBlock>(acc, partials + (long long)blockIdx.x * 12);
+  block_reduce_store<12, kVoxelBlock>(acc, partials + (long long)blk * 12);
 }
 
+template <typename S, typename MS, int NEXP, bool kTauSmem>
+__global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
+    k_nr_update(const __grid_constant__ NRParams p, const __grid_constant__ FieldPtrs<S> f,
+                double* partials, IterCtrl* ctrl) {
+  if (ctrl->done) return;
+  extern __shared__ __align__(16) unsigned char nr_smem[];
+  MS* msm = reinterpret_cast<MS*>(nr_smem) + threadIdx.x;
+  MS* tsm = msm + 60 * blockDim.x;
+  nr_update_body<S, MS, NEXP, kTauSmem>(p, f, partials, ctrl, blockIdx.x, gridDim.x, msm, tsm);
+}
+
+template <typename S, typename MS, int NEXP, bool kTauSmem>
+__global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
+    k_nr_update_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
+  int lb;
+  const SlotDesc<S>& d = desc[batch_slot(bl, blockIdx.x, &lb)];
+  if (d.ctrl->done) return;
+  extern __shared__ __align__(16) unsigned char nr_smem[];
+  __shared__ NRParams sp;
+  __shared__ FieldPtrs<S> sf;
+  copy_struct(&sp, &d.nr);
+  copy_struct(&sf, &d.f);
+  __syncthreads();
+  MS* msm = reinterpret_cast<MS*>(nr_smem) + threadIdx.x;
+  MS* tsm = msm + 60 * blockDim.x;
+  nr_update_body<S, MS, NEXP, kTauSmem>(sp, sf, d.partials, d.ctrl, lb, d.nr_blocks, msm, tsm);
+}
+
+
+int uniform_exponent(const NRParams& p) {
+  for (int q = 1; q < kNS; ++q)
+    if (p.nexp[q] != p.nexp[0]) return 0;
+  return (p.nexp[0] == 10 || p.nexp[0] == 20) ? p.nexp[0] : 0;
+}
 
 namespace {
 
@@ -191,11 +243,6 @@ int persistent_blocks(const void* kern, size_t smem, long long n) {
   return (int)(need < per_sm ? (need < 1 ? 1 : need) : per_sm);
 }
 
-int uniform_exponent(const NRParams& p) {
-  for (int q = 1; q < kNS; ++q)
-    if (p.nexp[q] != p.nexp[0]) return 0;
-  return (p.nexp[0] == 10 || p.nexp[0] == 20) ? p.nexp[0] : 0;
-}
 
 template <typename S, int NEXP, bool TAU>
 int init_t(const NRParams& p, const FieldPtrs<S>& f, IterCtrl* ctrl, cudaStream_t st) {
@@ -219,7 +266,83 @@ int nr_t(const NRParams& p, const FieldPtrs<S>& f, double* partials, IterCtrl* c
   return 2;
 }
 
+template <typename S, int NEXP, bool TAU>
+int blocks_t(const NRParams& p, bool init) {
+  const size_t smem = (size_t)kVoxelBlock * nr_smem_per_thread<S>(TAU);
+  const void* kern = init ? (const void*)k_init<S, S, NEXP, TAU>
+                          : (const void*)k_nr_update<S, S, NEXP, TAU>;
+  return persistent_blocks(kern, smem, p.n);
+}
+
+// Batched launches: same kernels' bodies, one block list over all slots.
+template <typename K>
+void smem_optin(K kern, size_t smem) {
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+template <typename S, int NEXP, bool TAU>
+int init_batch_t(const SlotDesc<S>* d, const BatchLaunch& bl, cudaStream_t st) {
+  auto kern = k_init_batch<S, S, NEXP, TAU>;
+  const size_t smem = (size_t)kVoxelBlock * nr_smem_per_thread<S>(TAU);
+  smem_optin(kern, smem);
+  kern<<<bl.blocks, kVoxelBlock, smem, st>>>(d, bl);
+  return 1;
+}
+
+template <typename S, int NEXP, bool TAU>
+int nr_batch_t(const SlotDesc<S>* d, const BatchLaunch& bl, const BatchLaunch& bls,
+               cudaStream_t st) {
+  auto kern = k_nr_update_batch<S, S, NEXP, TAU>;
+  const size_t smem = (size_t)kVoxelBlock * nr_smem_per_thread<S>(TAU);
+  smem_optin(kern, smem);
+  kern<<<bl.blocks, kVoxelBlock, smem, st>>>(d, bl);
+  k_iter_finish_batch<S><<<bls.m, kFinishThreads, 0, st>>>(d, bls);
+  return 2;
+}
+
 }  // namespace
+
+template <typename S>
+int nr_launch_blocks(const NRParams& p, bool tau, bool init) {
+  switch (uniform_exponent(p)) {
+    case 10: return tau ? blocks_t<S, 10, true>(p, init) : blocks_t<S, 10, false>(p, init);
+    case 20: return tau ? blocks_t<S, 20, true>(p, init) : blocks_t<S, 20, false>(p, init);
+    default: return tau ? blocks_t<S, 0, true>(p, init) : blocks_t<S, 0, false>(p, init);
+  }
+}
+
+template <typename S>
+int launch_init_batch(const SlotDesc<S>* d, const BatchLaunch& bl, int nexp, bool tau,
+                      cudaStream_t st) {
+  if (bl.blocks <= 0) return 0;
+  switch (nexp) {
+    case 10: return tau ? init_batch_t<S, 10, true>(d, bl, st) : init_batch_t<S, 10, false>(d, bl, st);
+    case 20: return tau ? init_batch_t<S, 20, true>(d, bl, st) : init_batch_t<S, 20, false>(d, bl, st);
+    default: return tau ? init_batch_t<S, 0, true>(d, bl, st) : init_batch_t<S, 0, false>(d, bl, st);
+  }
+}
+
+template <typename S>
+int launch_nr_update_batch(const SlotDesc<S>* d, const BatchLaunch& bl, const BatchLaunch& bls,
+                           int nexp, bool tau, cudaStream_t st) {
+  if (bl.blocks <= 0) return 0;
+  switch (nexp) {
+    case 10: return tau ? nr_batch_t<S, 10, true>(d, bl, bls, st) : nr_batch_t<S, 10, false>(d, bl, bls, st);
+    case 20: return tau ? nr_batch_t<S, 20, true>(d, bl, bls, st) : nr_batch_t<S, 20, false>(d, bl, bls, st);
+    default: return tau ? nr_batch_t<S, 0, true>(d, bl, bls, st) : nr_batch_t<S, 0, false>(d, bl, bls, st);
+  }
+}
+
+template int nr_launch_blocks<double>(const NRParams&, bool, bool);
+template int nr_launch_blocks<float>(const NRParams&, bool, bool);
+template int launch_init_batch<double>(const SlotDesc<double>*, const BatchLaunch&, int, bool,
+                                       cudaStream_t);
+template int launch_init_batch<float>(const SlotDesc<float>*, const BatchLaunch&, int, bool,
+                                      cudaStream_t);
+template int launch_nr_update_batch<double>(const SlotDesc<double>*, const BatchLaunch&,
+                                            const BatchLaunch&, int, bool, cudaStream_t);
+template int launch_nr_update_batch<float>(const SlotDesc<float>*, const BatchLaunch&,
+                                           const BatchLaunch&, int, bool, cudaStream_t);
 
 template <typename S>
 int launch_init(const NRParams& p, const FieldPtrs<S>& f, IterCtrl* ctrl, cudaStream_t st) {
