@@ -248,6 +248,127 @@ def e2e_arm(args, R, edot):
     return dict(seconds=dt, iters=iters, N=N, h2d=N * 14 * 8, d2h=N * 5 * 8 + 40)
 
 
+# ------------------------------------------------------------------ batched and serving
+def material_n10():
+    import vpfft_b200 as vp
+
+    return vp.material(gamma_dot_base=1.0, rate_sensitivity=10, crss=1.0, tau0=1.0, tau1=0.5,
+                       theta0=20.0, theta1=1.0)
+
+
+def batched_arm(n_rves: int) -> dict:
+    """Batched RVE solves: n_rves RVEs with edges uniform in {16, 32, 48, 64},
+    8-200 Voronoi grains, random traceless velocity gradients (equivalent
+    strain rate 1), n = 10, one increment each (max 100 iterations, eps 1e-5),
+    all in one mixed-precision batch; against the same solves one at a time on
+    the FP64 single-grid path."""
+    import vpfft_b200 as vp
+    from vpfft_b200 import fixtures
+
+    rng = np.random.default_rng(SEED + 4)
+    specs = [(int(rng.choice([16, 32, 48, 64])), int(rng.integers(8, 201))) for _ in range(n_rves)]
+    edots = [fixtures.edot_from_matrix(fixtures.random_traceless_velocity_gradient(rng))
+             for _ in specs]
+    Rs = [fixtures.polycrystal(e, e, e, ng, SEED * 7 + k) for k, (e, ng) in enumerate(specs)]
+    mat = material_n10()
+    voxels = sum(e ** 3 for e, _ in specs)
+
+    def run_batch(precision, grids):
+        b = vp.Batch(precision, material=mat, max_slots=len(grids))
+        gs = [b.new_grid(e, e, e) for e, _ in grids]
+        return b, gs
+
+    # warm-up batch (module loading, shared-memory attributes, graph capture)
+    b, gs = run_batch("mixed", specs[:8])
+    for g, R, e in zip(gs, Rs[:8], edots[:8]):
+        g.SendDataAndInitialize(R)
+        b.submit(g, e)
+    b.run()
+    b.poll()
+    for g in gs:
+        g.close()
+    b.close()
+
+    b, gs = run_batch("mixed", specs)
+    for g, R in zip(gs, Rs):
+        g.SendDataAndInitialize(R)
+    t0 = time.perf_counter()
+    ids = [b.submit(g, e) for g, e in zip(gs, edots)]
+    b.run()
+    t_batch = time.perf_counter() - t0
+    res = {r.request_id: r for r in b.poll()}
+    info = b.info()
+    avg_mixed = [res[i].avg_stress for i in ids]
+    iters = [res[i].iterations for i in ids]
+    for g in gs:
+        g.close()
+    b.close()
+
+    # one at a time, FP64 single-grid path
+    t_seq = 0.0
+    err = []
+    for k, ((e, _), R, ed) in enumerate(zip(specs, Rs, edots)):
+        g = vp.MaterialGrid(e, e, e, material=mat, precision="fp64")
+        g.SendDataAndInitialize(R)
+        if k == 0:  # warm-up of the FP64 kernels
+            g.RunSingleStrainStep(ed, 100, 0.005, 1e-5)
+            g.SendDataAndInitialize(R)
+        t0 = time.perf_counter()
+        avg = g.RunSingleStrainStep(ed, 100, 0.005, 1e-5)
+        t_seq += time.perf_counter() - t0
+        err.append(float(np.linalg.norm(avg_mixed[k] - avg) / np.linalg.norm(avg)))
+        g.close()
+    return {
+        "metric": "RVE solves/s (one increment each), batched mixed vs one-at-a-time FP64",
+        "value": n_rves / t_batch, "unit": "solves/s",
+        "one_at_a_time_fp64": n_rves / t_seq,
+        "speedup_vs_one_at_a_time_fp64": t_seq / t_batch,
+        "rves": n_rves, "voxels": voxels, "iterations_mean": float(np.mean(iters)),
+        "voxel_iters_per_s": float(sum(e ** 3 * it for (e, _), it in zip(specs, iters)) / t_batch),
+        "avg_stress_rel_err_vs_fp64_max": float(max(err)),
+        "graph_replays": info["graph_replays"], "kernel_launches": info["kernel_launches"],
+        "ticks": info["ticks"],
+        "timing": "host wall clock around submit + run (the batch synchronises every tick)",
+        "config": ("edges uniform {16,32,48,64}, grains uniform [8,200], random traceless L, "
+                   "n=10, gdot0=1, CRSS=1, max 100 iterations, eps 1e-5, dt 0.005"),
+    }
+
+
+def serving_arm(n_requests: int) -> dict:
+    """Serving: Poisson arrivals (mean 500/s) of one-increment requests on a
+    pool of 64 persistent RVEs with edges {32, 48, 64, 96} (weights
+    0.4/0.3/0.2/0.1), each request with its own random traceless velocity
+    gradient; continuous batching through one mixed-precision batch."""
+    import vpfft_b200 as vp
+    from vpfft_b200 import serving
+
+    budget = 2 << 30
+    b = vp.Batch("mixed", material=material_n10(), max_slots=64, iterations_per_tick=4,
+                 hbm_budget_bytes=budget)
+    pool = serving.rve_pool(b, [32, 48, 64, 96], [0.4, 0.3, 0.2, 0.1], 64, SEED)
+    serving.serve(b, pool, serving.poisson_trace(32, 500.0, len(pool), SEED + 1))  # warm-up
+    trace = serving.poisson_trace(n_requests, 500.0, len(pool), SEED + 2)
+    r = serving.serve(b, pool, trace)
+    info = b.info()
+    for g in pool:
+        g.close()
+    b.close()
+    return {
+        "metric": "served RVE solves/s with p50/p99 latency (arrival -> result)",
+        "value": r["throughput"], "unit": "solves/s",
+        "offered_rate": r["offered_rate"], "requests": r["requests"],
+        "completed_ok": r["completed_ok"],
+        "latency_p50_s": r["latency_p50_s"], "latency_p99_s": r["latency_p99_s"],
+        "latency_max_s": r["latency_max_s"], "iterations_mean": r["iterations_mean"],
+        "pool_rves": len(pool), "max_slots": 64, "iterations_per_tick": 4,
+        "hbm_budget_bytes": budget,
+        "admissions_deferred_for_memory": info["admissions_deferred_for_memory"],
+        "config": ("Poisson arrivals mean 500/s, pool of 64 RVEs, edges {32,48,64,96} weights "
+                   "0.4/0.3/0.2/0.1, grains uniform [8,200], random traceless L per request, "
+                   "n=10, mixed, max 100 iterations, eps 1e-5, dt 0.005"),
+    }
+
+
 # ------------------------------------------------------------------ CPU side
 def ref_binary():
     from oracle import refio
@@ -311,7 +432,11 @@ def cpu_baseline_ours():
 _dist = None
 
 
-def setup_dist(n_gpus):
+def setup_dist(n_gpus, backend: str = "nccl"):
+    """One process per GPU under torchrun (RANK/WORLD_SIZE/MASTER_* from the
+    environment); the process group only carries the barrier and the
+    max-over-ranks of the timings (replicas: no collective in the data path).
+    backend "gloo" runs the same logic on CPU."""
     global _dist
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     if ws > 1:
@@ -319,16 +444,23 @@ def setup_dist(n_gpus):
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
         _dist = dist
     return int(os.environ.get("RANK", "0")), ws
 
 
+def _coll_device():
+    return "cuda" if _dist is not None and _dist.get_backend() == "nccl" else "cpu"
+
+
 def barrier():
     if _dist is not None:
-        import torch
+        if _coll_device() == "cuda":
+            import torch
 
-        _dist.barrier(device_ids=[torch.cuda.current_device()])
+            _dist.barrier(device_ids=[torch.cuda.current_device()])
+        else:
+            _dist.barrier()
 
 
 def max_over_ranks(x: float) -> float:
@@ -336,9 +468,15 @@ def max_over_ranks(x: float) -> float:
         return x
     import torch
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_coll_device())
     _dist.all_reduce(t, op=_dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_rate(units_per_rank: float, world_size: int, seconds_max: float) -> float:
+    """Aggregate rate of a replica run: every rank processed units_per_rank in
+    at most seconds_max (the maximum over ranks)."""
+    return units_per_rank * world_size / seconds_max
 
 
 # ------------------------------------------------------------------ main
@@ -384,6 +522,10 @@ def main(argv=None):
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--batch-rves", type=int, default=256)
+    ap.add_argument("--serve-requests", type=int, default=1000)
     args = ap.parse_args(argv)
     rank, ws = setup_dist(args.gpus)
     if args.impl == "reference":
@@ -407,7 +549,7 @@ def main(argv=None):
     main_res = device_arm(args, R, edot, args.precision)
     ms = max_over_ranks(main_res["ms"])
     N = main_res["N"]
-    value = N * args.steps * ws / (ms / 1e3)
+    value = whole_job_rate(N * args.steps, ws, ms / 1e3)
 
     # per-kernel device times and the roofline of the dominant kernel
     s = 4 if args.precision == "mixed" else 8
@@ -495,6 +637,10 @@ def main(argv=None):
                        "step": ("one increment via vpfft_run_single_strain_step (max_iter 100, "
                                 "eps 1e-5) with pinned host orientation/stress in and the "
                                 "stress field out")}
+    if ws == 1 and not args.no_batched:
+        line["batched"] = batched_arm(args.batch_rves)
+    if ws == 1 and not args.no_serving:
+        line["serving"] = serving_arm(args.serve_requests)
     if rank == 0 and ws == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline_ours()
     if rank == 0:

@@ -15,7 +15,8 @@ increments, voxel lengths, orientations or their SHA-256 for the large case),
 per increment the iteration count, <sigma>, the per-iteration history
 (<sigma>, <edot>, delta_sigma, delta_eps) and L0, and the fields after the run
 (stress, Lagrange multiplier, orientation, CRSS, accumulated shear, P and d~ of
-the last iteration; sampled voxels only for the 64^3 case).
+the last iteration; for the 64^3 case every field's mean and RMS after each
+increment, and sampled voxels after increments 1, 5, 10, 15 and 20).
 """
 from __future__ import annotations
 
@@ -64,7 +65,7 @@ CASES = {
     # hardening and texture update (long: tens of minutes on one core)
     "c2_64": dict(dims=(64, 64, 64), grains=125, seed=2, n=10, L=UNIAXIAL, nsteps=20,
                   max_iter=100, dt=0.005, eps=1e-5, h=(1.0, 1.0, 1.0), dump_iters=(),
-                  sample=4096),
+                  sample=4096, sample_stride=4, store_increments=(0, 4, 9, 14, 19)),
 }
 SMALL = ["c1_16", "hard_16", "odd_15x12x10", "n20_16"]
 
@@ -109,11 +110,13 @@ def make_case(name: str, binary: str = refio.REF_BIN) -> str:
     else:
         idx = np.unique(np.concatenate([np.arange(0, n, n // (sample // 2)),
                                         np.random.default_rng(0).choice(n, sample // 2, False)]))
+        idx = idx[::c.get("sample_stride", 1)]
         rec["sample_index"] = idx
         for s in range(c["nsteps"]):
             for f in ("sigma", "lambda", "R", "crss"):
                 full = out[f"inc{s}_{f}"]
-                rec[f"inc{s}_{f}"] = full[idx]
+                if s in c.get("store_increments", range(c["nsteps"])):
+                    rec[f"inc{s}_{f}"] = full[idx]
                 rec[f"inc{s}_{f}_mean"] = full.mean(axis=0)
                 rec[f"inc{s}_{f}_rms"] = np.sqrt((full ** 2).mean(axis=0))
     path = os.path.join(HERE, f"{name}.npz")

@@ -165,3 +165,48 @@ def test_errors_are_returned(lib):
     assert np.all(np.isfinite(avg))
     assert grid.last_stats.iterations == 3
     grid.close()
+
+
+def test_c2_twenty_increments_with_hardening_and_texture(golden, lib):
+    """The 64^3 multi-increment case (125 grains, 20 increments of uniaxial
+    tension, Voce hardening and texture update), FP64, against the reference
+    run field by field: every increment's <sigma> history (1e-9), L0 (1e-7),
+    the mean and RMS of sigma, lambda, R and CRSS (1e-9 relative), and sampled
+    voxels after increments 1, 5, 10, 15 and 20 (1e-7 max-relative)."""
+    import hashlib
+
+    from vpfft_b200 import fixtures
+
+    g = golden("c2_64")
+    dims = tuple(int(x) for x in g["dims"])
+    R = fixtures.polycrystal(*dims, int(g["grains"]), int(g["seed"]))
+    assert hashlib.sha256(np.ascontiguousarray(R).tobytes()).hexdigest() == str(g["R_in_sha256"])
+    grid = MaterialGrid(*dims, material=material_of(g), precision="fp64")
+    grid.SendDataAndInitialize(R, np.zeros((grid.N, 5)))
+    e = g["edot"]
+    idx = g["sample_index"]
+    off = 0
+    getters = {"sigma": grid.Stress, "lambda": grid.LagrangeMultiplier, "R": grid.Orientation,
+               "crss": grid.CRSS}
+    for s in range(int(g["nsteps"])):
+        grid.InitializeComputation(e)
+        L0 = grid.BuildLinearRefMediumStiffness()
+        hist = grid.FixedPoint(e, int(g["max_iter"]), float(g["eps"]))
+        grid.PostIncrement(e, float(g["dt"]))
+        assert len(hist) == int(g["iters"][s])
+        assert np.abs(L0 - g["L0"][s]).max() <= 1e-7 * np.abs(g["L0"][s]).max()
+        ref = g["history"][off: off + len(hist)]
+        off += int(g["hist_counts"][s])
+        rel = np.linalg.norm(hist[:, :5] - ref[:, :5], axis=1) / np.linalg.norm(ref[:, :5], axis=1)
+        assert rel.max() <= 1e-9, (s, rel.max())
+        np.testing.assert_allclose(hist[:, 10:], ref[:, 10:], rtol=1e-6)
+        for f, get in getters.items():
+            full = get().reshape(grid.N, -1)
+            np.testing.assert_allclose(full.mean(axis=0), g[f"inc{s}_{f}_mean"], rtol=1e-9,
+                                       atol=1e-12 * np.abs(g[f"inc{s}_{f}_rms"]).max())
+            np.testing.assert_allclose(np.sqrt((full ** 2).mean(axis=0)), g[f"inc{s}_{f}_rms"],
+                                       rtol=1e-9)
+            if f"inc{s}_{f}" in g:
+                assert voxel_rel(full[idx], g[f"inc{s}_{f}"]) <= 1e-7, (s, f)
+    np.testing.assert_allclose(grid.VoxelLength(), g["voxlen"], rtol=1e-14)
+    grid.close()

@@ -178,6 +178,7 @@ NRParams nr_params(const vpfft_grid* g, const double edot[5], bool init) {
     p.max_rss = g->opt.nr_max_resolved;
     p.max_iter = g->opt.nr_max_iter;
   }
+  set_fp32_copies(p);
   return p;
 }
 

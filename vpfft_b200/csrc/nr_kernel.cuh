@@ -80,6 +80,41 @@ struct NRParams {
   double max_rss;     // admissibility cap of |r_s|
   int32_t max_iter;
   int32_t pad_;
+  // FP32 copies for the Newton predictor of the mixed path (set_fp32_copies)
+  float gdot_f[kNS];
+  float icrss_f[kNS];
+  float n_f[kNS];
+  float eps_f;
+  float max_rss_f;
+};
+
+// Fills the FP32 copies of the per-system constants from the FP64 values.
+__host__ __device__ inline void set_fp32_copies(NRParams& p) {
+  for (int q = 0; q < kNS; ++q) {
+    p.gdot_f[q] = (float)p.gdot[q];
+    p.icrss_f[q] = (float)p.icrss[q];
+    p.n_f[q] = (float)p.nexp[q];
+  }
+  p.eps_f = (float)p.eps;
+  p.max_rss_f = (float)p.max_rss;
+}
+
+// The per-system constants in the arithmetic type of a Newton pass.
+template <typename T>
+struct NRConst;
+template <>
+struct NRConst<double> {
+  __device__ static double gdot(const NRParams& p, int q) { return p.gdot[q]; }
+  __device__ static double icrss(const NRParams& p, int q) { return p.icrss[q]; }
+  __device__ static double n(const NRParams& p, int q) { return (double)p.nexp[q]; }
+  __device__ static double max_rss(const NRParams& p) { return p.max_rss; }
+};
+template <>
+struct NRConst<float> {
+  __device__ static float gdot(const NRParams& p, int q) { return p.gdot_f[q]; }
+  __device__ static float icrss(const NRParams& p, int q) { return p.icrss_f[q]; }
+  __device__ static float n(const NRParams& p, int q) { return p.n_f[q]; }
+  __device__ static float max_rss(const NRParams& p) { return p.max_rss_f; }
 };
 
 // packed index of (i, j), i <= j, in a symmetric 5x5
@@ -166,10 +201,14 @@ __device__ __forceinline__ double itau_of(const MS* tsm, int bs, const NRParams&
 // One pass over the systems: r_s, admissibility, S = sum m gdot r, K = sum n gdot/tau m m^T,
 // in arithmetic type T (double, or float for the predictor of the mixed path).
 // snap: set |r| < 1e-10 to 0 (the unconstrained solver does, Solvers.cpp:50-51).
-template <int NEXP, bool kSnap, bool kTauSmem, typename T, typename MS>
+// rmax (kRmax): max_s |r_s| at s.
+template <int NEXP, bool kSnap, bool kTauSmem, typename T, typename MS, bool kRmax = false>
 __device__ __forceinline__ bool accumulate(const MS* msm, const MS* tsm, int bs,
-                                           const NRParams& p, const T s[5], T S[5], T K[15]) {
+                                           const NRParams& p, const T s[5], T S[5], T K[15],
+                                           T* rmax = nullptr) {
+  using C = NRConst<T>;
   bool adm = true;
+  T rm = T(0);
 #pragma unroll
   for (int c = 0; c < 5; ++c) S[c] = T(0);
 #pragma unroll
@@ -179,16 +218,21 @@ __device__ __forceinline__ bool accumulate(const MS* msm, const MS* tsm, int bs,
     T m[5];
 #pragma unroll
     for (int c = 0; c < 5; ++c) m[c] = (T)msm[(q * 5 + c) * bs];
-    const T it = (T)itau_of<kTauSmem>(tsm, bs, p, q);
+    T it;
+    if constexpr (kTauSmem)
+      it = (T)tsm[q * bs];
+    else
+      it = C::icrss(p, q);
     T r = (m[0] * s[0] + m[1] * s[1] + m[2] * s[2] + m[3] * s[3] + m[4] * s[4]) * it;
     if (kSnap) r = fabs(r) < T(1e-10) ? T(0) : r;
-    adm = adm && !(fabs(r) > (T)p.max_rss);
+    adm = adm && !(fabs(r) > C::max_rss(p));
+    if constexpr (kRmax) rm = fmax(rm, fabs(r));
     const int n = p.nexp[q];
     // the constrained solver tests n != 1, the unconstrained n - 1 > 0 (Solvers.cpp:66,177)
     const bool power = kSnap ? (n - 1 > 0) : (n != 1);
-    const T g = power ? (T)p.gdot[q] * pow_nm1<NEXP>(fabs(r), n) : (T)p.gdot[q];
+    const T g = power ? C::gdot(p, q) * pow_nm1<NEXP>(fabs(r), n) : C::gdot(p, q);
     const T gr = g * r;
-    const T w = (T)n * g * it;
+    const T w = C::n(p, q) * g * it;
 #pragma unroll
     for (int i = 0; i < 5; ++i) {
       S[i] += m[i] * gr;
@@ -197,6 +241,7 @@ __device__ __forceinline__ bool accumulate(const MS* msm, const MS* tsm, int bs,
       for (int j = i; j < 5; ++j) K[sym5(i, j)] += mw * m[j];
     }
   }
+  if constexpr (kRmax) *rmax = rm;
   return adm;
 }
 
@@ -204,11 +249,12 @@ __device__ __forceinline__ bool accumulate(const MS* msm, const MS* tsm, int bs,
 // the reference's iteration and stopping rule in single precision.  Returns
 // true and the iterate in s_io when it converged with finite values; the
 // caller then takes the accepted step with FP64 residual and Jacobian.
+// *rmax0 gets max_s |r_s| at the starting point.
 template <int NEXP, bool kTauSmem, typename MS>
 __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, int bs,
                                                 const NRParams& p, const float L0i[15],
                                                 const double lam[5], const double ed[5],
-                                                double s_io[5], int max_steps) {
+                                                double s_io[5], int max_steps, float* rmax0) {
   float cur[5], l32[5], e32[5];
 #pragma unroll
   for (int c = 0; c < 5; ++c) {
@@ -216,9 +262,13 @@ __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, in
     l32[c] = (float)lam[c];
     e32[c] = (float)ed[c];
   }
+  *rmax0 = 0.f;
   for (int it = 0; it < max_steps; ++it) {
-    float S[5], K[15];
-    if (!accumulate<NEXP, false, kTauSmem, float>(msm, tsm, bs, p, cur, S, K)) return false;
+    float S[5], K[15], rm;
+    const bool adm =
+        accumulate<NEXP, false, kTauSmem, float, MS, true>(msm, tsm, bs, p, cur, S, K, &rm);
+    if (it == 0) *rmax0 = rm;
+    if (!adm) return false;
     float y[5];
 #pragma unroll
     for (int i = 0; i < 5; ++i) {
@@ -242,7 +292,7 @@ __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, in
     }
     const float rel = sqrtf(dn) / sqrtf(an);
     if (!isfinite(rel)) return false;
-    if (rel < (float)p.eps) {
+    if (rel < p.eps_f) {
 #pragma unroll
       for (int c = 0; c < 5; ++c) s_io[c] = (double)cur[c];
       return true;
@@ -257,7 +307,8 @@ template <int NEXP, bool kTauSmem, typename MS>
 __device__ __forceinline__ int nr_constrained_smem(const MS* msm, const MS* tsm, int bs,
                                                    const NRParams& p, const double lam[5],
                                                    const double ed[5], double s_io[5],
-                                                   double* rel_out, bool* capped) {
+                                                   double* rel_out, bool* capped,
+                                                   double* e_lin = nullptr) {
   double cur[5], saved[5], nw[5] = {-1.0, -3.0, -7.0, -9.0, -11.0};
 #pragma unroll
   for (int c = 0; c < 5; ++c) cur[c] = saved[c] = s_io[c];
@@ -318,6 +369,17 @@ __device__ __forceinline__ int nr_constrained_smem(const MS* msm, const MS* tsm,
   *capped = !(rel < p.eps);
 #pragma unroll
   for (int c = 0; c < 5; ++c) s_io[c] = nw[c];
+  if (e_lin) {
+    // strain rate at the new point from the last Newton linearisation:
+    // S + K delta = ed - L0^-1 (sigma_new - lambda)  (error O(|delta|^2))
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      double a = ed[i];
+#pragma unroll
+      for (int j = 0; j < 5; ++j) a -= p.L0inv[sym5(i, j)] * (nw[j] - lam[j]);
+      e_lin[i] = a;
+    }
+  }
   return steps;
 }
 

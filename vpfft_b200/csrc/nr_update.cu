@@ -24,6 +24,12 @@ template <typename MS>
 constexpr int nr_min_blocks() {
   return sizeof(MS) == 8 ? 3 : 4;
 }
+// The batched kernels read the slot's constants from shared memory instead of
+// the constant bank, which costs registers: three blocks per SM.
+template <typename MS>
+constexpr int nr_batch_min_blocks() {
+  return 3;
+}
 
 template <bool kTauSmem, typename S, typename MS>
 __device__ __forceinline__ void voxel_schmid(const FieldPtrs<S>& f, long long n, long long v,
@@ -85,7 +91,7 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
 // The same over a batch of RVEs: each block finds its slot and works on the
 // slot's voxels with the slot's block count.
 template <typename S, typename MS, int NEXP, bool kTauSmem>
-__global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
+__global__ void __launch_bounds__(kVoxelBlock, nr_batch_min_blocks<MS>())
     k_init_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
   extern __shared__ __align__(16) unsigned char nr_smem[];
   __shared__ NRParams sp;
@@ -126,29 +132,47 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const FieldPtr
     load5(f.lambda, n, v, lam);
     load5(f.work, n, v, d);
     if (f.dkeep) store5(f.dkeep, n, v, d);
-    const double mx = max_resolved<kTauSmem>(msm, tsm, bs, p, s);
-    if (mx < 1e-10) status |= kStatusMaxRssTiny;
     double ed[5];
 #pragma unroll
-    for (int c = 0; c < 5; ++c) {
-      s[c] /= mx;
-      ed[c] = p.edot[c] + d[c];
-    }
-    double rel;
+    for (int c = 0; c < 5; ++c) ed[c] = p.edot[c] + d[c];
+    double rel, e[5];
     bool capped;
     if constexpr (sizeof(S) == 4) {
-      // mixed precision: FP32 Newton predictor, then the FP64 solve from its
-      // iterate (normally one Newton step with FP64 residual and Jacobian);
-      // from the original start if the predictor failed
-      float L0i[15];
+      // mixed precision: an FP32 Newton predictor from the previous stress,
+      // then the FP64 solve from its iterate (normally one Newton step with
+      // FP64 residual and Jacobian).  If the predictor fails, the FP64 solve
+      // starts where the reference's does, at sigma / MaxRSS.  The strain rate
+      // comes from the last Newton linearisation when that step was tiny.
+      float L0i[15], mx0;
 #pragma unroll
       for (int k = 0; k < 15; ++k) L0i[k] = (float)p.L0inv[k];
-      nr_predict_fp32<NEXP, kTauSmem>(msm, tsm, bs, p, L0i, lam, ed, s, 8);
+      double s0[5];
+#pragma unroll
+      for (int c = 0; c < 5; ++c) s0[c] = s[c];
+      const bool ok = nr_predict_fp32<NEXP, kTauSmem>(msm, tsm, bs, p, L0i, lam, ed, s, 8, &mx0);
+      if (mx0 < 1e-10f) status |= kStatusMaxRssTiny;
+      if (!ok) {
+        const double mx = max_resolved<kTauSmem>(msm, tsm, bs, p, s0);
+#pragma unroll
+        for (int c = 0; c < 5; ++c) s[c] = s0[c] / mx;
+      }
+      double el[5];
+      nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, lam, ed, s, &rel, &capped, el);
+      if (!capped && rel < 1e-5) {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) e[c] = el[c];
+      } else {
+        apply_smem<NEXP, kTauSmem>(msm, tsm, bs, p, s, e);
+      }
+    } else {
+      const double mx = max_resolved<kTauSmem>(msm, tsm, bs, p, s);
+      if (mx < 1e-10) status |= kStatusMaxRssTiny;
+#pragma unroll
+      for (int c = 0; c < 5; ++c) s[c] /= mx;
+      nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, lam, ed, s, &rel, &capped);
+      apply_smem<NEXP, kTauSmem>(msm, tsm, bs, p, s, e);
     }
-    nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, lam, ed, s, &rel, &capped);
     capped_count += capped ? 1 : 0;
-    double e[5];
-    apply_smem<NEXP, kTauSmem>(msm, tsm, bs, p, s, e);
     double P[5];
 #pragma unroll
     for (int i = 0; i < 5; ++i) {
@@ -194,7 +218,7 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
 }
 
 template <typename S, typename MS, int NEXP, bool kTauSmem>
-__global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
+__global__ void __launch_bounds__(kVoxelBlock, nr_batch_min_blocks<MS>())
     k_nr_update_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
   int lb;
   const SlotDesc<S>& d = desc[batch_slot(bl, blockIdx.x, &lb)];
@@ -431,6 +455,7 @@ static NRParams batch_params(const MaterialParams& mp, const double edot[5], con
   p.eps = eps;
   p.max_rss = max_rss;
   p.max_iter = max_iter;
+  set_fp32_copies(p);
   return p;
 }
 
