@@ -74,12 +74,13 @@ __device__ T* line_fft(T* a, T* b, const T* tw, const LinePlan& pl, int nlines, 
     const int nb = n / Rr;
     const int total = nb * nlines;
     const int tws = n / (Ns * Rr);
+    const FastDiv dnb = pl.by_nb[st], dns = pl.by_ns[st];
     for (int t = threadIdx.x; t < total; t += blockDim.x) {
-      const int line = t / nb;
+      const int line = (int)fast_div((uint32_t)t, dnb);
       const int j = t - line * nb;
       const T* in = a + line * ls;
       T* out = b + line * ls;
-      const int jm = j % Ns;
+      const int jm = j - (int)fast_div((uint32_t)j, dns) * Ns;
       const int e = jm * tws;
       const int od = (j - jm) * Rr + jm;
       if (Rr == 4) {
@@ -280,7 +281,7 @@ __device__ __forceinline__ void pass_z_c2r_body(const typename CX<S>::T* __restr
   __syncthreads();
   // packed full lines: Z = A_even + i A_odd, Hermitian extension for k >= nh
   for (int i = threadIdx.x; i < npair * nz; i += blockDim.x) {
-    const int p = i / nz, k = i - p * nz;
+    const int p = (int)fast_div((uint32_t)i, pl.by_n), k = i - p * nz;
     const bool cj = k >= nh;
     const int kk = cj ? nz - k : k;
     T Ae = b[(2 * p) * hs + kk];
@@ -389,7 +390,7 @@ __device__ __forceinline__ void pass_x_body(typename CX<R>::T* __restrict__ B, c
   }
   if (MODE == 2) {
     for (int i = threadIdx.x; i < TK * nx; i += blockDim.x) {
-      const int kl = i / nx, xx = i - kl * nx;
+      const int kl = (int)fast_div((uint32_t)i, pl.by_n), xx = i - kl * nx;
       if (kl >= tk) continue;
       R pre[5], pim[5];
 #pragma unroll

@@ -42,7 +42,15 @@ bool make_line_plan(int n, LinePlan* p) {
       p->rad[p->nrad++] = r;
       m /= r;
     }
-  return m == 1;
+  if (m != 1) return false;
+  p->by_n = make_fast_div((uint32_t)n);
+  int ns = 1;
+  for (int st = 0; st < p->nrad; ++st) {
+    p->by_nb[st] = make_fast_div((uint32_t)(n / p->rad[st]));
+    p->by_ns[st] = make_fast_div((uint32_t)ns);
+    ns *= p->rad[st];
+  }
+  return true;
 }
 
 // Neumaier (improved Kahan) accumulator; combined pairwise in a fixed tree.

@@ -51,10 +51,32 @@ struct IterCtrl {
 };
 enum : int32_t { kStatusMaxRssTiny = 1, kStatusNonFinite = 2 };
 
+// Division of 32-bit unsigned t < 2^31 by a fixed d >= 1 without a divide:
+// q = (umulhi(t, mul) + t) >> shift, with shift = ceil(log2 d) and
+// mul = floor(2^32 (2^shift - d) / d) + 1 (the round-up multiply method).
+struct FastDiv {
+  uint32_t mul;
+  uint32_t shift;
+};
+inline FastDiv make_fast_div(uint32_t d) {
+  uint32_t l = 0;
+  while ((1ull << l) < d) ++l;
+  const uint64_t m = (((1ull << l) - d) << 32) / d + 1;
+  return FastDiv{(uint32_t)m, l};
+}
+#ifdef __CUDACC__
+__device__ __forceinline__ uint32_t fast_div(uint32_t t, const FastDiv& f) {
+  return (__umulhi(t, f.mul) + t) >> f.shift;
+}
+#endif
+
 struct LinePlan {
   int n;
   int nrad;
   int rad[16];
+  FastDiv by_n;          // division by n
+  FastDiv by_nb[16];     // by n / rad[st]  (butterflies per line in stage st)
+  FastDiv by_ns[16];     // by the stage's span Ns = rad[0] * ... * rad[st-1]
 };
 bool make_line_plan(int n, LinePlan* p);
 
