@@ -565,7 +565,8 @@ __device__ __forceinline__ void green_apply(const GreenParams<R>& gp, int ix, in
     for (int c = 0; c < 5; ++c) pre[c] = pim[c] = R(0);
     return;
   }
-  const int mx = (gp.nx - ix) % gp.nx, my = (gp.ny - iy) % gp.ny, mz = (gp.nz - iz) % gp.nz;
+  // index of -k (indices are in [0, n))
+  const int mx = ix ? gp.nx - ix : 0, my = iy ? gp.ny - iy : 0, mz = iz ? gp.nz - iz : 0;
   const bool ovk = nyq_override(ix, gp.nx) || nyq_override(iy, gp.ny) || nyq_override(iz, gp.nz);
   const bool ovm = nyq_override(mx, gp.nx) || nyq_override(my, gp.ny) || nyq_override(mz, gp.nz);
   const R wg = R(0.5) * R((ovk ? 0 : 1) + (ovm ? 0 : 1));  // weight of Gamma
@@ -575,7 +576,11 @@ __device__ __forceinline__ void green_apply(const GreenParams<R>& gp, int ix, in
     R k0 = R(ix > gp.nx / 2 ? ix - gp.nx : ix) * gp.inv_len[0];
     R k1 = R(iy > gp.ny / 2 ? iy - gp.ny : iy) * gp.inv_len[1];
     R k2 = R(iz > gp.nz / 2 ? iz - gp.nz : iz) * gp.inv_len[2];
-    const R il = R(1) / sqrt(k0 * k0 + k1 * k1 + k2 * k2);
+    R il;
+    if constexpr (sizeof(R) == 4)
+      il = rsqrtf(k0 * k0 + k1 * k1 + k2 * k2);
+    else
+      il = R(1) / sqrt(k0 * k0 + k1 * k1 + k2 * k2);
     k0 *= il;
     k1 *= il;
     k2 *= il;

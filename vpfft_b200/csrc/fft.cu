@@ -227,7 +227,7 @@ __device__ __forceinline__ void pass_z_r2c_body(const S* __restrict__ W,
   const S* src = W + ((long long)(c * nx + x) * ny + y0) * nz;
   copy_rows<S>(
       2 * npair, nz,
-      [&](int l, int z) { return l < ty ? src[(long long)l * nz + z] : S(0); },
+      [&](int l, int z) { return l < ty ? src[l * nz + z] : S(0); },
       [&](int l, int z, S v) { reinterpret_cast<S*>(&a[(l >> 1) * ls + z])[l & 1] = v; });
   __syncthreads();
   const T* r = line_fft<-1>(a, b, tw, pl, npair, ls);
@@ -249,7 +249,7 @@ __device__ __forceinline__ void pass_z_r2c_body(const S* __restrict__ W,
         return o;
       },
       [&](int k, int l, T v) {
-        if (l < ty) dst[(long long)k * ny + l] = v;
+        if (l < ty) dst[k * ny + l] = v;
       });
 }
 
@@ -276,7 +276,7 @@ __device__ __forceinline__ void pass_z_c2r_body(const typename CX<S>::T* __restr
   const T* src = A + ((long long)(c * nx + x) * nh) * ny + y0;
   const int hs = nh + 1;
   copy_short_rows<TY, T>(
-      nh, [&](int k, int l) { return l < ty ? src[(long long)k * ny + l] : T{S(0), S(0)}; },
+      nh, [&](int k, int l) { return l < ty ? src[k * ny + l] : T{S(0), S(0)}; },
       [&](int k, int l, T v) { b[l * hs + k] = v; });
   __syncthreads();
   // packed full lines: Z = A_even + i A_odd, Hermitian extension for k >= nh
@@ -305,7 +305,7 @@ __device__ __forceinline__ void pass_z_c2r_body(const typename CX<S>::T* __restr
         const T Z = r[(l >> 1) * ls + z];
         return ((l & 1) ? Z.y : Z.x) * scale;
       },
-      [&](int l, int z, S v) { dst[(long long)l * nz + z] = v; });
+      [&](int l, int z, S v) { dst[l * nz + z] = v; });
 }
 
 // ---------------------------------------------------------------- y passes
@@ -327,16 +327,21 @@ __device__ __forceinline__ void pass_y_body(const typename CX<R>::T* __restrict_
   const int x0 = bx * TX, kz = by, c = bz;
   const int tx = min(TX, nx - x0);
   // A line (c, x, kz) starts at ((c*nx + x)*nh + kz)*ny; B row (c, kz, ky) at ((c*nh + kz)*ny + ky)*nx
+  // (offsets below are < 2^31 for dimensions <= 512: 32-bit index arithmetic)
   const long long a_base = ((long long)(c * nx + x0) * nh + kz) * ny;
-  const long long a_xs = (long long)nh * ny;
+  const int a_xs = nh * ny;
   const long long b_base = ((long long)(c * nh + kz) * ny) * nx + x0;
+  const T* in_a = in + a_base;
+  const T* in_b = in + b_base;
+  T* out_a = out + a_base;
+  T* out_b = out + b_base;
   if (SIGN < 0) {
     copy_rows<T>(
-        TX, ny, [&](int xl, int y) { return xl < tx ? in[a_base + xl * a_xs + y] : T{R(0), R(0)}; },
+        TX, ny, [&](int xl, int y) { return xl < tx ? in_a[xl * a_xs + y] : T{R(0), R(0)}; },
         [&](int xl, int y, T v) { a[xl * ls + y] = v; });
   } else {
     copy_short_rows<TX, T>(
-        ny, [&](int y, int xl) { return xl < tx ? in[b_base + (long long)y * nx + xl] : T{R(0), R(0)}; },
+        ny, [&](int y, int xl) { return xl < tx ? in_b[y * nx + xl] : T{R(0), R(0)}; },
         [&](int y, int xl, T v) { a[xl * ls + y] = v; });
   }
   __syncthreads();
@@ -345,12 +350,12 @@ __device__ __forceinline__ void pass_y_body(const typename CX<R>::T* __restrict_
     copy_short_rows<TX, T>(
         ny, [&](int y, int xl) { return r[xl * ls + y]; },
         [&](int y, int xl, T v) {
-          if (xl < tx) out[b_base + (long long)y * nx + xl] = v;
+          if (xl < tx) out_b[y * nx + xl] = v;
         });
   } else {
     copy_rows<T>(
         tx, ny, [&](int xl, int y) { return r[xl * ls + y]; },
-        [&](int xl, int y, T v) { out[a_base + xl * a_xs + y] = v; });
+        [&](int xl, int y, T v) { out_a[xl * a_xs + y] = v; });
   }
 }
 
@@ -371,14 +376,15 @@ __device__ __forceinline__ void pass_x_body(typename CX<R>::T* __restrict__ B, c
   load_twiddles(tw, twg, nx);
   const int ky0 = bx * TK, kz = by;
   const int tk = min(TK, ny - ky0);
-  const long long cs = (long long)nh * ny * nx;  // component stride
-  const long long base = ((long long)kz * ny + ky0) * nx;
+  // component stride and the block's offset: < 2^31 for dimensions <= 512
+  const int cs = nh * ny * nx;
+  T* Bb = B + ((long long)kz * ny + ky0) * nx;
   const int nl = ncomp * TK;
   copy_rows<T>(
       nl, nx,
       [&](int L, int xx) {
         const int c = L / TK, kl = L - c * TK;
-        return kl < tk ? B[c * cs + base + (long long)kl * nx + xx] : T{R(0), R(0)};
+        return kl < tk ? Bb[c * cs + kl * nx + xx] : T{R(0), R(0)};
       },
       [&](int L, int xx, T v) { a[L * ls + xx] = v; });
   __syncthreads();
@@ -410,7 +416,7 @@ __device__ __forceinline__ void pass_x_body(typename CX<R>::T* __restrict__ B, c
       nl, nx, [&](int L, int xx) { return r[L * ls + xx]; },
       [&](int L, int xx, T v) {
         const int c = L / TK, kl = L - c * TK;
-        if (kl < tk) B[c * cs + base + (long long)kl * nx + xx] = v;
+        if (kl < tk) Bb[c * cs + kl * nx + xx] = v;
       });
 }
 

@@ -86,6 +86,8 @@ struct NRParams {
   float n_f[kNS];
   float eps_f;
   float max_rss_f;
+  float L0inv_f[15];
+  float pad_f_;
 };
 
 // Fills the FP32 copies of the per-system constants from the FP64 values.
@@ -97,6 +99,7 @@ __host__ __device__ inline void set_fp32_copies(NRParams& p) {
   }
   p.eps_f = (float)p.eps;
   p.max_rss_f = (float)p.max_rss;
+  for (int k = 0; k < 15; ++k) p.L0inv_f[k] = (float)p.L0inv[k];
 }
 
 // The per-system constants in the arithmetic type of a Newton pass.
@@ -122,30 +125,52 @@ __host__ __device__ constexpr int sym5(int i, int j) {
   return i <= j ? (i * (9 - i)) / 2 + j : (j * (9 - j)) / 2 + i;
 }
 
-// Rotated Schmid 5-vectors of one voxel into shared memory (see schmid_from_R).
+// Shared-memory layout of a thread's Schmid 5-vectors m(q, c) and reciprocal
+// CRSS t(q), relative to the thread's base pointer (base + kThreadStride * tid):
+// FP64 staging, one value per thread per row ([(q*5+c)*bs], [q*bs]); FP32
+// staging, systems q and q+1 interleaved so that one 8-byte load returns
+// (m(q, c), m(q+1, c)) for the paired FP32 arithmetic of the Newton predictor.
 template <typename MS>
-__device__ __forceinline__ void schmid_to_smem(const double R[9], MS* msm, int bs) {
+struct SL;
+template <>
+struct SL<double> {
+  static constexpr int kThreadStride = 1;
+  __device__ static int m(int q, int c, int bs) { return (q * 5 + c) * bs; }
+  __device__ static int t(int q, int bs) { return q * bs; }
+};
+template <>
+struct SL<float> {
+  static constexpr int kThreadStride = 2;
+  __device__ static int m(int q, int c, int bs) { return ((q >> 1) * 5 + c) * 2 * bs + (q & 1); }
+  __device__ static int t(int q, int bs) { return (q >> 1) * 2 * bs + (q & 1); }
+};
+
+// Rotated Schmid 5-vectors of one voxel into shared memory (see schmid_from_R),
+// computed in the staging precision MS (FP64 path: double; mixed: float).
+template <typename MS>
+__device__ __forceinline__ void schmid_to_smem(const MS R[9], MS* msm, int bs) {
 #pragma unroll
   for (int s = 0; s < kNS; ++s) {
-    double b[3], n[3];
+    MS b[3], n[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
       b[i] = R[3 * i + 0] * slip_b(s, 0) + R[3 * i + 1] * slip_b(s, 1) + R[3 * i + 2] * slip_b(s, 2);
       n[i] = R[3 * i + 0] * slip_n(s, 0) + R[3 * i + 1] * slip_n(s, 1) + R[3 * i + 2] * slip_n(s, 2);
     }
-    const double q00 = b[0] * n[0], q11 = b[1] * n[1], q22 = b[2] * n[2];
-    msm[(s * 5 + 0) * bs] = (MS)((q11 - q00) * VPFFT_INV_2SQRT3);
-    msm[(s * 5 + 1) * bs] = (MS)((2.0 * q22 - q00 - q11) * (1.0 / 6.0));
-    msm[(s * 5 + 2) * bs] = (MS)((b[1] * n[2] + b[2] * n[1]) * VPFFT_INV_2SQRT3);
-    msm[(s * 5 + 3) * bs] = (MS)((b[0] * n[2] + b[2] * n[0]) * VPFFT_INV_2SQRT3);
-    msm[(s * 5 + 4) * bs] = (MS)((b[0] * n[1] + b[1] * n[0]) * VPFFT_INV_2SQRT3);
+    const MS q00 = b[0] * n[0], q11 = b[1] * n[1], q22 = b[2] * n[2];
+    const MS c23 = (MS)VPFFT_INV_2SQRT3, c6 = (MS)(1.0 / 6.0);
+    msm[SL<MS>::m(s, 0, bs)] = (q11 - q00) * c23;
+    msm[SL<MS>::m(s, 1, bs)] = (MS(2) * q22 - q00 - q11) * c6;
+    msm[SL<MS>::m(s, 2, bs)] = (b[1] * n[2] + b[2] * n[1]) * c23;
+    msm[SL<MS>::m(s, 3, bs)] = (b[0] * n[2] + b[2] * n[0]) * c23;
+    msm[SL<MS>::m(s, 4, bs)] = (b[0] * n[1] + b[1] * n[0]) * c23;
   }
 }
 
 template <typename MS>
 __device__ __forceinline__ void load_m(const MS* msm, int bs, int s, double m[5]) {
 #pragma unroll
-  for (int c = 0; c < 5; ++c) m[c] = (double)msm[(s * 5 + c) * bs];
+  for (int c = 0; c < 5; ++c) m[c] = (double)msm[SL<MS>::m(s, c, bs)];
 }
 
 // LDL^T solve of a symmetric positive-definite 5x5 A (packed upper) x = b.
@@ -193,7 +218,7 @@ __device__ __forceinline__ bool ldlt5_solve(const T A[15], const T b[5], T x[5])
 template <bool kTauSmem, typename MS>
 __device__ __forceinline__ double itau_of(const MS* tsm, int bs, const NRParams& p, int q) {
   if constexpr (kTauSmem)
-    return (double)tsm[q * bs];
+    return (double)tsm[SL<MS>::t(q, bs)];
   else
     return p.icrss[q];
 }
@@ -217,10 +242,10 @@ __device__ __forceinline__ bool accumulate(const MS* msm, const MS* tsm, int bs,
   for (int q = 0; q < kNS; ++q) {
     T m[5];
 #pragma unroll
-    for (int c = 0; c < 5; ++c) m[c] = (T)msm[(q * 5 + c) * bs];
+    for (int c = 0; c < 5; ++c) m[c] = (T)msm[SL<MS>::m(q, c, bs)];
     T it;
     if constexpr (kTauSmem)
-      it = (T)tsm[q * bs];
+      it = (T)tsm[SL<MS>::t(q, bs)];
     else
       it = C::icrss(p, q);
     T r = (m[0] * s[0] + m[1] * s[1] + m[2] * s[2] + m[3] * s[3] + m[4] * s[4]) * it;
@@ -245,6 +270,82 @@ __device__ __forceinline__ bool accumulate(const MS* msm, const MS* tsm, int bs,
   return adm;
 }
 
+// x^E for both lanes of a float2 (E >= 0 at compile time), paired multiplies.
+template <int E>
+__device__ __forceinline__ float2 cpow2(float2 x) {
+  if constexpr (E == 0) {
+    return make_float2(1.f, 1.f);
+  } else if constexpr (E == 1) {
+    return x;
+  } else {
+    const float2 h = cpow2<E / 2>(x);
+    if constexpr (E & 1)
+      return __fmul2_rn(__fmul2_rn(h, h), x);
+    else
+      return __fmul2_rn(h, h);
+  }
+}
+
+// The predictor's pass over the systems with paired FP32 arithmetic: lane 0
+// of every float2 carries system q, lane 1 system q+1 (FFMA2/FMUL2 issue two
+// FMAs per instruction); the two partial sums of S and K are added at the end.
+// Compile-time rate exponent NEXP > 1 (the power branch of Solvers.cpp:177).
+template <int NEXP, bool kTauSmem>
+__device__ __forceinline__ bool accumulate_pairs(const float* msm, const float* tsm, int bs,
+                                                 const NRParams& p, const float s[5], float S[5],
+                                                 float K[15], float* rmax) {
+  static_assert(NEXP > 1, "paired predictor needs a compile-time exponent > 1");
+  const float2* m2p = reinterpret_cast<const float2*>(msm);
+  const float2* t2p = reinterpret_cast<const float2*>(tsm);
+  float2 S2[5], K2[15], s2[5];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) {
+    S2[c] = make_float2(0.f, 0.f);
+    s2[c] = make_float2(s[c], s[c]);
+  }
+#pragma unroll
+  for (int k = 0; k < 15; ++k) K2[k] = make_float2(0.f, 0.f);
+  const float2 nn = make_float2((float)NEXP, (float)NEXP);
+  const float mr = p.max_rss_f;
+  bool adm = true;
+  float rm = 0.f;
+#pragma unroll 2
+  for (int pq = 0; pq < kNS / 2; ++pq) {
+    float2 m[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) m[c] = m2p[(pq * 5 + c) * bs];
+    float2 it;
+    if constexpr (kTauSmem)
+      it = t2p[pq * bs];
+    else
+      it = make_float2(p.icrss_f[2 * pq], p.icrss_f[2 * pq + 1]);
+    float2 r = __fmul2_rn(m[0], s2[0]);
+#pragma unroll
+    for (int c = 1; c < 5; ++c) r = __ffma2_rn(m[c], s2[c], r);
+    r = __fmul2_rn(r, it);
+    const float ax = fabsf(r.x), ay = fabsf(r.y);
+    adm = adm && !(ax > mr) && !(ay > mr);
+    rm = fmaxf(rm, fmaxf(ax, ay));
+    const float2 pw = cpow2<NEXP - 1>(make_float2(ax, ay));
+    const float2 g = __fmul2_rn(make_float2(p.gdot_f[2 * pq], p.gdot_f[2 * pq + 1]), pw);
+    const float2 gr = __fmul2_rn(g, r);
+    const float2 w = __fmul2_rn(__fmul2_rn(nn, g), it);
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      S2[i] = __ffma2_rn(m[i], gr, S2[i]);
+      const float2 mw = __fmul2_rn(m[i], w);
+#pragma unroll
+      for (int j = i; j < 5; ++j) K2[sym5(i, j)] = __ffma2_rn(mw, m[j], K2[sym5(i, j)]);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 5; ++c) S[c] = S2[c].x + S2[c].y;
+#pragma unroll
+  for (int k = 0; k < 15; ++k) K[k] = K2[k].x + K2[k].y;
+  *rmax = rm;
+  return adm;
+}
+
 // Newton predictor of the constrained solve in FP32 (mixed precision only):
 // the reference's iteration and stopping rule in single precision.  Returns
 // true and the iterate in s_io when it converged with finite values; the
@@ -265,8 +366,11 @@ __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, in
   *rmax0 = 0.f;
   for (int it = 0; it < max_steps; ++it) {
     float S[5], K[15], rm;
-    const bool adm =
-        accumulate<NEXP, false, kTauSmem, float, MS, true>(msm, tsm, bs, p, cur, S, K, &rm);
+    bool adm;
+    if constexpr (NEXP > 1 && sizeof(MS) == 4)
+      adm = accumulate_pairs<NEXP, kTauSmem>(msm, tsm, bs, p, cur, S, K, &rm);
+    else
+      adm = accumulate<NEXP, false, kTauSmem, float, MS, true>(msm, tsm, bs, p, cur, S, K, &rm);
     if (it == 0) *rmax0 = rm;
     if (!adm) return false;
     float y[5];

@@ -34,12 +34,13 @@ constexpr int nr_batch_min_blocks() {
 template <bool kTauSmem, typename S, typename MS>
 __device__ __forceinline__ void voxel_schmid(const FieldPtrs<S>& f, long long n, long long v,
                                              MS* msm, MS* tsm, int bs) {
-  double R[9];
-  load_R(f.R, n, v, R);
-  schmid_to_smem(R, msm, bs);
+  MS R[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) R[k] = (MS)f.R[k * n + v];
+  schmid_to_smem<MS>(R, msm, bs);
   if constexpr (kTauSmem) {
 #pragma unroll
-    for (int q = 0; q < kNS; ++q) tsm[q * bs] = (MS)(1.0 / (double)f.crss[q * n + v]);
+    for (int q = 0; q < kNS; ++q) tsm[SL<MS>::t(q, bs)] = (MS)(1.0 / (double)f.crss[q * n + v]);
   }
 }
 
@@ -83,7 +84,7 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
     k_init(const __grid_constant__ NRParams p, const __grid_constant__ FieldPtrs<S> f,
            IterCtrl* ctrl) {
   extern __shared__ __align__(16) unsigned char nr_smem[];
-  MS* msm = reinterpret_cast<MS*>(nr_smem) + threadIdx.x;
+  MS* msm = reinterpret_cast<MS*>(nr_smem) + SL<MS>::kThreadStride * threadIdx.x;
   MS* tsm = msm + 60 * blockDim.x;
   init_body<S, MS, NEXP, kTauSmem>(p, f, ctrl, blockIdx.x, gridDim.x, msm, tsm);
 }
@@ -101,7 +102,7 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_batch_min_blocks<MS>())
   copy_struct(&sp, &d.nr_init);
   copy_struct(&sf, &d.f);
   __syncthreads();
-  MS* msm = reinterpret_cast<MS*>(nr_smem) + threadIdx.x;
+  MS* msm = reinterpret_cast<MS*>(nr_smem) + SL<MS>::kThreadStride * threadIdx.x;
   MS* tsm = msm + 60 * blockDim.x;
   init_body<S, MS, NEXP, kTauSmem>(sp, sf, d.ctrl, lb, d.init_blocks, msm, tsm);
 }
@@ -143,9 +144,8 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const FieldPtr
       // FP64 residual and Jacobian).  If the predictor fails, the FP64 solve
       // starts where the reference's does, at sigma / MaxRSS.  The strain rate
       // comes from the last Newton linearisation when that step was tiny.
-      float L0i[15], mx0;
-#pragma unroll
-      for (int k = 0; k < 15; ++k) L0i[k] = (float)p.L0inv[k];
+      float mx0;
+      const float* L0i = p.L0inv_f;
       double s0[5];
 #pragma unroll
       for (int c = 0; c < 5; ++c) s0[c] = s[c];
@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
                 double* partials, IterCtrl* ctrl) {
   if (ctrl->done) return;
   extern __shared__ __align__(16) unsigned char nr_smem[];
-  MS* msm = reinterpret_cast<MS*>(nr_smem) + threadIdx.x;
+  MS* msm = reinterpret_cast<MS*>(nr_smem) + SL<MS>::kThreadStride * threadIdx.x;
   MS* tsm = msm + 60 * blockDim.x;
   nr_update_body<S, MS, NEXP, kTauSmem>(p, f, partials, ctrl, blockIdx.x, gridDim.x, msm, tsm);
 }
@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_batch_min_blocks<MS>())
   copy_struct(&sp, &d.nr);
   copy_struct(&sf, &d.f);
   __syncthreads();
-  MS* msm = reinterpret_cast<MS*>(nr_smem) + threadIdx.x;
+  MS* msm = reinterpret_cast<MS*>(nr_smem) + SL<MS>::kThreadStride * threadIdx.x;
   MS* tsm = msm + 60 * blockDim.x;
   nr_update_body<S, MS, NEXP, kTauSmem>(sp, sf, d.partials, d.ctrl, lb, d.nr_blocks, msm, tsm);
 }
