@@ -654,7 +654,7 @@ def main(argv=None):
 # divided by the voxel count) from the ncu capture at 192^3 summarised in
 # profiles/k_nr_update_192cubed_mixed.md; the kernel's traffic is proportional to
 # the voxel count (it streams each voxel's fields once), so it scales to 256^3.
-TRAFFIC_PER_VOXEL: dict = {("mixed", "nr_update"): (682.147328e6 + 377.704704e6) / 192 ** 3}
+TRAFFIC_PER_VOXEL: dict = {("mixed", "nr_update"): (680.249088e6 + 380.631808e6) / 192 ** 3}
 
 
 if __name__ == "__main__":
