@@ -73,28 +73,38 @@ __device__ __forceinline__ Neu neu_merge(Neu a, Neu b) {
 }
 
 
-// Column sums of partials[nparts][width] with compensated, fixed-order
-// summation; one block.
-__device__ void column_sums(const double* partials, int nparts, int width, double* out) {
+// Sum of column col of partials[nparts][width] with compensated, fixed-order
+// summation (thread-strided Neumaier sums, then a fixed pairwise tree); one
+// block of kFinishThreads threads.
+__device__ void column_sum(const double* partials, int nparts, int width, int col, double* out) {
   __shared__ double ss[kFinishThreads], sc[kFinishThreads];
-  for (int col = 0; col < width; ++col) {
-    Neu a{0.0, 0.0};
-    for (int i = threadIdx.x; i < nparts; i += kFinishThreads) neu_add(a, partials[(long long)i * width + col]);
-    ss[threadIdx.x] = a.s;
-    sc[threadIdx.x] = a.c;
-    __syncthreads();
-    for (int off = kFinishThreads / 2; off > 0; off >>= 1) {
-      if (threadIdx.x < off) {
-        Neu x{ss[threadIdx.x], sc[threadIdx.x]}, y{ss[threadIdx.x + off], sc[threadIdx.x + off]};
-        Neu z = neu_merge(x, y);
-        ss[threadIdx.x] = z.s;
-        sc[threadIdx.x] = z.c;
-      }
-      __syncthreads();
+  Neu a{0.0, 0.0};
+  for (int i = threadIdx.x; i < nparts; i += kFinishThreads) neu_add(a, partials[(long long)i * width + col]);
+  ss[threadIdx.x] = a.s;
+  sc[threadIdx.x] = a.c;
+  __syncthreads();
+  for (int off = kFinishThreads / 2; off > 0; off >>= 1) {
+    if (threadIdx.x < off) {
+      Neu x{ss[threadIdx.x], sc[threadIdx.x]}, y{ss[threadIdx.x + off], sc[threadIdx.x + off]};
+      Neu z = neu_merge(x, y);
+      ss[threadIdx.x] = z.s;
+      sc[threadIdx.x] = z.c;
     }
-    if (threadIdx.x == 0) out[col] = ss[0] + sc[0];
     __syncthreads();
   }
+  if (threadIdx.x == 0) out[col] = ss[0] + sc[0];
+  __syncthreads();
+}
+
+// All columns, one after the other, in one block.
+__device__ void column_sums(const double* partials, int nparts, int width, double* out) {
+  for (int col = 0; col < width; ++col) column_sum(partials, nparts, width, col, out);
+}
+
+// One block per column (the same per-column order as column_sums).
+__global__ void __launch_bounds__(kFinishThreads)
+    k_column_sums_cols(const double* partials, int nparts, int width, double* out) {
+  column_sum(partials, nparts, width, blockIdx.x, out);
 }
 
 __global__ void k_column_sums(const double* partials, int nparts, int width, double* out) {
@@ -175,12 +185,13 @@ __global__ void __launch_bounds__(kVoxelBlock)
   ref_medium_body<S>(sp, sf, d.partials, lb);
 }
 
-// Per-slot column sums of the reference-medium partials (one block per slot).
+// Per-slot column sums of the reference-medium partials (block (slot, column)).
 template <typename S>
 __global__ void __launch_bounds__(kFinishThreads)
     k_column_sums_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
   const SlotDesc<S>& d = desc[bl.slot[blockIdx.x]];
-  column_sums(d.partials, (int)((d.vox.n + kVoxelBlock - 1) / kVoxelBlock), 25, d.sum25);
+  column_sum(d.partials, (int)((d.vox.n + kVoxelBlock - 1) / kVoxelBlock), 25, blockIdx.y,
+             d.sum25);
 }
 
 // Reductions and convergence test of one iteration (MaterialGrid.cpp:1009-1068).
@@ -386,7 +397,7 @@ int launch_ref_medium(const VoxelParams& p, const FieldPtrs<S>& f, double* parti
                       double* out25, cudaStream_t st) {
   const int nb = ref_medium_blocks(p.n);
   k_ref_medium<S><<<nb, kVoxelBlock, 0, st>>>(p, f, partials);
-  k_column_sums<<<1, kFinishThreads, 0, st>>>(partials, nb, 25, out25);
+  k_column_sums_cols<<<25, kFinishThreads, 0, st>>>(partials, nb, 25, out25);
   return 2;
 }
 template <typename S>
@@ -394,7 +405,7 @@ int launch_ref_medium_batch(const SlotDesc<S>* d, const BatchLaunch& bl, const B
                             cudaStream_t st) {
   if (bl.blocks <= 0) return 0;
   k_ref_medium_batch<S><<<bl.blocks, kVoxelBlock, 0, st>>>(d, bl);
-  k_column_sums_batch<S><<<bls.m, kFinishThreads, 0, st>>>(d, bls);
+  k_column_sums_batch<S><<<dim3(bls.m, 25), kFinishThreads, 0, st>>>(d, bls);
   return 2;
 }
 template <typename S>

@@ -561,6 +561,61 @@ __device__ __forceinline__ int nr_unconstrained_smem(const MS* msm, const MS* ts
   return steps;
 }
 
+// Newton predictor of the unconstrained solve in FP32 (mixed precision only):
+// the reference's iteration (Solvers.cpp:19-101: admissibility back-off towards
+// the previous iterate, K delta = -(S - Edot), stop at 2|delta|/|new + old| <
+// eps) in single precision.  Returns true with the iterate in s_io when it
+// converged; the caller then runs the FP64 iteration from there.
+template <int NEXP, bool kTauSmem, typename MS>
+__device__ __forceinline__ bool nr_predict_unconstrained_fp32(const MS* msm, const MS* tsm,
+                                                              int bs, const NRParams& p,
+                                                              const double edot[5],
+                                                              double s_io[5], int max_steps) {
+  float cur[5], saved[5], e32[5];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) {
+    cur[c] = (float)s_io[c];
+    saved[c] = 0.f;
+    e32[c] = (float)edot[c];
+  }
+  for (int it = 0; it < max_steps; ++it) {
+    float S[5], K[15], rm;
+    for (int back = 0;; ++back) {
+      bool adm;
+      if constexpr (NEXP > 1 && sizeof(MS) == 4)
+        adm = accumulate_pairs<NEXP, kTauSmem>(msm, tsm, bs, p, cur, S, K, &rm);
+      else
+        adm = accumulate<NEXP, false, kTauSmem, float, MS, true>(msm, tsm, bs, p, cur, S, K, &rm);
+      if (adm) break;
+      if (back >= 40) return false;
+#pragma unroll
+      for (int c = 0; c < 5; ++c) cur[c] = saved[c] + (cur[c] - saved[c]) * 0.2f;
+    }
+    float mres[5], delta[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) mres[c] = e32[c] - S[c];
+    if (!ldlt5_solve(K, mres, delta)) return false;
+    float dn = 0.f, sn = 0.f;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      saved[c] = cur[c];
+      const float nw = cur[c] + delta[c];
+      const float sm = nw + cur[c];
+      dn += delta[c] * delta[c];
+      sn += sm * sm;
+      cur[c] = nw;
+    }
+    const float rel = 2.f * sqrtf(dn) / sqrtf(sn);
+    if (!isfinite(rel)) return false;
+    if (rel < p.eps_f) {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) s_io[c] = (double)cur[c];
+      return true;
+    }
+  }
+  return false;
+}
+
 // GetMaxRSS (MaterialGrid.h:550-566) and the Sachs bound (Solvers.cpp:234-240):
 // max_s |m_s . x| / tau_s
 template <bool kTauSmem, typename MS>

@@ -69,6 +69,11 @@ __device__ __forceinline__ void init_body(const NRParams& p, const FieldPtrs<S>&
     // a zero strain rate makes the Sachs guess 0/0 (Solvers.cpp:241)
     if (!isfinite(mx)) status |= kStatusNonFinite;
     bool capped;
+    if constexpr (sizeof(S) == 4) {
+      // mixed precision: FP32 Newton predictor from the Sachs guess, then the
+      // reference's FP64 iteration from its iterate (from the guess if it failed)
+      nr_predict_unconstrained_fp32<NEXP, kTauSmem>(msm, tsm, bs, p, p.edot, g, 60);
+    }
     nr_unconstrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, p.edot, g, &capped);
     capped_count += capped ? 1 : 0;
     store5(f.sigma, n, v, g);
