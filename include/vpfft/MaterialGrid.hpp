@@ -114,6 +114,12 @@ class MaterialGrid {
   std::vector<EigenRep> LagrangeMultiplier() { return fetch<EigenRep>(VPFFT_FIELD_LAGRANGE); }
   std::vector<SMatrix3x3> Orientation() { return fetch<SMatrix3x3>(VPFFT_FIELD_ORIENTATION); }
 
+  // Print* text dumps (MaterialGrid.cpp:15-100), byte-compatible
+  void PrintStrain(const std::string& f) { print(VPFFT_PRINT_STRAIN, f); }
+  void PrintStress(const std::string& f) { print(VPFFT_PRINT_STRESS, f); }
+  void PrintLagrangeMultiplier(const std::string& f) { print(VPFFT_PRINT_LAGRANGE, f); }
+  void PrintPolarization(const std::string& f) { print(VPFFT_PRINT_POLARIZATION, f); }
+
   vpfft_grid* handle() { return g_; }
 
  private:
@@ -122,6 +128,9 @@ class MaterialGrid {
     std::vector<T> v((size_t)DimX_ * DimY_ * DimZ_);
     detail::check(vpfft_grid_get_field(g_, f, reinterpret_cast<double*>(v.data())), g_);
     return v;
+  }
+  void print(vpfft_print_kind k, const std::string& f) {
+    detail::check(vpfft_grid_print(g_, k, f.c_str()), g_);
   }
   int DimX_, DimY_, DimZ_;
   vpfft_grid* g_ = nullptr;

@@ -345,6 +345,37 @@ vpfft_status vpfft_batch_cancel(vpfft_batch *b, int64_t request_id);
 vpfft_status vpfft_batch_get_info(const vpfft_batch *b, vpfft_batch_info *info);
 const char *vpfft_batch_last_error(const vpfft_batch *b);
 
+/* ------------------------------------------------------------------ text I/O
+ * The reference's text formats, byte-compatible (numbers through C++ streams
+ * with the reference's defaults).  Host code: no device needed except for
+ * vpfft_grid_print. */
+typedef enum {
+  VPFFT_PRINT_STRAIN = 0,       /* MaterialGrid::PrintStrain (MaterialGrid.cpp:15-35): d~, re/im */
+  VPFFT_PRINT_STRESS = 1,       /* PrintStress (40-55) */
+  VPFFT_PRINT_LAGRANGE = 2,     /* PrintLagrangeMultiplier (60-75), x outermost */
+  VPFFT_PRINT_POLARIZATION = 3  /* PrintPolarization (80-100), re/im */
+} vpfft_print_kind;
+/* One line per voxel "x y z v0 v1 ..." from host arrays: re N x 5
+ * (voxel-major), im N x 5 or NULL (zeros) for the complex kinds. */
+vpfft_status vpfft_print_field(const char *path, vpfft_print_kind kind, int nx, int ny, int nz,
+                               const double *re, const double *im);
+/* The same from a grid's fields.  The imaginary parts are written as 0: the
+ * reference's P has none, and the imaginary part of its d~ (a by-product of
+ * its c2c transform that the algorithm never uses) is not formed here. */
+vpfft_status vpfft_grid_print(vpfft_grid *g, vpfft_print_kind kind, const char *path);
+/* UnitTester::WriteRandomMaterial / ReadRandomMaterial (UnitTester.cpp:116-167):
+ * per voxel (x outermost) the 9 orientation entries and the 5 stress values. */
+vpfft_status vpfft_write_random_material(const char *path, int nx, int ny, int nz,
+                                         const double *orientations, const double *stress);
+vpfft_status vpfft_read_random_material(const char *path, int nx, int ny, int nz,
+                                        double *orientations, double *stress);
+/* UnitTester::ReadRicardoData (UnitTester.cpp:237-265): N lines of
+ * "phi1 Phi phi2 x y z i j" (Euler angles in degrees, 1-based voxel indices,
+ * two ignored integers) -> active Euler matrices (LinearAlgebra.cpp:160-181)
+ * written into orientations (N x 9); indices out of range are an error. */
+vpfft_status vpfft_read_euler_texture(const char *path, int nx, int ny, int nz,
+                                      double *orientations);
+
 /* ------------------------------------------------------------------ config
  * Utilities::ConfigFile (Config.h:21-85, Config.cpp:11-300) with its defects
  * fixed: slip-system lists are read into indices 0..11 (the reference writes

@@ -210,3 +210,32 @@ def test_c2_twenty_increments_with_hardening_and_texture(golden, lib):
                 assert voxel_rel(full[idx], g[f"inc{s}_{f}"]) <= 1e-7, (s, f)
     np.testing.assert_allclose(grid.VoxelLength(), g["voxlen"], rtol=1e-14)
     grid.close()
+
+
+def test_print_dumps_of_a_solved_grid(golden, lib, tmp_path):
+    """MaterialGrid::Print* of the device fields: the reference's layout (z
+    outermost for stress, x outermost for the Lagrange multiplier) and the
+    values of the grid at 6 significant digits."""
+    g = golden("c1_16")
+    grid = grid_of(g)
+    grid.RunSingleStrainStep(g["edot"], 3, float(g["dt"]), float(g["eps"]))
+    nx, ny, nz = (int(x) for x in g["dims"])
+    for name, get, zouter in (("PrintStress", grid.Stress, True),
+                              ("PrintLagrangeMultiplier", grid.LagrangeMultiplier, False),
+                              ("PrintPolarization", grid.PolarizationField, True),
+                              ("PrintStrain", grid.DisplacementVariation, True)):
+        path = tmp_path / f"{name}.txt"
+        getattr(grid, name)(str(path))
+        rows = [line.split() for line in path.read_text().splitlines()]
+        assert len(rows) == grid.N
+        ijk = np.array([[int(t) for t in r[:3]] for r in rows])
+        vals = np.array([[float(t) for t in r[3:]] for r in rows])
+        if vals.shape[1] == 10:  # re/im pairs; the imaginary parts are written as 0
+            assert np.all(vals[:, 1::2] == 0)
+            vals = vals[:, 0::2]
+        expect_first = (1, 0, 0) if zouter else (0, 0, 1)
+        assert tuple(ijk[1]) == expect_first
+        idx = (ijk[:, 0] * ny + ijk[:, 1]) * nz + ijk[:, 2]
+        ref = get()[idx]
+        np.testing.assert_allclose(vals, ref, rtol=6e-6, atol=1e-300)
+    grid.close()

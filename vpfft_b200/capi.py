@@ -50,6 +50,11 @@ FIELD_WIDTH = {0: 5, 1: 5, 2: 9, 3: 12, 4: 1, 5: 5, 6: 5, 7: 5, 8: 60}
 NUM_PHASES = 7
 NOALLOC_MAX_POINTS = 4096
 
+PRINT_STRAIN = 0
+PRINT_STRESS = 1
+PRINT_LAGRANGE = 2
+PRINT_POLARIZATION = 3
+
 
 class Material(C.Structure):
     _fields_ = [
@@ -212,6 +217,11 @@ _PROTOS = {
     "vpfft_batch_cancel": (C.c_int, [_G, C.c_int64]),
     "vpfft_batch_get_info": (C.c_int, [_G, C.POINTER(BatchInfo)]),
     "vpfft_batch_last_error": (C.c_char_p, [_G]),
+    "vpfft_print_field": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, _D, _D]),
+    "vpfft_grid_print": (C.c_int, [_G, C.c_int, C.c_char_p]),
+    "vpfft_write_random_material": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _D, _D]),
+    "vpfft_read_random_material": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _D, _D]),
+    "vpfft_read_euler_texture": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _D]),
     "vpfft_config_read": (C.c_int, [C.c_char_p, C.POINTER(Config), C.c_char_p, C.c_size_t]),
 }
 

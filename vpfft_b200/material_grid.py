@@ -188,6 +188,26 @@ class MaterialGrid:
     def SchmidtTensorList(self) -> np.ndarray:
         return self.field(capi.FIELD_SCHMID).reshape(self.N, 12, 5)
 
+    # ---------------------------------------------------------------- text dumps
+    def _print(self, kind: int, filename: str) -> None:
+        check(self._lib.vpfft_grid_print(self._h, kind, str(filename).encode()), self._h)
+
+    def PrintStrain(self, filename: str) -> None:
+        """MaterialGrid::PrintStrain (MaterialGrid.cpp:15-35)."""
+        self._print(capi.PRINT_STRAIN, filename)
+
+    def PrintStress(self, filename: str) -> None:
+        """MaterialGrid::PrintStress (MaterialGrid.cpp:40-55)."""
+        self._print(capi.PRINT_STRESS, filename)
+
+    def PrintLagrangeMultiplier(self, filename: str) -> None:
+        """MaterialGrid::PrintLagrangeMultiplier (MaterialGrid.cpp:60-75)."""
+        self._print(capi.PRINT_LAGRANGE, filename)
+
+    def PrintPolarization(self, filename: str) -> None:
+        """MaterialGrid::PrintPolarization (MaterialGrid.cpp:80-100)."""
+        self._print(capi.PRINT_POLARIZATION, filename)
+
     def launch_count(self) -> int:
         return int(self._lib.vpfft_grid_launch_count(self._h))
 
