@@ -376,6 +376,13 @@ vpfft_status vpfft_read_random_material(const char *path, int nx, int ny, int nz
 vpfft_status vpfft_read_euler_texture(const char *path, int nx, int ny, int nz,
                                       double *orientations);
 
+/* SMatrix3x3::BuildActiveEulerMatrix (LinearAlgebra.cpp:160-181), radians,
+ * with the reference's single-precision cosf/sinf. */
+vpfft_status vpfft_euler_matrix(double phi, double theta, double psi, double orientation[9]);
+/* The two-grain microstructure of the config's TwoGrainInit
+ * (UnitTester::SetMaterialGrid, UnitTester.cpp:46-74). */
+vpfft_status vpfft_fixture_two_grain(int nx, int ny, int nz, double *orientations);
+
 /* ------------------------------------------------------------------ config
  * Utilities::ConfigFile (Config.h:21-85, Config.cpp:11-300) with its defects
  * fixed: slip-system lists are read into indices 0..11 (the reference writes

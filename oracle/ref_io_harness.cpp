@@ -13,6 +13,7 @@
 //   texture.txt, texture_R.bin
 //                            UnitTester::ReadRicardoData (UnitTester.cpp:237-265) of a
 //                            generated Euler-angle file, and the orientations it set
+//   two_grain_R.bin          UnitTester::SetMaterialGrid (UnitTester.cpp:46-74) on 7 x 5 x 2
 // Inputs: in_R.bin (N x 9), in_S.bin (N x 5), in_L.bin (N x 5),
 // in_D.bin / in_P.bin (N x 5 x 2, re/im).
 #include <cmath>
@@ -27,6 +28,15 @@
 #include "UnitTester.h"
 #undef private
 #undef protected
+
+// defined in UnitTester.cpp:46-74 (the header declares other overloads)
+namespace VPFFT {
+namespace UnitTester {
+void SetMaterialGrid(VPFFT::LinearAlgebra::SMatrix3x3* OrientList,
+                     VPFFT::LinearAlgebra::EigenRep* Stress, int NumX, int NumY, int NumZ,
+                     const VPFFT::DataStructures::MaterialGrid& Grid);
+}
+}  // namespace VPFFT
 
 using VPFFT::DataStructures::MaterialGrid;
 using VPFFT::LinearAlgebra::EigenRep;
@@ -141,6 +151,21 @@ int main(int argc, char** argv) {
           for (int b = 0; b < 3; ++b) tR[v * 9 + a * 3 + b] = grid.Orientation(x, y, z).m[a][b];
       }
   dump(out + "texture_R.bin", tR);
+
+  // the two-grain microstructure of the config's TwoGrainInit
+  // (UnitTester::SetMaterialGrid, UnitTester.cpp:46-74), on a 7 x 5 x 2 grid
+  {
+    const int ax = 7, ay = 5, az = 2, an = ax * ay * az;
+    MaterialGrid g2(ax, ay, az);
+    std::vector<SMatrix3x3> R2g(an);
+    std::vector<EigenRep> S2g(an);
+    VPFFT::UnitTester::SetMaterialGrid(R2g.data(), S2g.data(), ax, ay, az, g2);
+    std::vector<double> o(an * 9);
+    for (int v = 0; v < an; ++v)
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) o[v * 9 + a * 3 + b] = R2g[v].m[a][b];
+    dump(out + "two_grain_R.bin", o);
+  }
   MPI_Finalize();
   return 0;
 }

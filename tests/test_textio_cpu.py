@@ -71,3 +71,10 @@ def test_io_errors(lib, tmp_path):
     with pytest.raises(capi.VpfftError) as e:
         textio.ReadRicardoData(bad, DIMS)
     assert e.value.status == capi.ERR_IO
+
+
+def test_two_grain_microstructure_matches_reference(lib):
+    from vpfft_b200 import fixtures
+
+    ref = np.fromfile(os.path.join(IO, "two_grain_R.bin"), dtype=np.float64).reshape(70, 9)
+    assert np.array_equal(fixtures.two_grain(7, 5, 2), ref)

@@ -222,6 +222,8 @@ _PROTOS = {
     "vpfft_write_random_material": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _D, _D]),
     "vpfft_read_random_material": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _D, _D]),
     "vpfft_read_euler_texture": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _D]),
+    "vpfft_euler_matrix": (C.c_int, [C.c_double, C.c_double, C.c_double, _D]),
+    "vpfft_fixture_two_grain": (C.c_int, [C.c_int, C.c_int, C.c_int, _D]),
     "vpfft_config_read": (C.c_int, [C.c_char_p, C.POINTER(Config), C.c_char_p, C.c_size_t]),
 }
 

@@ -165,4 +165,30 @@ vpfft_status vpfft_read_euler_texture(const char* path, int nx, int ny, int nz, 
   return VPFFT_OK;
 }
 
+vpfft_status vpfft_euler_matrix(double phi, double theta, double psi, double R9[9]) {
+  if (!R9) return vpfft::lib_fail(VPFFT_ERR_INVALID_ARGUMENT, "bad argument");
+  active_euler(phi, theta, psi, R9);
+  return VPFFT_OK;
+}
+
+// UnitTester::SetMaterialGrid (UnitTester.cpp:46-74): quadrants of the x-y
+// plane alternate between two grains, Euler (-40, 0, 0) and (0, 40, 0) degrees.
+vpfft_status vpfft_fixture_two_grain(int nx, int ny, int nz, double* R9) {
+  if (!R9 || !dims_ok(nx, ny, nz)) return vpfft::lib_fail(VPFFT_ERR_INVALID_ARGUMENT, "bad argument");
+  const double to_rad = 3.14159265358979323846 / (double)180.0f;
+  double left[9], right[9];
+  active_euler(-40 * to_rad, 0, 0, left);
+  active_euler(0 * to_rad, 40 * to_rad, 0, right);
+  const int xh = nx / 2, yh = ny / 2;
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k) {
+        const bool l = (i >= xh && j >= yh) || (i < xh && j < yh);
+        const double* src = l ? left : right;
+        double* dst = R9 + voxel(i, j, k, ny, nz) * 9;
+        for (int e = 0; e < 9; ++e) dst[e] = src[e];
+      }
+  return VPFFT_OK;
+}
+
 }  // extern "C"

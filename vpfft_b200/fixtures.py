@@ -41,3 +41,18 @@ def random_traceless_velocity_gradient(rng: np.random.Generator) -> np.ndarray:
     D = 0.5 * (L + L.T)
     eq = np.sqrt(2.0 / 3.0 * np.sum(D * D))
     return L / eq
+
+
+def two_grain(nx: int, ny: int, nz: int) -> np.ndarray:
+    """The config's TwoGrainInit microstructure (UnitTester::SetMaterialGrid,
+    UnitTester.cpp:46-74): (N, 9)."""
+    R = np.zeros((nx * ny * nz, 9))
+    check(capi.load().vpfft_fixture_two_grain(nx, ny, nz, dptr(R)))
+    return R
+
+
+def euler_matrix(phi: float, theta: float, psi: float) -> np.ndarray:
+    """SMatrix3x3::BuildActiveEulerMatrix (LinearAlgebra.cpp:160-181), radians: (3, 3)."""
+    R = np.zeros(9)
+    check(capi.load().vpfft_euler_matrix(float(phi), float(theta), float(psi), dptr(R)))
+    return R.reshape(3, 3)
