@@ -248,6 +248,7 @@ def test_config_driven_run(lib, tmp_path):
 
     cfg = tmp_path / "run.config"
     cfg.write_text("GridDimension 8 8 4\nInputStrainRate\n  -0.5 0 0\n  0 -0.5 0\n  0 0 1\n"
+                   "MaxNRIter 100\nNRTolerence 1e-5\n"
                    "TimeStep 0.01\nNumTimeIter 2\nTwoGrainInit\nCRSS 1\nGammaDotBase 1\n"
                    "RateSensitivity 10\nTau0 1\nTau1 0.5\nTheta0 20\nTheta1 1\n"
                    "HardeningMatrix 1\nMaxIter 12\nPrecision FP64\n")
