@@ -358,6 +358,9 @@ void build_iter_lists(vpfft_batch* b, IterLists& L) {
     L.smax.smem_z_c2r = std::max(L.smax.smem_z_c2r, sh.smem_z_c2r);
     L.smax.smem_y = std::max(L.smax.smem_y, sh.smem_y);
     L.smax.smem_x = std::max(L.smax.smem_x, sh.smem_x);
+    L.smax.r16_z = L.smax.r16_z || sh.r16_z;
+    L.smax.r16_y = L.smax.r16_y || sh.r16_y;
+    L.smax.r16_x = L.smax.r16_x || sh.r16_x;
   }
 }
 

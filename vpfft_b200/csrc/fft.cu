@@ -62,79 +62,136 @@ __device__ __forceinline__ T mul_si(T z) {
   return T{-z.y, z.x};
 }
 
+// In-register DFTs of size R (forward SIGN = -1: W = exp(-2 pi i / R)), input
+// and output in natural order.
+template <int SIGN, typename T>
+__device__ __forceinline__ void dft4(T& a0, T& a1, T& a2, T& a3) {
+  const T u0 = add(a0, a2), u1 = sub(a0, a2), u2 = add(a1, a3);
+  const T u3 = mul_si<SIGN>(sub(a1, a3));
+  a0 = add(u0, u2);
+  a1 = add(u1, u3);
+  a2 = sub(u0, u2);
+  a3 = sub(u1, u3);
+}
+
+// exp(-i theta) = (cos theta, -sin theta), the convention of the twiddle
+// tables: tw_mul<SIGN> conjugates it for the inverse transform.
+template <int SIGN, typename T, typename R>
+__device__ __forceinline__ T wconst(R c, R s) {
+  return T{c, -s};
+}
+
+template <int RADIX, int SIGN, typename T>
+__device__ __forceinline__ void dft(T (&v)[RADIX]) {
+  using R = decltype(T{}.x);
+  if constexpr (RADIX == 2) {
+    const T t = v[0];
+    v[0] = add(t, v[1]);
+    v[1] = sub(t, v[1]);
+  } else if constexpr (RADIX == 3) {
+    const T t1 = add(v[1], v[2]);
+    const T t2 = sub(v[0], scl(t1, R(0.5)));
+    const T t3 = mul_si<SIGN>(scl(sub(v[1], v[2]), R(0.86602540378443864676)));
+    v[0] = add(v[0], t1);
+    v[1] = add(t2, t3);
+    v[2] = sub(t2, t3);
+  } else if constexpr (RADIX == 4) {
+    dft4<SIGN>(v[0], v[1], v[2], v[3]);
+  } else if constexpr (RADIX == 5) {
+    const R c1 = R(0.30901699437494742410), c2 = R(-0.80901699437494742410);
+    const R s1 = R(0.95105651629515357212), s2 = R(0.58778525229247312917);
+    const T a1 = add(v[1], v[4]), a2 = add(v[2], v[3]), b1 = sub(v[1], v[4]),
+            b2 = sub(v[2], v[3]);
+    const T p1 = add(v[0], add(scl(a1, c1), scl(a2, c2)));
+    const T p2 = add(v[0], add(scl(a1, c2), scl(a2, c1)));
+    const T q1 = mul_si<SIGN>(add(scl(b1, s1), scl(b2, s2)));
+    const T q2 = mul_si<SIGN>(sub(scl(b1, s2), scl(b2, s1)));
+    v[0] = add(v[0], add(a1, a2));
+    v[1] = add(p1, q1);
+    v[4] = sub(p1, q1);
+    v[2] = add(p2, q2);
+    v[3] = sub(p2, q2);
+  } else if constexpr (RADIX == 16) {
+    // 16 = 4 x 4: Y[n1][k1] = DFT4 over n2 of v[n1 + 4 n2], times W16^(n1 k1);
+    // X[k1 + 4 k2] = DFT4 over n1 of Y[n1][k1]
+#pragma unroll
+    for (int n1 = 0; n1 < 4; ++n1) dft4<SIGN>(v[n1], v[n1 + 4], v[n1 + 8], v[n1 + 12]);
+    // now v[n1 + 4 k1] = Y[n1][k1]
+    const R c = R(0.92387953251128675613), s = R(0.38268343236508977173);
+    const R h = R(0.70710678118654752440);
+    v[5] = tw_mul<SIGN>(v[5], wconst<SIGN, T>(c, s));     // n1 1, k1 1: W^1
+    v[9] = tw_mul<SIGN>(v[9], wconst<SIGN, T>(h, h));     // n1 1, k1 2: W^2
+    v[13] = tw_mul<SIGN>(v[13], wconst<SIGN, T>(s, c));   // n1 1, k1 3: W^3
+    v[6] = tw_mul<SIGN>(v[6], wconst<SIGN, T>(h, h));     // n1 2, k1 1: W^2
+    v[10] = mul_si<SIGN>(v[10]);                          // n1 2, k1 2: W^4
+    v[14] = tw_mul<SIGN>(v[14], wconst<SIGN, T>(-h, h));  // n1 2, k1 3: W^6
+    v[7] = tw_mul<SIGN>(v[7], wconst<SIGN, T>(s, c));     // n1 3, k1 1: W^3
+    v[11] = tw_mul<SIGN>(v[11], wconst<SIGN, T>(-h, h));  // n1 3, k1 2: W^6
+    v[15] = tw_mul<SIGN>(v[15], wconst<SIGN, T>(-c, -s)); // n1 3, k1 3: W^9
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1)
+      dft4<SIGN>(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]);
+    // now v[4 k1 + k2] = X[k1 + 4 k2]: transpose 4 x 4 into natural order
+    T x[16];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1)
+#pragma unroll
+      for (int k2 = 0; k2 < 4; ++k2) x[k1 + 4 * k2] = v[4 * k1 + k2];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = x[r];
+  }
+}
+
+// One Stockham stage of radix R over nlines lines: butterfly j of a line
+// reads in[j + r nb] (nb = n / R), multiplies by tw[r e] (e = (j mod Ns) n /
+// (Ns R)), transforms in registers and writes out[(j - j mod Ns) R + j mod Ns + r Ns].
+template <int RADIX, int SIGN, typename T>
+__device__ __forceinline__ void stockham_stage(const T* a, T* b, const T* tw, int n, int Ns,
+                                               int nlines, int ls, const FastDiv& dnb,
+                                               const FastDiv& dns) {
+  const int nb = n / RADIX;
+  const int total = nb * nlines;
+  const int tws = n / (Ns * RADIX);
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int line = (int)fast_div((uint32_t)t, dnb);
+    const int j = t - line * nb;
+    const T* in = a + line * ls;
+    T* out = b + line * ls;
+    const int jm = j - (int)fast_div((uint32_t)j, dns) * Ns;
+    const int e = jm * tws;
+    const int od = (j - jm) * RADIX + jm;
+    T v[RADIX];
+#pragma unroll
+    for (int r = 0; r < RADIX; ++r) v[r] = in[j + r * nb];
+    if (e) {
+#pragma unroll
+      for (int r = 1; r < RADIX; ++r) v[r] = tw_mul<SIGN>(v[r], tw[r * e]);
+    }
+    dft<RADIX, SIGN>(v);
+#pragma unroll
+    for (int r = 0; r < RADIX; ++r) out[od + r * Ns] = v[r];
+  }
+}
+
 // Stockham autosort FFT of nlines lines (line stride ls) of length pl.n in
 // shared memory; a and b are ping-pong buffers, the result buffer is returned.
-template <int SIGN, typename T>
+// B16: whether the plan may contain a radix-16 stage (kernels without it keep
+// a smaller register footprint for lines that never use one).
+template <int SIGN, bool B16, typename T>
 __device__ T* line_fft(T* a, T* b, const T* tw, const LinePlan& pl, int nlines, int ls) {
-  using R = decltype(T{}.x);
   const int n = pl.n;
   int Ns = 1;
   for (int st = 0; st < pl.nrad; ++st) {
     const int Rr = pl.rad[st];
-    const int nb = n / Rr;
-    const int total = nb * nlines;
-    const int tws = n / (Ns * Rr);
     const FastDiv dnb = pl.by_nb[st], dns = pl.by_ns[st];
-    for (int t = threadIdx.x; t < total; t += blockDim.x) {
-      const int line = (int)fast_div((uint32_t)t, dnb);
-      const int j = t - line * nb;
-      const T* in = a + line * ls;
-      T* out = b + line * ls;
-      const int jm = j - (int)fast_div((uint32_t)j, dns) * Ns;
-      const int e = jm * tws;
-      const int od = (j - jm) * Rr + jm;
-      if (Rr == 4) {
-        T v0 = in[j], v1 = in[j + nb], v2 = in[j + 2 * nb], v3 = in[j + 3 * nb];
-        if (e) {
-          v1 = tw_mul<SIGN>(v1, tw[e]);
-          v2 = tw_mul<SIGN>(v2, tw[2 * e]);
-          v3 = tw_mul<SIGN>(v3, tw[3 * e]);
-        }
-        const T u0 = add(v0, v2), u1 = sub(v0, v2), u2 = add(v1, v3);
-        const T u3 = mul_si<SIGN>(sub(v1, v3));
-        out[od] = add(u0, u2);
-        out[od + Ns] = add(u1, u3);
-        out[od + 2 * Ns] = sub(u0, u2);
-        out[od + 3 * Ns] = sub(u1, u3);
-      } else if (Rr == 2) {
-        T v0 = in[j], v1 = in[j + nb];
-        if (e) v1 = tw_mul<SIGN>(v1, tw[e]);
-        out[od] = add(v0, v1);
-        out[od + Ns] = sub(v0, v1);
-      } else if (Rr == 3) {
-        T v0 = in[j], v1 = in[j + nb], v2 = in[j + 2 * nb];
-        if (e) {
-          v1 = tw_mul<SIGN>(v1, tw[e]);
-          v2 = tw_mul<SIGN>(v2, tw[2 * e]);
-        }
-        const T t1 = add(v1, v2);
-        const T t2 = sub(v0, scl(t1, R(0.5)));
-        const T t3 = mul_si<SIGN>(scl(sub(v1, v2), R(0.86602540378443864676)));
-        out[od] = add(v0, t1);
-        out[od + Ns] = add(t2, t3);
-        out[od + 2 * Ns] = sub(t2, t3);
-      } else {  // 5
-        T v0 = in[j], v1 = in[j + nb], v2 = in[j + 2 * nb], v3 = in[j + 3 * nb],
-          v4 = in[j + 4 * nb];
-        if (e) {
-          v1 = tw_mul<SIGN>(v1, tw[e]);
-          v2 = tw_mul<SIGN>(v2, tw[2 * e]);
-          v3 = tw_mul<SIGN>(v3, tw[3 * e]);
-          v4 = tw_mul<SIGN>(v4, tw[4 * e]);
-        }
-        const R c1 = R(0.30901699437494742410), c2 = R(-0.80901699437494742410);
-        const R s1 = R(0.95105651629515357212), s2 = R(0.58778525229247312917);
-        const T a1 = add(v1, v4), a2 = add(v2, v3), b1 = sub(v1, v4), b2 = sub(v2, v3);
-        const T p1 = add(v0, add(scl(a1, c1), scl(a2, c2)));
-        const T p2 = add(v0, add(scl(a1, c2), scl(a2, c1)));
-        const T q1 = mul_si<SIGN>(add(scl(b1, s1), scl(b2, s2)));
-        const T q2 = mul_si<SIGN>(sub(scl(b1, s2), scl(b2, s1)));
-        out[od] = add(v0, add(a1, a2));
-        out[od + Ns] = add(p1, q1);
-        out[od + 4 * Ns] = sub(p1, q1);
-        out[od + 2 * Ns] = add(p2, q2);
-        out[od + 3 * Ns] = sub(p2, q2);
-      }
+    switch (Rr) {
+      case 16:
+        if constexpr (B16) stockham_stage<16, SIGN>(a, b, tw, n, Ns, nlines, ls, dnb, dns);
+        break;
+      case 4: stockham_stage<4, SIGN>(a, b, tw, n, Ns, nlines, ls, dnb, dns); break;
+      case 2: stockham_stage<2, SIGN>(a, b, tw, n, Ns, nlines, ls, dnb, dns); break;
+      case 3: stockham_stage<3, SIGN>(a, b, tw, n, Ns, nlines, ls, dnb, dns); break;
+      default: stockham_stage<5, SIGN>(a, b, tw, n, Ns, nlines, ls, dnb, dns); break;
     }
     __syncthreads();
     T* tmp = a;
@@ -207,7 +264,7 @@ struct FftTiles {
 constexpr int kFftThreads = 256;
 
 // ---------------------------------------------------------------- z, forward
-template <typename S>
+template <typename S, bool B16>
 __device__ __forceinline__ void pass_z_r2c_body(const S* __restrict__ W,
                                                 typename CX<S>::T* __restrict__ A,
                                                 const LinePlan& pl,
@@ -230,7 +287,7 @@ __device__ __forceinline__ void pass_z_r2c_body(const S* __restrict__ W,
       [&](int l, int z) { return l < ty ? src[l * nz + z] : S(0); },
       [&](int l, int z, S v) { reinterpret_cast<S*>(&a[(l >> 1) * ls + z])[l & 1] = v; });
   __syncthreads();
-  const T* r = line_fft<-1>(a, b, tw, pl, npair, ls);
+  const T* r = line_fft<-1, B16>(a, b, tw, pl, npair, ls);
   T* dst = A + ((long long)(c * nx + x) * nh) * ny + y0;
   copy_short_rows<TY, T>(
       nh,
@@ -254,7 +311,7 @@ __device__ __forceinline__ void pass_z_r2c_body(const S* __restrict__ W,
 }
 
 // ---------------------------------------------------------------- z, inverse
-template <typename S>
+template <typename S, bool B16>
 __device__ __forceinline__ void pass_z_c2r_body(const typename CX<S>::T* __restrict__ A,
                                                 S* __restrict__ W, const LinePlan& pl,
                                                 const typename CX<S>::T* __restrict__ twg, int nx,
@@ -297,7 +354,7 @@ __device__ __forceinline__ void pass_z_c2r_body(const typename CX<S>::T* __restr
     a[p * ls + k] = T{Ae.x - Ao.y, Ae.y + Ao.x};
   }
   __syncthreads();
-  const T* r = line_fft<1>(a, b, tw, pl, npair, ls);
+  const T* r = line_fft<1, B16>(a, b, tw, pl, npair, ls);
   S* dst = W + ((long long)(c * nx + x) * ny + y0) * nz;
   copy_rows<S>(
       ty, nz,
@@ -310,7 +367,7 @@ __device__ __forceinline__ void pass_z_c2r_body(const typename CX<S>::T* __restr
 
 // ---------------------------------------------------------------- y passes
 // Forward: A[c][x][kz][y] -> B[c][kz][ky][x]; inverse: B -> A.
-template <int SIGN, typename R>
+template <int SIGN, bool B16, typename R>
 __device__ __forceinline__ void pass_y_body(const typename CX<R>::T* __restrict__ in,
                                             typename CX<R>::T* __restrict__ out,
                                             const LinePlan& pl,
@@ -345,7 +402,7 @@ __device__ __forceinline__ void pass_y_body(const typename CX<R>::T* __restrict_
         [&](int y, int xl, T v) { a[xl * ls + y] = v; });
   }
   __syncthreads();
-  const T* r = line_fft<SIGN>(a, b, tw, pl, TX, ls);
+  const T* r = line_fft<SIGN, B16>(a, b, tw, pl, TX, ls);
   if (SIGN < 0) {
     copy_short_rows<TX, T>(
         ny, [&](int y, int xl) { return r[xl * ls + y]; },
@@ -361,7 +418,7 @@ __device__ __forceinline__ void pass_y_body(const typename CX<R>::T* __restrict_
 
 // ---------------------------------------------------------------- x pass
 // In place on B[c][kz][ky][x]: MODE 0 forward, 1 inverse, 2 forward + Green + inverse.
-template <int MODE, typename R>
+template <int MODE, bool B16, typename R>
 __device__ __forceinline__ void pass_x_body(typename CX<R>::T* __restrict__ B, const LinePlan& pl,
                                             const typename CX<R>::T* __restrict__ twg,
                                             const GreenParams<R>& gp, int ny, int nh, int ncomp,
@@ -391,7 +448,7 @@ __device__ __forceinline__ void pass_x_body(typename CX<R>::T* __restrict__ B, c
   T* r = a;
   T* o = b;
   if (MODE != 1) {
-    r = line_fft<-1>(a, b, tw, pl, nl, ls);
+    r = line_fft<-1, B16>(a, b, tw, pl, nl, ls);
     o = (r == a) ? b : a;
   }
   if (MODE == 2) {
@@ -411,7 +468,7 @@ __device__ __forceinline__ void pass_x_body(typename CX<R>::T* __restrict__ B, c
     }
     __syncthreads();
   }
-  if (MODE != 0) r = line_fft<1>(r, o, tw, pl, nl, ls);
+  if (MODE != 0) r = line_fft<1, B16>(r, o, tw, pl, nl, ls);
   copy_rows<T>(
       nl, nx, [&](int L, int xx) { return r[L * ls + xx]; },
       [&](int L, int xx, T v) {
@@ -421,37 +478,37 @@ __device__ __forceinline__ void pass_x_body(typename CX<R>::T* __restrict__ B, c
 }
 
 // ---------------------------------------------------------------- kernels
-template <typename S>
+template <typename S, bool B16>
 __global__ void __launch_bounds__(kFftThreads)
     k_pass_z_r2c(const S* __restrict__ W, typename CX<S>::T* __restrict__ A, LinePlan pl,
                  const typename CX<S>::T* __restrict__ twg, int nx, int ny, int nh,
                  const IterCtrl* ctrl) {
   if (ctrl && ctrl->done) return;
-  pass_z_r2c_body<S>(W, A, pl, twg, nx, ny, nh, blockIdx.x, blockIdx.y, blockIdx.z);
+  pass_z_r2c_body<S, B16>(W, A, pl, twg, nx, ny, nh, blockIdx.x, blockIdx.y, blockIdx.z);
 }
-template <typename S>
+template <typename S, bool B16>
 __global__ void __launch_bounds__(kFftThreads)
     k_pass_z_c2r(const typename CX<S>::T* __restrict__ A, S* __restrict__ W, LinePlan pl,
                  const typename CX<S>::T* __restrict__ twg, int nx, int ny, int nh, S scale,
                  const IterCtrl* ctrl) {
   if (ctrl && ctrl->done) return;
-  pass_z_c2r_body<S>(A, W, pl, twg, nx, ny, nh, scale, blockIdx.x, blockIdx.y, blockIdx.z);
+  pass_z_c2r_body<S, B16>(A, W, pl, twg, nx, ny, nh, scale, blockIdx.x, blockIdx.y, blockIdx.z);
 }
-template <int SIGN, typename R>
+template <int SIGN, bool B16, typename R>
 __global__ void __launch_bounds__(kFftThreads)
     k_pass_y(const typename CX<R>::T* __restrict__ in, typename CX<R>::T* __restrict__ out,
              LinePlan pl, const typename CX<R>::T* __restrict__ twg, int nx, int nh,
              const IterCtrl* ctrl) {
   if (ctrl && ctrl->done) return;
-  pass_y_body<SIGN, R>(in, out, pl, twg, nx, nh, blockIdx.x, blockIdx.y, blockIdx.z);
+  pass_y_body<SIGN, B16, R>(in, out, pl, twg, nx, nh, blockIdx.x, blockIdx.y, blockIdx.z);
 }
-template <int MODE, typename R>
+template <int MODE, bool B16, typename R>
 __global__ void __launch_bounds__(kFftThreads, 2)
     k_pass_x(typename CX<R>::T* __restrict__ B, LinePlan pl,
              const typename CX<R>::T* __restrict__ twg, GreenParams<R> gp, int ny, int nh,
              int ncomp, const IterCtrl* ctrl) {
   if (ctrl && ctrl->done) return;
-  pass_x_body<MODE, R>(B, pl, twg, gp, ny, nh, ncomp, blockIdx.x, blockIdx.y);
+  pass_x_body<MODE, B16, R>(B, pl, twg, gp, ny, nh, ncomp, blockIdx.x, blockIdx.y);
 }
 
 // Batched passes of the fixed-point iteration (5 components): block -> slot,
@@ -473,7 +530,7 @@ __device__ __forceinline__ const SlotDesc<S>* batch_pass_setup(const SlotDesc<S>
   return d;
 }
 
-template <typename S>
+template <typename S, bool B16>
 __global__ void __launch_bounds__(kFftThreads)
     k_pass_z_r2c_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
   __shared__ SlotSpectral<S> sm;
@@ -483,11 +540,11 @@ __global__ void __launch_bounds__(kFftThreads)
   const Spectral<S>& sp = sm.sp;
   const int gx = (sp.ny + FftTiles<S>::kZ - 1) / FftTiles<S>::kZ;
   const int t = lb / gx;
-  pass_z_r2c_body<S>(d->f.work, reinterpret_cast<typename CX<S>::T*>(sp.X), sp.pz,
+  pass_z_r2c_body<S, B16>(d->f.work, reinterpret_cast<typename CX<S>::T*>(sp.X), sp.pz,
                      reinterpret_cast<const typename CX<S>::T*>(sp.twz), sp.nx, sp.ny, sp.nh,
                      lb - t * gx, t % sp.nx, t / sp.nx);
 }
-template <typename S>
+template <typename S, bool B16>
 __global__ void __launch_bounds__(kFftThreads)
     k_pass_z_c2r_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
   __shared__ SlotSpectral<S> sm;
@@ -498,11 +555,11 @@ __global__ void __launch_bounds__(kFftThreads)
   const int gx = (sp.ny + FftTiles<S>::kZ - 1) / FftTiles<S>::kZ;
   const int t = lb / gx;
   const S scale = S(1.0 / ((double)sp.nx * sp.ny * sp.nz));
-  pass_z_c2r_body<S>(reinterpret_cast<const typename CX<S>::T*>(sp.X), d->f.work, sp.pz,
+  pass_z_c2r_body<S, B16>(reinterpret_cast<const typename CX<S>::T*>(sp.X), d->f.work, sp.pz,
                      reinterpret_cast<const typename CX<S>::T*>(sp.twz), sp.nx, sp.ny, sp.nh,
                      scale, lb - t * gx, t % sp.nx, t / sp.nx);
 }
-template <int SIGN, typename S>
+template <int SIGN, bool B16, typename S>
 __global__ void __launch_bounds__(kFftThreads)
     k_pass_y_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
   using T = typename CX<S>::T;
@@ -515,10 +572,10 @@ __global__ void __launch_bounds__(kFftThreads)
   const int t = lb / gx;
   const T* in = reinterpret_cast<const T*>(SIGN < 0 ? sp.X : sp.X2);
   T* out = reinterpret_cast<T*>(SIGN < 0 ? sp.X2 : sp.X);
-  pass_y_body<SIGN, S>(in, out, sp.py, reinterpret_cast<const T*>(sp.twy), sp.nx, sp.nh,
+  pass_y_body<SIGN, B16, S>(in, out, sp.py, reinterpret_cast<const T*>(sp.twy), sp.nx, sp.nh,
                        lb - t * gx, t % sp.nh, t / sp.nh);
 }
-template <typename S>
+template <typename S, bool B16>
 __global__ void __launch_bounds__(kFftThreads, 2)
     k_pass_x_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
   using T = typename CX<S>::T;
@@ -528,7 +585,7 @@ __global__ void __launch_bounds__(kFftThreads, 2)
   if (!d) return;
   const Spectral<S>& sp = sm.sp;
   const int gx = (sp.ny + FftTiles<S>::kX - 1) / FftTiles<S>::kX;
-  pass_x_body<2, S>(reinterpret_cast<T*>(sp.X2), sp.px, reinterpret_cast<const T*>(sp.twx),
+  pass_x_body<2, B16, S>(reinterpret_cast<T*>(sp.X2), sp.px, reinterpret_cast<const T*>(sp.twx),
                     sm.gp, sp.ny, sp.nh, 5, lb % gx, lb / gx);
 }
 
@@ -559,27 +616,38 @@ void optin_rest(K kern, int total) {
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        total - (int)a.sharedSizeBytes);
 }
+template <typename R, bool B16>
+void pass_optin_variant(int s) {
+  cudaFuncSetAttribute(k_pass_z_r2c<R, B16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  cudaFuncSetAttribute(k_pass_z_c2r<R, B16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  cudaFuncSetAttribute(k_pass_y<-1, B16, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  cudaFuncSetAttribute(k_pass_y<1, B16, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  cudaFuncSetAttribute(k_pass_x<0, B16, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  cudaFuncSetAttribute(k_pass_x<1, B16, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  cudaFuncSetAttribute(k_pass_x<2, B16, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  // the batched kernels hold the slot's descriptor in static shared memory
+  optin_rest(k_pass_z_r2c_batch<R, B16>, s);
+  optin_rest(k_pass_z_c2r_batch<R, B16>, s);
+  optin_rest(k_pass_y_batch<-1, B16, R>, s);
+  optin_rest(k_pass_y_batch<1, B16, R>, s);
+  optin_rest(k_pass_x_batch<R, B16>, s);
+}
 template <typename R>
 void pass_optin() {
   static bool done = false;  // attributes are per function and device-independent here
   if (done) return;
   const int s = 227 * 1024;
-  cudaFuncSetAttribute(k_pass_z_r2c<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
-  cudaFuncSetAttribute(k_pass_z_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
-  cudaFuncSetAttribute(k_pass_y<-1, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
-  cudaFuncSetAttribute(k_pass_y<1, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
-  cudaFuncSetAttribute(k_pass_x<0, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
-  cudaFuncSetAttribute(k_pass_x<1, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
-  cudaFuncSetAttribute(k_pass_x<2, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
-  // the batched kernels hold the slot's descriptor in static shared memory
-  optin_rest(k_pass_z_r2c_batch<R>, s);
-  optin_rest(k_pass_z_c2r_batch<R>, s);
-  optin_rest(k_pass_y_batch<-1, R>, s);
-  optin_rest(k_pass_y_batch<1, R>, s);
-  optin_rest(k_pass_x_batch<R>, s);
+  pass_optin_variant<R, false>(s);
+  pass_optin_variant<R, true>(s);
   done = true;
 }
 }  // namespace
+
+static bool has16(const LinePlan& p) {
+  for (int st = 0; st < p.nrad; ++st)
+    if (p.rad[st] == 16) return true;
+  return false;
+}
 
 template <typename S>
 int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S* work,
@@ -597,17 +665,22 @@ int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S
   const dim3 gy((sp.nx + FftTiles<S>::kY - 1) / FftTiles<S>::kY, sp.nh, ncomp);
   const dim3 gx((sp.ny + FftTiles<S>::kX - 1) / FftTiles<S>::kX, sp.nh);
   if (ev) cudaEventRecord(ev[0], st);
-  k_pass_z_r2c<S><<<gz, kFftThreads, sm.z_r2c, st>>>(work, A, sp.pz, twz, sp.nx, sp.ny, sp.nh, ctrl);
+  const bool bz = has16(sp.pz), by = has16(sp.py), bx = has16(sp.px);
+  (bz ? k_pass_z_r2c<S, true> : k_pass_z_r2c<S, false>)<<<gz, kFftThreads, sm.z_r2c, st>>>(
+      work, A, sp.pz, twz, sp.nx, sp.ny, sp.nh, ctrl);
   if (ev) cudaEventRecord(ev[1], st);
-  k_pass_y<-1, S><<<gy, kFftThreads, sm.y, st>>>(A, B, sp.py, twy, sp.nx, sp.nh, ctrl);
+  (by ? k_pass_y<-1, true, S> : k_pass_y<-1, false, S>)<<<gy, kFftThreads, sm.y, st>>>(
+      A, B, sp.py, twy, sp.nx, sp.nh, ctrl);
   if (ev) cudaEventRecord(ev[2], st);
-  k_pass_x<2, S><<<gx, kFftThreads, sm.x, st>>>(B, sp.px, twx, gp, sp.ny, sp.nh, ncomp, ctrl);
+  (bx ? k_pass_x<2, true, S> : k_pass_x<2, false, S>)<<<gx, kFftThreads, sm.x, st>>>(
+      B, sp.px, twx, gp, sp.ny, sp.nh, ncomp, ctrl);
   if (ev) cudaEventRecord(ev[3], st);
-  k_pass_y<1, S><<<gy, kFftThreads, sm.y, st>>>(B, A, sp.py, twy, sp.nx, sp.nh, ctrl);
+  (by ? k_pass_y<1, true, S> : k_pass_y<1, false, S>)<<<gy, kFftThreads, sm.y, st>>>(
+      B, A, sp.py, twy, sp.nx, sp.nh, ctrl);
   if (ev) cudaEventRecord(ev[4], st);
   const S scale = S(1.0 / ((double)sp.nx * sp.ny * sp.nz));
-  k_pass_z_c2r<S><<<gz, kFftThreads, sm.z_c2r, st>>>(A, work, sp.pz, twz, sp.nx, sp.ny, sp.nh,
-                                                     scale, ctrl);
+  (bz ? k_pass_z_c2r<S, true> : k_pass_z_c2r<S, false>)<<<gz, kFftThreads, sm.z_c2r, st>>>(
+      A, work, sp.pz, twz, sp.nx, sp.ny, sp.nh, scale, ctrl);
   if (ev) cudaEventRecord(ev[5], st);
   return 5;
 }
@@ -627,15 +700,23 @@ int launch_fft3d(const Spectral<S>& sp, S* real, int ncomp, int mode, cudaStream
   const dim3 gx((sp.ny + FftTiles<S>::kX - 1) / FftTiles<S>::kX, sp.nh);
   GreenParams<S> gp{};
   if (mode == 0) {
-    k_pass_z_r2c<S><<<gz, kFftThreads, sm.z_r2c, st>>>(real, A, sp.pz, twz, sp.nx, sp.ny, sp.nh,
+    const bool bz = has16(sp.pz), by = has16(sp.py), bx = has16(sp.px);
+    (bz ? k_pass_z_r2c<S, true> : k_pass_z_r2c<S, false>)<<<gz, kFftThreads, sm.z_r2c, st>>>(
+        real, A, sp.pz, twz, sp.nx, sp.ny, sp.nh,
                                                        nullptr);
-    k_pass_y<-1, S><<<gy, kFftThreads, sm.y, st>>>(A, B, sp.py, twy, sp.nx, sp.nh, nullptr);
-    k_pass_x<0, S><<<gx, kFftThreads, sm.x, st>>>(B, sp.px, twx, gp, sp.ny, sp.nh, ncomp, nullptr);
+    (by ? k_pass_y<-1, true, S> : k_pass_y<-1, false, S>)<<<gy, kFftThreads, sm.y, st>>>(
+        A, B, sp.py, twy, sp.nx, sp.nh, nullptr);
+    (bx ? k_pass_x<0, true, S> : k_pass_x<0, false, S>)<<<gx, kFftThreads, sm.x, st>>>(
+        B, sp.px, twx, gp, sp.ny, sp.nh, ncomp, nullptr);
   } else {
-    k_pass_x<1, S><<<gx, kFftThreads, sm.x, st>>>(B, sp.px, twx, gp, sp.ny, sp.nh, ncomp, nullptr);
-    k_pass_y<1, S><<<gy, kFftThreads, sm.y, st>>>(B, A, sp.py, twy, sp.nx, sp.nh, nullptr);
+    const bool bz = has16(sp.pz), by = has16(sp.py), bx = has16(sp.px);
+    (bx ? k_pass_x<1, true, S> : k_pass_x<1, false, S>)<<<gx, kFftThreads, sm.x, st>>>(
+        B, sp.px, twx, gp, sp.ny, sp.nh, ncomp, nullptr);
+    (by ? k_pass_y<1, true, S> : k_pass_y<1, false, S>)<<<gy, kFftThreads, sm.y, st>>>(
+        B, A, sp.py, twy, sp.nx, sp.nh, nullptr);
     const S scale = S(1.0 / ((double)sp.nx * sp.ny * sp.nz));
-    k_pass_z_c2r<S><<<gz, kFftThreads, sm.z_c2r, st>>>(A, real, sp.pz, twz, sp.nx, sp.ny, sp.nh,
+    (bz ? k_pass_z_c2r<S, true> : k_pass_z_c2r<S, false>)<<<gz, kFftThreads, sm.z_c2r, st>>>(
+        A, real, sp.pz, twz, sp.nx, sp.ny, sp.nh,
                                                        scale, nullptr);
   }
   return 3;
@@ -652,6 +733,9 @@ SpectralShape spectral_shape(const Spectral<S>& sp, int ncomp) {
   r.smem_z_c2r = sm.z_c2r;
   r.smem_y = sm.y;
   r.smem_x = sm.x;
+  r.r16_z = has16(sp.pz);
+  r.r16_y = has16(sp.py);
+  r.r16_x = has16(sp.px);
   return r;
 }
 
@@ -660,11 +744,17 @@ int launch_spectral_batch(const SlotDesc<S>* d, const BatchLaunch& bl_z, const B
                           const BatchLaunch& bl_x, const SpectralShape& sm, cudaStream_t st) {
   if (bl_z.blocks <= 0) return 0;
   pass_optin<S>();
-  k_pass_z_r2c_batch<S><<<bl_z.blocks, kFftThreads, sm.smem_z_r2c, st>>>(d, bl_z);
-  k_pass_y_batch<-1, S><<<bl_y.blocks, kFftThreads, sm.smem_y, st>>>(d, bl_y);
-  k_pass_x_batch<S><<<bl_x.blocks, kFftThreads, sm.smem_x, st>>>(d, bl_x);
-  k_pass_y_batch<1, S><<<bl_y.blocks, kFftThreads, sm.smem_y, st>>>(d, bl_y);
-  k_pass_z_c2r_batch<S><<<bl_z.blocks, kFftThreads, sm.smem_z_c2r, st>>>(d, bl_z);
+  const bool bz = sm.r16_z, by = sm.r16_y, bx = sm.r16_x;
+  (bz ? k_pass_z_r2c_batch<S, true> : k_pass_z_r2c_batch<S, false>)<<<bl_z.blocks, kFftThreads,
+                                                                     sm.smem_z_r2c, st>>>(d, bl_z);
+  (by ? k_pass_y_batch<-1, true, S> : k_pass_y_batch<-1, false, S>)<<<bl_y.blocks, kFftThreads,
+                                                                       sm.smem_y, st>>>(d, bl_y);
+  (bx ? k_pass_x_batch<S, true> : k_pass_x_batch<S, false>)<<<bl_x.blocks, kFftThreads,
+                                                              sm.smem_x, st>>>(d, bl_x);
+  (by ? k_pass_y_batch<1, true, S> : k_pass_y_batch<1, false, S>)<<<bl_y.blocks, kFftThreads,
+                                                                     sm.smem_y, st>>>(d, bl_y);
+  (bz ? k_pass_z_c2r_batch<S, true> : k_pass_z_c2r_batch<S, false>)<<<bl_z.blocks, kFftThreads,
+                                                                     sm.smem_z_c2r, st>>>(d, bl_z);
   return 5;
 }
 

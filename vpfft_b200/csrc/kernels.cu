@@ -24,17 +24,17 @@
 namespace vpfft {
 
 // ============================================================== line plans
-// Radix-4 stages first, then 2, 3 and 5; returns false for other prime factors.
+// Radix-4 stages first, then 2, 3 and 5; returns false for other prime
+// factors.  When at least four radix-4 stages occur, the last two become one
+// radix-16 stage (two radix-4 layers in registers per pass through shared
+// memory): its span is then >= 16, so its Stockham stores are contiguous
+// across threads (a radix-16 first stage would store with a 16-element stride
+// and 16-way bank conflicts).
 bool make_line_plan(int n, LinePlan* p) {
   if (n < 1) return false;
   p->n = n;
   p->nrad = 0;
   int m = n;
-  while (m % 4 == 0 && m > 4) {
-    if (p->nrad >= 16) return false;
-    p->rad[p->nrad++] = 4;
-    m /= 4;
-  }
   const int rs[4] = {4, 2, 3, 5};
   for (int r : rs)
     while (m % r == 0) {
@@ -43,6 +43,17 @@ bool make_line_plan(int n, LinePlan* p) {
       m /= r;
     }
   if (m != 1) return false;
+  int last4 = -1, count4 = 0;
+  for (int st = 0; st < p->nrad; ++st)
+    if (p->rad[st] == 4) {
+      ++count4;
+      last4 = st;
+    }
+  if (count4 >= 4 && p->rad[last4 - 1] == 4) {
+    p->rad[last4 - 1] = 16;
+    for (int st = last4; st + 1 < p->nrad; ++st) p->rad[st] = p->rad[st + 1];
+    --p->nrad;
+  }
   p->by_n = make_fast_div((uint32_t)n);
   int ns = 1;
   for (int st = 0; st < p->nrad; ++st) {

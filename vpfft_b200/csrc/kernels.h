@@ -194,6 +194,7 @@ int launch_post_batch(const SlotDesc<S>* d, const BatchLaunch& bl, cudaStream_t 
 struct SpectralShape {
   int blocks_z, blocks_y, blocks_x;
   size_t smem_z_r2c, smem_z_c2r, smem_y, smem_x;
+  bool r16_z, r16_y, r16_x;  // a line plan of that axis has a radix-16 stage
 };
 template <typename S>
 SpectralShape spectral_shape(const Spectral<S>& sp, int ncomp);
