@@ -62,6 +62,13 @@ __device__ __forceinline__ T mul_si(T z) {
   return T{-z.y, z.x};
 }
 
+// Shared-memory layout of a staged line: element i at sw(i) = i + i/16 (one
+// pad slot per 16 elements), line stride line_stride(n) (odd, so lines are
+// staggered across banks).  The pad spreads the stores of the early Stockham
+// stages (span 1 and 4: stride-4 across threads) over all banks.
+__host__ __device__ __forceinline__ int line_stride(int n) { return n + (n >> 4) + 1; }
+__device__ __forceinline__ int sw(int i) { return i + (i >> 4); }
+
 // In-register DFTs of size R (forward SIGN = -1: W = exp(-2 pi i / R)), input
 // and output in natural order.
 template <int SIGN, typename T>
@@ -162,14 +169,14 @@ __device__ __forceinline__ void stockham_stage(const T* a, T* b, const T* tw, in
     const int od = (j - jm) * RADIX + jm;
     T v[RADIX];
 #pragma unroll
-    for (int r = 0; r < RADIX; ++r) v[r] = in[j + r * nb];
+    for (int r = 0; r < RADIX; ++r) v[r] = in[sw(j + r * nb)];
     if (e) {
 #pragma unroll
       for (int r = 1; r < RADIX; ++r) v[r] = tw_mul<SIGN>(v[r], tw[r * e]);
     }
     dft<RADIX, SIGN>(v);
 #pragma unroll
-    for (int r = 0; r < RADIX; ++r) out[od + r * Ns] = v[r];
+    for (int r = 0; r < RADIX; ++r) out[sw(od + r * Ns)] = v[r];
   }
 }
 
@@ -273,7 +280,7 @@ __device__ __forceinline__ void pass_z_r2c_body(const S* __restrict__ W,
   using T = typename CX<S>::T;
   constexpr int TY = FftTiles<S>::kZ;
   extern __shared__ __align__(16) unsigned char smraw[];
-  const int nz = pl.n, ls = nz + 1;
+  const int nz = pl.n, ls = line_stride(nz);
   T* tw = reinterpret_cast<T*>(smraw);
   T* a = tw + nz;
   T* b = a + (TY / 2) * ls;
@@ -285,7 +292,7 @@ __device__ __forceinline__ void pass_z_r2c_body(const S* __restrict__ W,
   copy_rows<S>(
       2 * npair, nz,
       [&](int l, int z) { return l < ty ? src[l * nz + z] : S(0); },
-      [&](int l, int z, S v) { reinterpret_cast<S*>(&a[(l >> 1) * ls + z])[l & 1] = v; });
+      [&](int l, int z, S v) { reinterpret_cast<S*>(&a[(l >> 1) * ls + sw(z)])[l & 1] = v; });
   __syncthreads();
   const T* r = line_fft<-1, B16>(a, b, tw, pl, npair, ls);
   T* dst = A + ((long long)(c * nx + x) * nh) * ny + y0;
@@ -293,8 +300,8 @@ __device__ __forceinline__ void pass_z_r2c_body(const S* __restrict__ W,
       nh,
       [&](int k, int l) {
         const int p = l >> 1;
-        const T Z = r[p * ls + k];
-        const T Zm = r[p * ls + (k == 0 ? 0 : nz - k)];
+        const T Z = r[p * ls + sw(k)];
+        const T Zm = r[p * ls + sw(k == 0 ? 0 : nz - k)];
         T o;
         if ((l & 1) == 0) {  // (Z + conj(Zm)) / 2
           o.x = (Z.x + Zm.x) * S(0.5);
@@ -319,7 +326,7 @@ __device__ __forceinline__ void pass_z_c2r_body(const typename CX<S>::T* __restr
   using T = typename CX<S>::T;
   constexpr int TY = FftTiles<S>::kZ;
   extern __shared__ __align__(16) unsigned char smraw[];
-  const int nz = pl.n, ls = nz + 1;
+  const int nz = pl.n, ls = line_stride(nz);
   // a: (TY/2) packed lines; b: the tile's half spectra first (TY x (nh+1)),
   // then the FFT's ping-pong buffer -- sized max of the two (see pass_smem)
   T* tw = reinterpret_cast<T*>(smraw);
@@ -351,7 +358,7 @@ __device__ __forceinline__ void pass_z_c2r_body(const typename CX<S>::T* __restr
       Ae.y = S(0);
       Ao.y = S(0);
     }
-    a[p * ls + k] = T{Ae.x - Ao.y, Ae.y + Ao.x};
+    a[p * ls + sw(k)] = T{Ae.x - Ao.y, Ae.y + Ao.x};
   }
   __syncthreads();
   const T* r = line_fft<1, B16>(a, b, tw, pl, npair, ls);
@@ -359,7 +366,7 @@ __device__ __forceinline__ void pass_z_c2r_body(const typename CX<S>::T* __restr
   copy_rows<S>(
       ty, nz,
       [&](int l, int z) {
-        const T Z = r[(l >> 1) * ls + z];
+        const T Z = r[(l >> 1) * ls + sw(z)];
         return ((l & 1) ? Z.y : Z.x) * scale;
       },
       [&](int l, int z, S v) { dst[l * nz + z] = v; });
@@ -376,7 +383,7 @@ __device__ __forceinline__ void pass_y_body(const typename CX<R>::T* __restrict_
   using T = typename CX<R>::T;
   constexpr int TX = FftTiles<R>::kY;
   extern __shared__ __align__(16) unsigned char smraw[];
-  const int ny = pl.n, ls = ny + 1;
+  const int ny = pl.n, ls = line_stride(ny);
   T* tw = reinterpret_cast<T*>(smraw);
   T* a = tw + ny;
   T* b = a + TX * ls;
@@ -395,23 +402,23 @@ __device__ __forceinline__ void pass_y_body(const typename CX<R>::T* __restrict_
   if (SIGN < 0) {
     copy_rows<T>(
         TX, ny, [&](int xl, int y) { return xl < tx ? in_a[xl * a_xs + y] : T{R(0), R(0)}; },
-        [&](int xl, int y, T v) { a[xl * ls + y] = v; });
+        [&](int xl, int y, T v) { a[xl * ls + sw(y)] = v; });
   } else {
     copy_short_rows<TX, T>(
         ny, [&](int y, int xl) { return xl < tx ? in_b[y * nx + xl] : T{R(0), R(0)}; },
-        [&](int y, int xl, T v) { a[xl * ls + y] = v; });
+        [&](int y, int xl, T v) { a[xl * ls + sw(y)] = v; });
   }
   __syncthreads();
   const T* r = line_fft<SIGN, B16>(a, b, tw, pl, TX, ls);
   if (SIGN < 0) {
     copy_short_rows<TX, T>(
-        ny, [&](int y, int xl) { return r[xl * ls + y]; },
+        ny, [&](int y, int xl) { return r[xl * ls + sw(y)]; },
         [&](int y, int xl, T v) {
           if (xl < tx) out_b[y * nx + xl] = v;
         });
   } else {
     copy_rows<T>(
-        tx, ny, [&](int xl, int y) { return r[xl * ls + y]; },
+        tx, ny, [&](int xl, int y) { return r[xl * ls + sw(y)]; },
         [&](int xl, int y, T v) { out_a[xl * a_xs + y] = v; });
   }
 }
@@ -426,7 +433,7 @@ __device__ __forceinline__ void pass_x_body(typename CX<R>::T* __restrict__ B, c
   using T = typename CX<R>::T;
   constexpr int TK = FftTiles<R>::kX;
   extern __shared__ __align__(16) unsigned char smraw[];
-  const int nx = pl.n, ls = nx + 1;
+  const int nx = pl.n, ls = line_stride(nx);
   T* tw = reinterpret_cast<T*>(smraw);
   T* a = tw + nx;
   T* b = a + ncomp * TK * ls;
@@ -443,7 +450,7 @@ __device__ __forceinline__ void pass_x_body(typename CX<R>::T* __restrict__ B, c
         const int c = L / TK, kl = L - c * TK;
         return kl < tk ? Bb[c * cs + kl * nx + xx] : T{R(0), R(0)};
       },
-      [&](int L, int xx, T v) { a[L * ls + xx] = v; });
+      [&](int L, int xx, T v) { a[L * ls + sw(xx)] = v; });
   __syncthreads();
   T* r = a;
   T* o = b;
@@ -458,19 +465,19 @@ __device__ __forceinline__ void pass_x_body(typename CX<R>::T* __restrict__ B, c
       R pre[5], pim[5];
 #pragma unroll
       for (int c = 0; c < 5; ++c) {
-        const T z = r[(c * TK + kl) * ls + xx];
+        const T z = r[(c * TK + kl) * ls + sw(xx)];
         pre[c] = z.x;
         pim[c] = z.y;
       }
       green_apply<R>(gp, xx, ky0 + kl, kz, pre, pim);
 #pragma unroll
-      for (int c = 0; c < 5; ++c) r[(c * TK + kl) * ls + xx] = T{pre[c], pim[c]};
+      for (int c = 0; c < 5; ++c) r[(c * TK + kl) * ls + sw(xx)] = T{pre[c], pim[c]};
     }
     __syncthreads();
   }
   if (MODE != 0) r = line_fft<1, B16>(r, o, tw, pl, nl, ls);
   copy_rows<T>(
-      nl, nx, [&](int L, int xx) { return r[L * ls + xx]; },
+      nl, nx, [&](int L, int xx) { return r[L * ls + sw(xx)]; },
       [&](int L, int xx, T v) {
         const int c = L / TK, kl = L - c * TK;
         if (kl < tk) Bb[c * cs + kl * nx + xx] = v;
@@ -600,12 +607,12 @@ PassSmem<R> pass_smem(const Spectral<R>& sp, int ncomp) {
   using T = typename CX<R>::T;
   PassSmem<R> s;
   const int TY = FftTiles<R>::kZ, TX = FftTiles<R>::kY, TK = FftTiles<R>::kX;
-  const int lz = sp.nz + 1;
+  const int lz = line_stride(sp.nz);
   s.z_r2c = sizeof(T) * (sp.nz + 2 * (size_t)(TY / 2) * lz);
   const size_t bsz = std::max((size_t)(TY / 2) * lz, (size_t)TY * (sp.nh + 1));
   s.z_c2r = sizeof(T) * (sp.nz + (size_t)(TY / 2) * lz + bsz);
-  s.y = sizeof(T) * (sp.ny + 2 * (size_t)TX * (sp.ny + 1));
-  s.x = sizeof(T) * (sp.nx + 2 * (size_t)ncomp * TK * (sp.nx + 1));
+  s.y = sizeof(T) * (sp.ny + 2 * (size_t)TX * line_stride(sp.ny));
+  s.x = sizeof(T) * (sp.nx + 2 * (size_t)ncomp * TK * line_stride(sp.nx));
   return s;
 }
 // Dynamic shared memory limit = the opt-in maximum minus the kernel's static part.
