@@ -106,7 +106,8 @@ def test_green_operator(lib, port, dims, h):
 
 
 @pytest.mark.parametrize("dims", [(16, 16, 16), (15, 12, 10), (8, 6, 5), (32, 24, 48), (5, 9, 15),
-                                  (64, 64, 64), (1, 4, 3), (2, 2, 2)])
+                                  (64, 64, 64), (1, 4, 3), (2, 2, 2), (96, 16, 128),
+                                  (16, 256, 32), (48, 32, 512), (8, 384, 16), (192, 10, 16)])
 def test_fft_r2c_and_c2r(lib, dims):
     rng = np.random.default_rng(6)
     a = rng.normal(size=(3,) + dims)

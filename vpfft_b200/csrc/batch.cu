@@ -337,41 +337,59 @@ vpfft_status start_loop(vpfft_batch* b, Active& a) {
 }
 
 // The iteration lists of the slots in ITER phase.
-struct IterLists {
-  HostList z, y, x, nr[2], fin[2];
-  SpectralShape smax{};
+// The RVEs of one pass that share a line engine.
+struct GroupList {
+  const void* set;
+  HostList list;
+  size_t smem_a = 0, smem_b = 0;
 };
+struct IterLists {
+  std::vector<GroupList> z, y, x;
+  HostList nr[2], fin[2];
+};
+
+void add_to_group(std::vector<GroupList>& gs, const void* set, int slot, int blocks,
+                  size_t smem_a, size_t smem_b) {
+  GroupList* g = nullptr;
+  for (GroupList& e : gs)
+    if (e.set == set) g = &e;
+  if (!g) {
+    gs.push_back(GroupList{set, HostList{}, 0, 0});
+    g = &gs.back();
+  }
+  g->list.add(slot, blocks);
+  g->smem_a = std::max(g->smem_a, smem_a);
+  g->smem_b = std::max(g->smem_b, smem_b);
+}
 
 template <typename S>
 void build_iter_lists(vpfft_batch* b, IterLists& L) {
-  L.smax = SpectralShape{};
   for (const Active& a : b->active) {
     if (a.phase != kIter) continue;
     const SlotDesc<S>& d = *host_desc<S>(b, a.slot);
     const SpectralShape sh = spectral_shape<S>(d.sp, 5);
-    L.z.add(a.slot, sh.blocks_z);
-    L.y.add(a.slot, sh.blocks_y);
-    L.x.add(a.slot, sh.blocks_x);
+    add_to_group(L.z, sh.set_z, a.slot, sh.blocks_z, sh.smem_z_r2c, sh.smem_z_c2r);
+    add_to_group(L.y, sh.set_y, a.slot, sh.blocks_y, sh.smem_y, 0);
+    add_to_group(L.x, sh.set_x, a.slot, sh.blocks_x, sh.smem_x, 0);
     L.nr[a.tau].add(a.slot, d.nr_blocks);
     L.fin[a.tau].add(a.slot, 1);
-    L.smax.smem_z_r2c = std::max(L.smax.smem_z_r2c, sh.smem_z_r2c);
-    L.smax.smem_z_c2r = std::max(L.smax.smem_z_c2r, sh.smem_z_c2r);
-    L.smax.smem_y = std::max(L.smax.smem_y, sh.smem_y);
-    L.smax.smem_x = std::max(L.smax.smem_x, sh.smem_x);
-    L.smax.r16_z = L.smax.r16_z || sh.r16_z;
-    L.smax.r16_y = L.smax.r16_y || sh.r16_y;
-    L.smax.r16_x = L.smax.r16_x || sh.r16_x;
   }
 }
 
+// lists: the z, y and x groups in order, then nr[0], nr[1], fin[0], fin[1]
 template <typename S>
 int enqueue_iterations(vpfft_batch* b, const std::vector<BatchLaunch>& bl, const IterLists& L,
                        int iters) {
+  std::vector<PassGroup> z, y, x;
+  size_t k = 0;
+  for (const GroupList& g : L.z) z.push_back(PassGroup{g.set, bl[k++], g.smem_a, g.smem_b});
+  for (const GroupList& g : L.y) y.push_back(PassGroup{g.set, bl[k++], g.smem_a, g.smem_b});
+  for (const GroupList& g : L.x) x.push_back(PassGroup{g.set, bl[k++], g.smem_a, g.smem_b});
   int n = 0;
   for (int it = 0; it < iters; ++it) {
-    n += launch_spectral_batch<S>(dev_desc<S>(b), bl[0], bl[1], bl[2], L.smax, b->stream);
+    n += launch_spectral_batch<S>(dev_desc<S>(b), z, y, x, b->stream);
     for (int t = 0; t < 2; ++t)
-      n += launch_nr_update_batch<S>(dev_desc<S>(b), bl[3 + t], bl[5 + t], b->nexp, t == 1,
+      n += launch_nr_update_batch<S>(dev_desc<S>(b), bl[k + t], bl[k + 2 + t], b->nexp, t == 1,
                                      b->stream);
   }
   return n;
@@ -385,7 +403,7 @@ template <typename S>
 vpfft_status run_iterations(vpfft_batch* b) {
   IterLists L;
   build_iter_lists<S>(b, L);
-  if (L.z.m() == 0) return VPFFT_OK;
+  if (L.z.empty()) return VPFFT_OK;
   const int iters = std::max(1, b->bopt.iterations_per_tick);
   if (b->bopt.use_graphs && b->graph && b->graph_generation == b->iter_generation) {
     BCK(b, cudaGraphLaunch(b->graph, b->stream));
@@ -396,7 +414,10 @@ vpfft_status run_iterations(vpfft_batch* b) {
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
   }
-  std::vector<HostList*> lists = {&L.z, &L.y, &L.x, &L.nr[0], &L.nr[1], &L.fin[0], &L.fin[1]};
+  std::vector<HostList*> lists;
+  for (std::vector<GroupList>* gs : {&L.z, &L.y, &L.x})
+    for (GroupList& g : *gs) lists.push_back(&g.list);
+  for (HostList* h : {&L.nr[0], &L.nr[1], &L.fin[0], &L.fin[1]}) lists.push_back(h);
   std::vector<BatchLaunch> bl;
   if (vpfft_status s = upload_lists(b, b->iter_lists, lists, bl)) return s;
   if (b->bopt.use_graphs && b->eager_generation == b->iter_generation) {

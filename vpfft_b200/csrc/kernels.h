@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "device_math.cuh"
 #include "nr_kernel.cuh"
 
@@ -65,8 +67,12 @@ inline FastDiv make_fast_div(uint32_t d) {
   return FastDiv{(uint32_t)m, l};
 }
 #ifdef __CUDACC__
-__device__ __forceinline__ uint32_t fast_div(uint32_t t, const FastDiv& f) {
+__host__ __device__ __forceinline__ uint32_t fast_div(uint32_t t, const FastDiv& f) {
+#ifdef __CUDA_ARCH__
   return (__umulhi(t, f.mul) + t) >> f.shift;
+#else
+  return (uint32_t)((((uint64_t)t * f.mul) >> 32) + t) >> f.shift;
+#endif
 }
 #endif
 
@@ -190,19 +196,30 @@ int launch_ref_medium_batch(const SlotDesc<S>* d, const BatchLaunch& bl,
                             const BatchLaunch& bl_slots, cudaStream_t st);
 template <typename S>
 int launch_post_batch(const SlotDesc<S>* d, const BatchLaunch& bl, cudaStream_t st);
-// Blocks and dynamic shared memory of the five FFT passes of one RVE.
+// Blocks, dynamic shared memory and line engine ("pass set", chosen by the
+// axis length) of the five FFT passes of one RVE.
 struct SpectralShape {
   int blocks_z, blocks_y, blocks_x;
   size_t smem_z_r2c, smem_z_c2r, smem_y, smem_x;
-  bool r16_z, r16_y, r16_x;  // a line plan of that axis has a radix-16 stage
+  const void* set_z;
+  const void* set_y;
+  const void* set_x;
 };
 template <typename S>
 SpectralShape spectral_shape(const Spectral<S>& sp, int ncomp);
-// The five passes of one iteration over a batch; bl_z / bl_y / bl_x list the
-// blocks of the z, y and x passes, smem the maxima over the batch.
+// The RVEs of one batched pass that share a line engine: their blocks and the
+// largest dynamic shared memory among them (smem_a: r2c / forward / x pass,
+// smem_b: c2r).
+struct PassGroup {
+  const void* set;
+  BatchLaunch bl;
+  size_t smem_a, smem_b;
+};
+// The five passes of one iteration over a batch, one launch per pass and
+// engine group.
 template <typename S>
-int launch_spectral_batch(const SlotDesc<S>* d, const BatchLaunch& bl_z, const BatchLaunch& bl_y,
-                          const BatchLaunch& bl_x, const SpectralShape& smem_max,
+int launch_spectral_batch(const SlotDesc<S>* d, const std::vector<PassGroup>& z,
+                          const std::vector<PassGroup>& y, const std::vector<PassGroup>& x,
                           cudaStream_t st);
 
 // --- batched solver entry points for testing (double, voxel-major) ---------
