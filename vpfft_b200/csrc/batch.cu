@@ -385,12 +385,16 @@ int enqueue_iterations(vpfft_batch* b, const std::vector<BatchLaunch>& bl, const
   for (const GroupList& g : L.z) z.push_back(PassGroup{g.set, bl[k++], g.smem_a, g.smem_b});
   for (const GroupList& g : L.y) y.push_back(PassGroup{g.set, bl[k++], g.smem_a, g.smem_b});
   for (const GroupList& g : L.x) x.push_back(PassGroup{g.set, bl[k++], g.smem_a, g.smem_b});
+  // material and solver constants: those of any iterating slot (a batch admits
+  // only grids with its own material and options)
+  const int any = !L.nr[0].slot.empty() ? L.nr[0].slot[0] : L.nr[1].slot[0];
+  const NRParams& material = host_desc<S>(b, any)->nr;
   int n = 0;
   for (int it = 0; it < iters; ++it) {
     n += launch_spectral_batch<S>(dev_desc<S>(b), z, y, x, b->stream);
     for (int t = 0; t < 2; ++t)
-      n += launch_nr_update_batch<S>(dev_desc<S>(b), bl[k + t], bl[k + 2 + t], b->nexp, t == 1,
-                                     b->stream);
+      n += launch_nr_update_batch<S>(dev_desc<S>(b), bl[k + t], bl[k + 2 + t], material, b->nexp,
+                                     t == 1, b->stream);
   }
   return n;
 }

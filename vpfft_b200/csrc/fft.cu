@@ -85,7 +85,7 @@ int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S
   if (ev) cudaEventRecord(ev[1], st);
   Y.y_fwd<<<gy, Y.threads, sm.y, st>>>(A, B, sp.py, sp.px.by_n, twy, sp.nx, sp.nh, ctrl);
   if (ev) cudaEventRecord(ev[2], st);
-  X.x_green<<<gx, X.threads, sm.x, st>>>(B, sp.px, sp.py.by_n, twx, gp, sp.ny, sp.nh, ncomp,
+  X.x_green<<<gx, X.threads_x, sm.x, st>>>(B, sp.px, sp.py.by_n, twx, gp, sp.ny, sp.nh, ncomp,
                                          ctrl);
   if (ev) cudaEventRecord(ev[3], st);
   Y.y_inv<<<gy, Y.threads, sm.y, st>>>(B, A, sp.py, sp.px.by_n, twy, sp.nx, sp.nh, ctrl);
@@ -116,10 +116,10 @@ int launch_fft3d(const Spectral<S>& sp, S* real, int ncomp, int mode, cudaStream
     Z.z_r2c<<<gz, Z.threads, sm.z_r2c, st>>>(real, A, sp.pz, sp.py.by_n, twz, sp.nx, sp.ny, sp.nh,
                                              nullptr);
     Y.y_fwd<<<gy, Y.threads, sm.y, st>>>(A, B, sp.py, sp.px.by_n, twy, sp.nx, sp.nh, nullptr);
-    X.x_fwd<<<gx, X.threads, sm.x, st>>>(B, sp.px, sp.py.by_n, twx, gp, sp.ny, sp.nh, ncomp,
+    X.x_fwd<<<gx, X.threads_x, sm.x, st>>>(B, sp.px, sp.py.by_n, twx, gp, sp.ny, sp.nh, ncomp,
                                          nullptr);
   } else {
-    X.x_inv<<<gx, X.threads, sm.x, st>>>(B, sp.px, sp.py.by_n, twx, gp, sp.ny, sp.nh, ncomp,
+    X.x_inv<<<gx, X.threads_x, sm.x, st>>>(B, sp.px, sp.py.by_n, twx, gp, sp.ny, sp.nh, ncomp,
                                          nullptr);
     Y.y_inv<<<gy, Y.threads, sm.y, st>>>(B, A, sp.py, sp.px.by_n, twy, sp.nx, sp.nh, nullptr);
     const S scale = S(1.0 / ((double)sp.nx * sp.ny * sp.nz));
@@ -167,7 +167,7 @@ int launch_spectral_batch(const SlotDesc<S>* d, const std::vector<PassGroup>& z,
     }
   for (const PassGroup& g : x)
     if (g.bl.blocks > 0) {
-      set(g)->bx_green<<<g.bl.blocks, set(g)->threads, g.smem_a, st>>>(d, g.bl);
+      set(g)->bx_green<<<g.bl.blocks, set(g)->threads_x, g.smem_a, st>>>(d, g.bl);
       ++n;
     }
   for (const PassGroup& g : y)

@@ -31,14 +31,18 @@ namespace vpfft {
 namespace fft {
 
 // Lines per block and threads per block of an engine.  Fixed engines of
-// length >= 64 hold about 2048 complex values per ping-pong buffer, so a
-// radix-16 stage gives every one of the 128 threads one butterfly; shorter
-// lines take 512 so that a small grid still spreads over many blocks.  The
-// generic engine keeps 256 threads and its short tiles.
+// length >= 64 hold about 2048 (FP32) or 1024 (FP64) complex values per
+// ping-pong buffer; shorter lines take 512 so that a small grid still spreads
+// over many blocks.  The z and y passes run 256 (FP32) or 128 (FP64) threads
+// per block, the x pass (two transforms and the Green operator) 128 threads,
+// the settings measured fastest at 256^3.  The generic engine keeps 256
+// threads and its short tiles.
 template <typename S, class E>
 struct Tiles {
-  static constexpr int kElems = E::kN >= 64 ? 2048 : 512;
-  static constexpr int kThreads = E::kN ? 128 : 256;
+  static constexpr bool kF32 = sizeof(S) == 4;
+  static constexpr int kElems = E::kN >= 64 ? (kF32 ? 2048 : 1024) : 512;
+  static constexpr int kThreads = E::kN ? (kF32 ? 256 : 128) : 256;  // z and y passes
+  static constexpr int kThreadsX = E::kN ? 128 : 256;                // x pass
   static constexpr int cmax(int a, int b) { return a > b ? a : b; }
   static constexpr int kZ = E::kN ? cmax(2, 2 * (kElems / E::kN)) : 16;  // real z-lines
   static constexpr int kY = E::kN ? cmax(1, kElems / E::kN) : (sizeof(S) == 4 ? 16 : 8);
@@ -357,7 +361,7 @@ __global__ void __launch_bounds__(Tiles<S, E>::kThreads)
   pass_y_body<SIGN, S, E>(in, out, pl, dnx, twg, nx, nh, blockIdx.x, blockIdx.y);
 }
 template <int MODE, typename S, class E>
-__global__ void __launch_bounds__(Tiles<S, E>::kThreads, 512 / Tiles<S, E>::kThreads)
+__global__ void __launch_bounds__(Tiles<S, E>::kThreadsX, 512 / Tiles<S, E>::kThreadsX)
     k_pass_x(typename CX<S>::T* __restrict__ B, LinePlan pl, FastDiv dny,
              const typename CX<S>::T* __restrict__ twg, GreenParams<S> gp, int ny, int nh,
              int ncomp, const IterCtrl* ctrl) {
@@ -431,7 +435,7 @@ __global__ void __launch_bounds__(Tiles<S, E>::kThreads)
                           sp.nh, lb - c * gt, c);
 }
 template <typename S, class E>
-__global__ void __launch_bounds__(Tiles<S, E>::kThreads, 512 / Tiles<S, E>::kThreads)
+__global__ void __launch_bounds__(Tiles<S, E>::kThreadsX, 512 / Tiles<S, E>::kThreadsX)
     k_pass_x_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
   using T = typename CX<S>::T;
   __shared__ SlotSpectral<S> sm;
@@ -447,7 +451,7 @@ __global__ void __launch_bounds__(Tiles<S, E>::kThreads, 512 / Tiles<S, E>::kThr
 template <typename S>
 struct PassSet {
   using T = typename CX<S>::T;
-  int threads;
+  int threads, threads_x;  // z and y passes, x pass
   int tz, ty, tk;  // real z-lines, y-lines and ky-lines (per component) per block
   void (*z_r2c)(const S*, T*, LinePlan, FastDiv, const T*, int, int, int, const IterCtrl*);
   void (*z_c2r)(const T*, S*, LinePlan, FastDiv, const T*, int, int, int, S, const IterCtrl*);
@@ -478,6 +482,7 @@ PassSet<S> make_pass_set() {
   using Ti = Tiles<S, E>;
   PassSet<S> p;
   p.threads = Ti::kThreads;
+  p.threads_x = Ti::kThreadsX;
   p.tz = Ti::kZ;
   p.ty = Ti::kY;
   p.tk = Ti::kX;

@@ -186,10 +186,13 @@ int nr_launch_blocks(const NRParams& p, bool tau, bool init);
 template <typename S>
 int launch_init_batch(const SlotDesc<S>* d, const BatchLaunch& bl, int nexp, bool tau,
                       cudaStream_t st);
-// NR sweep + per-slot finish (bl_slots: one block per slot)
+// NR sweep + per-slot finish (bl_slots: one block per slot).  material: the
+// batch's material and solver constants (every slot's NRParams agrees on them;
+// the slot's strain rate and reference medium come from its descriptor).
 template <typename S>
 int launch_nr_update_batch(const SlotDesc<S>* d, const BatchLaunch& bl,
-                           const BatchLaunch& bl_slots, int nexp, bool tau, cudaStream_t st);
+                           const BatchLaunch& bl_slots, const NRParams& material, int nexp,
+                           bool tau, cudaStream_t st);
 // reference medium: per-voxel inverse + per-slot column sums into sum25
 template <typename S>
 int launch_ref_medium_batch(const SlotDesc<S>* d, const BatchLaunch& bl,

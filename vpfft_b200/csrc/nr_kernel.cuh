@@ -102,6 +102,26 @@ __host__ __device__ inline void set_fp32_copies(NRParams& p) {
   for (int k = 0; k < 15; ++k) p.L0inv_f[k] = (float)p.L0inv[k];
 }
 
+// The constants of a voxel solve that differ between the RVEs of a batch
+// (imposed strain rate, L0, L0^-1).  A single-grid kernel reads them from its
+// parameter struct (constant bank operands); a batched kernel reads its slot's
+// copy in shared memory through a volatile pointer, so every use is a fresh
+// load instead of a value the compiler keeps in registers across the solve.
+struct ParamConsts {
+  const NRParams& p;
+  __device__ __forceinline__ double edot(int k) const { return p.edot[k]; }
+  __device__ __forceinline__ double L0(int k) const { return p.L0[k]; }
+  __device__ __forceinline__ double L0inv(int k) const { return p.L0inv[k]; }
+  __device__ __forceinline__ float L0inv_f(int k) const { return p.L0inv_f[k]; }
+};
+struct SharedConsts {
+  const volatile NRParams* p;
+  __device__ __forceinline__ double edot(int k) const { return p->edot[k]; }
+  __device__ __forceinline__ double L0(int k) const { return p->L0[k]; }
+  __device__ __forceinline__ double L0inv(int k) const { return p->L0inv[k]; }
+  __device__ __forceinline__ float L0inv_f(int k) const { return p->L0inv_f[k]; }
+};
+
 // The per-system constants in the arithmetic type of a Newton pass.
 template <typename T>
 struct NRConst;
@@ -351,9 +371,9 @@ __device__ __forceinline__ bool accumulate_pairs(const float* msm, const float* 
 // true and the iterate in s_io when it converged with finite values; the
 // caller then takes the accepted step with FP64 residual and Jacobian.
 // *rmax0 gets max_s |r_s| at the starting point.
-template <int NEXP, bool kTauSmem, typename MS>
+template <int NEXP, bool kTauSmem, typename MS, class C>
 __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, int bs,
-                                                const NRParams& p, const float L0i[15],
+                                                const NRParams& p, const C& cs,
                                                 const double lam[5], const double ed[5],
                                                 double s_io[5], int max_steps, float* rmax0) {
   float cur[5], l32[5], e32[5];
@@ -378,11 +398,11 @@ __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, in
     for (int i = 0; i < 5; ++i) {
       float a = S[i] - e32[i];
 #pragma unroll
-      for (int j = 0; j < 5; ++j) a += L0i[sym5(i, j)] * (cur[j] - l32[j]);
+      for (int j = 0; j < 5; ++j) a += cs.L0inv_f(sym5(i, j)) * (cur[j] - l32[j]);
       y[i] = -a;
     }
 #pragma unroll
-    for (int k = 0; k < 15; ++k) K[k] += L0i[k];
+    for (int k = 0; k < 15; ++k) K[k] += cs.L0inv_f(k);
     float delta[5];
     if (!ldlt5_solve(K, y, delta)) return false;
     float dn = 0.f, an = 0.f;
@@ -407,9 +427,10 @@ __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, in
 
 // SolveConstrainedConstitutiveEquations (Solvers.cpp:111-222).  ed = Edot + d~.
 // Returns the Newton steps taken; *capped when the iteration budget ran out.
-template <int NEXP, bool kTauSmem, typename MS>
+template <int NEXP, bool kTauSmem, typename MS, class C = ParamConsts>
 __device__ __forceinline__ int nr_constrained_smem(const MS* msm, const MS* tsm, int bs,
-                                                   const NRParams& p, const double lam[5],
+                                                   const NRParams& p, const C& cs,
+                                                   const double lam[5],
                                                    const double ed[5], double s_io[5],
                                                    double* rel_out, bool* capped,
                                                    double* e_lin = nullptr) {
@@ -447,11 +468,11 @@ __device__ __forceinline__ int nr_constrained_smem(const MS* msm, const MS* tsm,
     for (int i = 0; i < 5; ++i) {
       double a = S[i] - ed[i];
 #pragma unroll
-      for (int j = 0; j < 5; ++j) a += p.L0inv[sym5(i, j)] * dl[j];
+      for (int j = 0; j < 5; ++j) a += cs.L0inv(sym5(i, j)) * dl[j];
       y[i] = -a;
     }
 #pragma unroll
-    for (int k = 0; k < 15; ++k) K[k] += p.L0inv[k];
+    for (int k = 0; k < 15; ++k) K[k] += cs.L0inv(k);
     double delta[5];
     ldlt5_solve<double>(K, y, delta);
     double dn = 0.0, an = 0.0;
@@ -480,7 +501,7 @@ __device__ __forceinline__ int nr_constrained_smem(const MS* msm, const MS* tsm,
     for (int i = 0; i < 5; ++i) {
       double a = ed[i];
 #pragma unroll
-      for (int j = 0; j < 5; ++j) a -= p.L0inv[sym5(i, j)] * (nw[j] - lam[j]);
+      for (int j = 0; j < 5; ++j) a -= cs.L0inv(sym5(i, j)) * (nw[j] - lam[j]);
       e_lin[i] = a;
     }
   }

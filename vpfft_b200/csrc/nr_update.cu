@@ -24,8 +24,10 @@ template <typename MS>
 constexpr int nr_min_blocks() {
   return sizeof(MS) == 8 ? 3 : 4;
 }
-// The batched kernels read the slot's constants from shared memory instead of
-// the constant bank, which costs registers: three blocks per SM.
+// The batched initialisation kernel reads all of the slot's constants from
+// shared memory instead of the constant bank, which costs registers: three
+// blocks per SM.  (The batched NR sweep takes its material constants from the
+// constant bank and has the single-grid kernel's bound.)
 template <typename MS>
 constexpr int nr_batch_min_blocks() {
   return 3;
@@ -50,7 +52,7 @@ __device__ __forceinline__ void voxel_schmid(const FieldPtrs<S>& f, long long n,
 template <typename S, typename MS, int NEXP, bool kTauSmem>
 __device__ __forceinline__ void init_body(const NRParams& p, const FieldPtrs<S>& f,
                                           IterCtrl* ctrl, int blk, int nblk, MS* msm, MS* tsm) {
-  const int bs = blockDim.x;
+  constexpr int bs = kVoxelBlock;  // every launch of these kernels uses kVoxelBlock threads
   const long long n = p.n;
   unsigned long long capped_count = 0;
   int status = 0;
@@ -90,7 +92,7 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
            IterCtrl* ctrl) {
   extern __shared__ __align__(16) unsigned char nr_smem[];
   MS* msm = reinterpret_cast<MS*>(nr_smem) + SL<MS>::kThreadStride * threadIdx.x;
-  MS* tsm = msm + 60 * blockDim.x;
+  MS* tsm = msm + 60 * kVoxelBlock;
   init_body<S, MS, NEXP, kTauSmem>(p, f, ctrl, blockIdx.x, gridDim.x, msm, tsm);
 }
 
@@ -108,7 +110,7 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_batch_min_blocks<MS>())
   copy_struct(&sf, &d.f);
   __syncthreads();
   MS* msm = reinterpret_cast<MS*>(nr_smem) + SL<MS>::kThreadStride * threadIdx.x;
-  MS* tsm = msm + 60 * blockDim.x;
+  MS* tsm = msm + 60 * kVoxelBlock;
   init_body<S, MS, NEXP, kTauSmem>(sp, sf, d.ctrl, lb, d.init_blocks, msm, tsm);
 }
 
@@ -120,12 +122,14 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_batch_min_blocks<MS>())
 // and P on exit.  Persistent grid-stride loop: every thread solves many voxels
 // and the block reduces once, so the spread of Newton iteration counts between
 // voxels averages out instead of idling warps at a barrier.
-template <typename S, typename MS, int NEXP, bool kTauSmem>
-__device__ __forceinline__ void nr_update_body(const NRParams& p, const FieldPtrs<S>& f,
-                                               double* partials, IterCtrl* ctrl, int blk,
-                                               int nblk, MS* msm, MS* tsm) {
-  const int bs = blockDim.x;
-  const long long n = p.n;
+// p: the material and solver constants; cs: the RVE's strain rate and
+// reference medium; n: its voxel count.
+template <typename S, typename MS, int NEXP, bool kTauSmem, class C>
+__device__ __forceinline__ void nr_update_body(const NRParams& p, const C& cs, long long n,
+                                               const FieldPtrs<S>& f, double* partials,
+                                               IterCtrl* ctrl, int blk, int nblk, MS* msm,
+                                               MS* tsm) {
+  constexpr int bs = kVoxelBlock;  // every launch of these kernels uses kVoxelBlock threads
   double acc[12];
 #pragma unroll
   for (int k = 0; k < 12; ++k) acc[k] = 0.0;
@@ -140,7 +144,7 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const FieldPtr
     if (f.dkeep) store5(f.dkeep, n, v, d);
     double ed[5];
 #pragma unroll
-    for (int c = 0; c < 5; ++c) ed[c] = p.edot[c] + d[c];
+    for (int c = 0; c < 5; ++c) ed[c] = cs.edot(c) + d[c];
     double rel, e[5];
     bool capped;
     if constexpr (sizeof(S) == 4) {
@@ -150,11 +154,10 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const FieldPtr
       // starts where the reference's does, at sigma / MaxRSS.  The strain rate
       // comes from the last Newton linearisation when that step was tiny.
       float mx0;
-      const float* L0i = p.L0inv_f;
       double s0[5];
 #pragma unroll
       for (int c = 0; c < 5; ++c) s0[c] = s[c];
-      const bool ok = nr_predict_fp32<NEXP, kTauSmem>(msm, tsm, bs, p, L0i, lam, ed, s, 8, &mx0);
+      const bool ok = nr_predict_fp32<NEXP, kTauSmem>(msm, tsm, bs, p, cs, lam, ed, s, 8, &mx0);
       if (mx0 < 1e-10f) status |= kStatusMaxRssTiny;
       if (!ok) {
         const double mx = max_resolved<kTauSmem>(msm, tsm, bs, p, s0);
@@ -162,7 +165,7 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const FieldPtr
         for (int c = 0; c < 5; ++c) s[c] = s0[c] / mx;
       }
       double el[5];
-      nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, lam, ed, s, &rel, &capped, el);
+      nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, cs, lam, ed, s, &rel, &capped, el);
       if (!capped && rel < 1e-5) {
 #pragma unroll
         for (int c = 0; c < 5; ++c) e[c] = el[c];
@@ -174,7 +177,7 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const FieldPtr
       if (mx < 1e-10) status |= kStatusMaxRssTiny;
 #pragma unroll
       for (int c = 0; c < 5; ++c) s[c] /= mx;
-      nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, lam, ed, s, &rel, &capped);
+      nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, cs, lam, ed, s, &rel, &capped);
       apply_smem<NEXP, kTauSmem>(msm, tsm, bs, p, s, e);
     }
     capped_count += capped ? 1 : 0;
@@ -184,8 +187,9 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const FieldPtr
       double ld = 0.0, lt = 0.0;
 #pragma unroll
       for (int j = 0; j < 5; ++j) {
-        ld += p.L0[j * 5 + i] * d[j];
-        lt += p.L0[j * 5 + i] * (ed[j] - e[j]);
+        const double l0 = cs.L0(j * 5 + i);
+        ld += l0 * d[j];
+        lt += l0 * (ed[j] - e[j]);
       }
       P[i] = s[i] - ld;
       lam[i] += lt;
@@ -199,7 +203,7 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const FieldPtr
       acc[c] += s[c];
       acc[5 + c] += e[c];
       const double ds = s[c] - lam[c];
-      const double de = e[c] - p.edot[c] - d[c];
+      const double de = e[c] - cs.edot(c) - d[c];
       es += ds * ds;
       ee += de * de;
     }
@@ -218,13 +222,15 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
   if (ctrl->done) return;
   extern __shared__ __align__(16) unsigned char nr_smem[];
   MS* msm = reinterpret_cast<MS*>(nr_smem) + SL<MS>::kThreadStride * threadIdx.x;
-  MS* tsm = msm + 60 * blockDim.x;
-  nr_update_body<S, MS, NEXP, kTauSmem>(p, f, partials, ctrl, blockIdx.x, gridDim.x, msm, tsm);
+  MS* tsm = msm + 60 * kVoxelBlock;
+  nr_update_body<S, MS, NEXP, kTauSmem>(p, ParamConsts{p}, p.n, f, partials, ctrl, blockIdx.x,
+                                        gridDim.x, msm, tsm);
 }
 
 template <typename S, typename MS, int NEXP, bool kTauSmem>
-__global__ void __launch_bounds__(kVoxelBlock, nr_batch_min_blocks<MS>())
-    k_nr_update_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
+__global__ void __launch_bounds__(kVoxelBlock, nr_min_blocks<MS>())
+    k_nr_update_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl,
+                      const __grid_constant__ NRParams pm) {
   int lb;
   const SlotDesc<S>& d = desc[batch_slot(bl, blockIdx.x, &lb)];
   if (d.ctrl->done) return;
@@ -235,8 +241,11 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_batch_min_blocks<MS>())
   copy_struct(&sf, &d.f);
   __syncthreads();
   MS* msm = reinterpret_cast<MS*>(nr_smem) + SL<MS>::kThreadStride * threadIdx.x;
-  MS* tsm = msm + 60 * blockDim.x;
-  nr_update_body<S, MS, NEXP, kTauSmem>(sp, sf, d.partials, d.ctrl, lb, d.nr_blocks, msm, tsm);
+  MS* tsm = msm + 60 * kVoxelBlock;
+  // material and solver constants (the same for every RVE of a batch) from the
+  // kernel parameter; the slot's strain rate and reference medium from shared memory
+  nr_update_body<S, MS, NEXP, kTauSmem>(pm, SharedConsts{&sp}, sp.n, sf, d.partials, d.ctrl, lb,
+                                        d.nr_blocks, msm, tsm);
 }
 
 
@@ -320,11 +329,11 @@ int init_batch_t(const SlotDesc<S>* d, const BatchLaunch& bl, cudaStream_t st) {
 
 template <typename S, int NEXP, bool TAU>
 int nr_batch_t(const SlotDesc<S>* d, const BatchLaunch& bl, const BatchLaunch& bls,
-               cudaStream_t st) {
+               const NRParams& material, cudaStream_t st) {
   auto kern = k_nr_update_batch<S, S, NEXP, TAU>;
   const size_t smem = (size_t)kVoxelBlock * nr_smem_per_thread<S>(TAU);
   smem_optin(kern, smem);
-  kern<<<bl.blocks, kVoxelBlock, smem, st>>>(d, bl);
+  kern<<<bl.blocks, kVoxelBlock, smem, st>>>(d, bl, material);
   k_iter_finish_batch<S><<<bls.m, kFinishThreads, 0, st>>>(d, bls);
   return 2;
 }
@@ -353,12 +362,19 @@ int launch_init_batch(const SlotDesc<S>* d, const BatchLaunch& bl, int nexp, boo
 
 template <typename S>
 int launch_nr_update_batch(const SlotDesc<S>* d, const BatchLaunch& bl, const BatchLaunch& bls,
-                           int nexp, bool tau, cudaStream_t st) {
+                           const NRParams& material, int nexp, bool tau, cudaStream_t st) {
   if (bl.blocks <= 0) return 0;
+  const NRParams& m = material;
   switch (nexp) {
-    case 10: return tau ? nr_batch_t<S, 10, true>(d, bl, bls, st) : nr_batch_t<S, 10, false>(d, bl, bls, st);
-    case 20: return tau ? nr_batch_t<S, 20, true>(d, bl, bls, st) : nr_batch_t<S, 20, false>(d, bl, bls, st);
-    default: return tau ? nr_batch_t<S, 0, true>(d, bl, bls, st) : nr_batch_t<S, 0, false>(d, bl, bls, st);
+    case 10:
+      return tau ? nr_batch_t<S, 10, true>(d, bl, bls, m, st)
+                 : nr_batch_t<S, 10, false>(d, bl, bls, m, st);
+    case 20:
+      return tau ? nr_batch_t<S, 20, true>(d, bl, bls, m, st)
+                 : nr_batch_t<S, 20, false>(d, bl, bls, m, st);
+    default:
+      return tau ? nr_batch_t<S, 0, true>(d, bl, bls, m, st)
+                 : nr_batch_t<S, 0, false>(d, bl, bls, m, st);
   }
 }
 
@@ -369,9 +385,11 @@ template int launch_init_batch<double>(const SlotDesc<double>*, const BatchLaunc
 template int launch_init_batch<float>(const SlotDesc<float>*, const BatchLaunch&, int, bool,
                                       cudaStream_t);
 template int launch_nr_update_batch<double>(const SlotDesc<double>*, const BatchLaunch&,
-                                            const BatchLaunch&, int, bool, cudaStream_t);
+                                            const BatchLaunch&, const NRParams&, int, bool,
+                                            cudaStream_t);
 template int launch_nr_update_batch<float>(const SlotDesc<float>*, const BatchLaunch&,
-                                           const BatchLaunch&, int, bool, cudaStream_t);
+                                           const BatchLaunch&, const NRParams&, int, bool,
+                                           cudaStream_t);
 
 template <typename S>
 int launch_init(const NRParams& p, const FieldPtrs<S>& f, IterCtrl* ctrl, cudaStream_t st) {
@@ -416,7 +434,7 @@ __global__ void __launch_bounds__(kVoxelBlock, 3)
                  const double* crss, const double* lambda, const double* dtilde, double* out,
                  double* nr_err) {
   extern __shared__ __align__(16) unsigned char nr_smem[];
-  const int bs = blockDim.x;
+  constexpr int bs = kVoxelBlock;  // every launch of these kernels uses kVoxelBlock threads
   double* msm = reinterpret_cast<double*>(nr_smem) + threadIdx.x;
   double* tsm = msm + 60 * bs;
   const int v = blockIdx.x * bs + threadIdx.x;
@@ -432,7 +450,7 @@ __global__ void __launch_bounds__(kVoxelBlock, 3)
       lam[c] = lambda[v * 5 + c];
       ed[c] = p.edot[c] + dtilde[v * 5 + c];
     }
-    nr_constrained_smem<0, true>(msm, tsm, bs, p, lam, ed, s, &rel, &capped);
+    nr_constrained_smem<0, true>(msm, tsm, bs, p, ParamConsts{p}, lam, ed, s, &rel, &capped);
     if (nr_err) nr_err[v] = rel;
   } else {
     nr_unconstrained_smem<0, true>(msm, tsm, bs, p, p.edot, s, &capped);
