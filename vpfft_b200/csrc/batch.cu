@@ -151,6 +151,12 @@ struct vpfft_batch {
   // captured iteration chunk
   uint64_t iter_generation = 1, graph_generation = 0, eager_generation = 0;
   cudaGraphExec_t graph = nullptr;
+  // the FFT pass chains of different size classes run concurrently: forked
+  // from `stream` onto these streams and joined back before the NR sweep
+  static constexpr int kAux = 8;
+  cudaStream_t aux[kAux] = {};
+  cudaEvent_t ev_fork = nullptr;
+  cudaEvent_t ev_join[kAux] = {};
   std::string err;
 };
 
@@ -299,6 +305,8 @@ vpfft_status admit(vpfft_batch* b, std::vector<int>& admitted) {
     d.vox = voxel_params(g, a.r.edot);
     d.f = fields<S>(g);
     d.sp = spectral<S>(g, base, base + spec_al);
+    d.fs = FftSlot<S>{d.sp.nx,  d.sp.ny,  d.sp.nz,  d.sp.nh, d.sp.px.by_n, d.sp.py.by_n,
+                      d.sp.twx, d.sp.twy, d.sp.twz, d.sp.X,  d.sp.X2,      d.f.work};
     d.crss_out = (S*)g->crss;
     d.partials = g->partials;
     d.sum25 = b->d_sum25 + 25 * (size_t)a.slot;
@@ -337,30 +345,18 @@ vpfft_status start_loop(vpfft_batch* b, Active& a) {
 }
 
 // The iteration lists of the slots in ITER phase.
-// The RVEs of one pass that share a line engine.
-struct GroupList {
-  const void* set;
-  HostList list;
-  size_t smem_a = 0, smem_b = 0;
+// The iterating RVEs of one size class (the same line engines on all axes).
+struct ClassList {
+  const void* set_z;
+  const void* set_y;
+  const void* set_x;
+  HostList z, y, x;
+  size_t smem_z_r2c = 0, smem_z_c2r = 0, smem_y = 0, smem_x = 0;
 };
 struct IterLists {
-  std::vector<GroupList> z, y, x;
+  std::vector<ClassList> cls;
   HostList nr[2], fin[2];
 };
-
-void add_to_group(std::vector<GroupList>& gs, const void* set, int slot, int blocks,
-                  size_t smem_a, size_t smem_b) {
-  GroupList* g = nullptr;
-  for (GroupList& e : gs)
-    if (e.set == set) g = &e;
-  if (!g) {
-    gs.push_back(GroupList{set, HostList{}, 0, 0});
-    g = &gs.back();
-  }
-  g->list.add(slot, blocks);
-  g->smem_a = std::max(g->smem_a, smem_a);
-  g->smem_b = std::max(g->smem_b, smem_b);
-}
 
 template <typename S>
 void build_iter_lists(vpfft_batch* b, IterLists& L) {
@@ -368,30 +364,56 @@ void build_iter_lists(vpfft_batch* b, IterLists& L) {
     if (a.phase != kIter) continue;
     const SlotDesc<S>& d = *host_desc<S>(b, a.slot);
     const SpectralShape sh = spectral_shape<S>(d.sp, 5);
-    add_to_group(L.z, sh.set_z, a.slot, sh.blocks_z, sh.smem_z_r2c, sh.smem_z_c2r);
-    add_to_group(L.y, sh.set_y, a.slot, sh.blocks_y, sh.smem_y, 0);
-    add_to_group(L.x, sh.set_x, a.slot, sh.blocks_x, sh.smem_x, 0);
+    ClassList* c = nullptr;
+    for (ClassList& e : L.cls)
+      if (e.set_z == sh.set_z && e.set_y == sh.set_y && e.set_x == sh.set_x) c = &e;
+    if (!c) {
+      L.cls.push_back(ClassList{sh.set_z, sh.set_y, sh.set_x, {}, {}, {}});
+      c = &L.cls.back();
+    }
+    c->z.add(a.slot, sh.blocks_z);
+    c->y.add(a.slot, sh.blocks_y);
+    c->x.add(a.slot, sh.blocks_x);
+    c->smem_z_r2c = std::max(c->smem_z_r2c, sh.smem_z_r2c);
+    c->smem_z_c2r = std::max(c->smem_z_c2r, sh.smem_z_c2r);
+    c->smem_y = std::max(c->smem_y, sh.smem_y);
+    c->smem_x = std::max(c->smem_x, sh.smem_x);
     L.nr[a.tau].add(a.slot, d.nr_blocks);
     L.fin[a.tau].add(a.slot, 1);
   }
 }
 
-// lists: the z, y and x groups in order, then nr[0], nr[1], fin[0], fin[1]
+// lists: z, y, x of every class in order, then nr[0], nr[1], fin[0], fin[1]
 template <typename S>
 int enqueue_iterations(vpfft_batch* b, const std::vector<BatchLaunch>& bl, const IterLists& L,
                        int iters) {
-  std::vector<PassGroup> z, y, x;
+  std::vector<PassChain> chains;
   size_t k = 0;
-  for (const GroupList& g : L.z) z.push_back(PassGroup{g.set, bl[k++], g.smem_a, g.smem_b});
-  for (const GroupList& g : L.y) y.push_back(PassGroup{g.set, bl[k++], g.smem_a, g.smem_b});
-  for (const GroupList& g : L.x) x.push_back(PassGroup{g.set, bl[k++], g.smem_a, g.smem_b});
+  for (const ClassList& c : L.cls) {
+    chains.push_back(PassChain{c.set_z, c.set_y, c.set_x, bl[k], bl[k + 1], bl[k + 2],
+                               c.smem_z_r2c, c.smem_z_c2r, c.smem_y, c.smem_x});
+    k += 3;
+  }
   // material and solver constants: those of any iterating slot (a batch admits
   // only grids with its own material and options)
   const int any = !L.nr[0].slot.empty() ? L.nr[0].slot[0] : L.nr[1].slot[0];
   const NRParams& material = host_desc<S>(b, any)->nr;
+  const int nch = (int)chains.size();
+  const int naux = std::min(nch, vpfft_batch::kAux);
   int n = 0;
   for (int it = 0; it < iters; ++it) {
-    n += launch_spectral_batch<S>(dev_desc<S>(b), z, y, x, b->stream);
+    if (nch == 1) {
+      n += launch_spectral_chain<S>(dev_desc<S>(b), chains[0], b->stream);
+    } else {
+      cudaEventRecord(b->ev_fork, b->stream);
+      for (int a = 0; a < naux; ++a) cudaStreamWaitEvent(b->aux[a], b->ev_fork, 0);
+      for (int c = 0; c < nch; ++c)
+        n += launch_spectral_chain<S>(dev_desc<S>(b), chains[c], b->aux[c % naux]);
+      for (int a = 0; a < naux; ++a) {
+        cudaEventRecord(b->ev_join[a], b->aux[a]);
+        cudaStreamWaitEvent(b->stream, b->ev_join[a], 0);
+      }
+    }
     for (int t = 0; t < 2; ++t)
       n += launch_nr_update_batch<S>(dev_desc<S>(b), bl[k + t], bl[k + 2 + t], material, b->nexp,
                                      t == 1, b->stream);
@@ -407,7 +429,7 @@ template <typename S>
 vpfft_status run_iterations(vpfft_batch* b) {
   IterLists L;
   build_iter_lists<S>(b, L);
-  if (L.z.empty()) return VPFFT_OK;
+  if (L.cls.empty()) return VPFFT_OK;
   const int iters = std::max(1, b->bopt.iterations_per_tick);
   if (b->bopt.use_graphs && b->graph && b->graph_generation == b->iter_generation) {
     BCK(b, cudaGraphLaunch(b->graph, b->stream));
@@ -419,8 +441,8 @@ vpfft_status run_iterations(vpfft_batch* b) {
     b->graph = nullptr;
   }
   std::vector<HostList*> lists;
-  for (std::vector<GroupList>* gs : {&L.z, &L.y, &L.x})
-    for (GroupList& g : *gs) lists.push_back(&g.list);
+  for (ClassList& c : L.cls)
+    for (HostList* h : {&c.z, &c.y, &c.x}) lists.push_back(h);
   for (HostList* h : {&L.nr[0], &L.nr[1], &L.fin[0], &L.fin[1]}) lists.push_back(h);
   std::vector<BatchLaunch> bl;
   if (vpfft_status s = upload_lists(b, b->iter_lists, lists, bl)) return s;
@@ -571,6 +593,11 @@ void free_batch(vpfft_batch* b) {
   for (void* p : hptrs)
     if (p) cudaFreeHost(p);
   if (b->stream) cudaStreamDestroy(b->stream);
+  for (int a = 0; a < vpfft_batch::kAux; ++a) {
+    if (b->aux[a]) cudaStreamDestroy(b->aux[a]);
+    if (b->ev_join[a]) cudaEventDestroy(b->ev_join[a]);
+  }
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
 }
 
 }  // namespace
@@ -635,6 +662,14 @@ vpfft_status vpfft_batch_create(vpfft_precision precision, const vpfft_material*
   cudaError_t e;
   if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess)
     return bail(e, "stream");
+  for (int a = 0; a < vpfft_batch::kAux; ++a) {
+    if ((e = cudaStreamCreateWithFlags(&b->aux[a], cudaStreamNonBlocking)) != cudaSuccess)
+      return bail(e, "stream");
+    if ((e = cudaEventCreateWithFlags(&b->ev_join[a], cudaEventDisableTiming)) != cudaSuccess)
+      return bail(e, "event");
+  }
+  if ((e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming)) != cudaSuccess)
+    return bail(e, "event");
   if (b->bopt.hbm_budget_bytes > 0 &&
       (e = cudaMalloc(&b->arena_base, (size_t)b->bopt.hbm_budget_bytes)) != cudaSuccess)
     return bail(e, "arena");

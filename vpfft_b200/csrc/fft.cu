@@ -45,17 +45,18 @@ template <typename S>
 struct PassSmem {
   size_t z_r2c, z_c2r, y, x;
 };
+// Dynamic shared memory of the passes for tiles tz (real z-lines), ty
+// (y-lines) and tk (ky-lines per component).
 template <typename S>
-PassSmem<S> pass_smem(const Spectral<S>& sp, const PassSet<S>& Z, const PassSet<S>& Y,
-                      const PassSet<S>& X, int ncomp) {
+PassSmem<S> pass_smem(const Spectral<S>& sp, int tz, int ty, int tk, int ncomp) {
   using T = typename CX<S>::T;
   PassSmem<S> s;
   const size_t lz = line_stride(sp.nz);
-  const size_t zl = (size_t)(Z.tz / 2) * lz;  // packed z-lines of a tile
+  const size_t zl = (size_t)(tz / 2) * lz;  // packed z-lines of a tile
   s.z_r2c = sizeof(T) * (sp.nz + 2 * zl);
-  s.z_c2r = sizeof(T) * (sp.nz + zl + std::max(zl, (size_t)Z.tz * (sp.nh + 1)));
-  s.y = sizeof(T) * (sp.ny + 2 * (size_t)Y.ty * line_stride(sp.ny));
-  s.x = sizeof(T) * (sp.nx + 2 * (size_t)ncomp * X.tk * line_stride(sp.nx));
+  s.z_c2r = sizeof(T) * (sp.nz + zl + std::max(zl, (size_t)tz * (sp.nh + 1)));
+  s.y = sizeof(T) * (sp.ny + 2 * (size_t)ty * line_stride(sp.ny));
+  s.x = sizeof(T) * (sp.nx + 2 * (size_t)ncomp * tk * line_stride(sp.nx));
   return s;
 }
 
@@ -69,7 +70,7 @@ int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S
   const PassSet<S>& Z = pass_set<S>(sp.pz);
   const PassSet<S>& Y = pass_set<S>(sp.py);
   const PassSet<S>& X = pass_set<S>(sp.px);
-  const PassSmem<S> sm = pass_smem(sp, Z, Y, X, ncomp);
+  const PassSmem<S> sm = pass_smem(sp, Z.tz, Y.ty, X.tk, ncomp);
   T* A = reinterpret_cast<T*>(sp.X);
   T* B = reinterpret_cast<T*>(sp.X2);
   const T* twx = reinterpret_cast<const T*>(sp.twx);
@@ -102,7 +103,7 @@ int launch_fft3d(const Spectral<S>& sp, S* real, int ncomp, int mode, cudaStream
   const PassSet<S>& Z = pass_set<S>(sp.pz);
   const PassSet<S>& Y = pass_set<S>(sp.py);
   const PassSet<S>& X = pass_set<S>(sp.px);
-  const PassSmem<S> sm = pass_smem(sp, Z, Y, X, ncomp);
+  const PassSmem<S> sm = pass_smem(sp, Z.tz, Y.ty, X.tk, ncomp);
   T* A = reinterpret_cast<T*>(sp.X);
   T* B = reinterpret_cast<T*>(sp.X2);
   const T* twx = reinterpret_cast<const T*>(sp.twx);
@@ -134,11 +135,11 @@ SpectralShape spectral_shape(const Spectral<S>& sp, int ncomp) {
   const PassSet<S>& Z = pass_set<S>(sp.pz);
   const PassSet<S>& Y = pass_set<S>(sp.py);
   const PassSet<S>& X = pass_set<S>(sp.px);
-  const PassSmem<S> sm = pass_smem(sp, Z, Y, X, ncomp);
+  const PassSmem<S> sm = pass_smem(sp, Z.btz, Y.bty, X.btk, ncomp);
   SpectralShape r;
-  r.blocks_z = cdiv(sp.nx * sp.ny, Z.tz) * ncomp;
-  r.blocks_y = cdiv(sp.nh * sp.nx, Y.ty) * ncomp;
-  r.blocks_x = cdiv(sp.nh * sp.ny, X.tk);
+  r.blocks_z = cdiv(sp.nx * sp.ny, Z.btz) * ncomp;
+  r.blocks_y = cdiv(sp.nh * sp.nx, Y.bty) * ncomp;
+  r.blocks_x = cdiv(sp.nh * sp.ny, X.btk);
   r.smem_z_r2c = sm.z_r2c;
   r.smem_z_c2r = sm.z_c2r;
   r.smem_y = sm.y;
@@ -150,47 +151,24 @@ SpectralShape spectral_shape(const Spectral<S>& sp, int ncomp) {
 }
 
 template <typename S>
-int launch_spectral_batch(const SlotDesc<S>* d, const std::vector<PassGroup>& z,
-                          const std::vector<PassGroup>& y, const std::vector<PassGroup>& x,
-                          cudaStream_t st) {
-  int n = 0;
-  auto set = [](const PassGroup& g) { return static_cast<const PassSet<S>*>(g.set); };
-  for (const PassGroup& g : z)
-    if (g.bl.blocks > 0) {
-      set(g)->bz_r2c<<<g.bl.blocks, set(g)->threads, g.smem_a, st>>>(d, g.bl);
-      ++n;
-    }
-  for (const PassGroup& g : y)
-    if (g.bl.blocks > 0) {
-      set(g)->by_fwd<<<g.bl.blocks, set(g)->threads, g.smem_a, st>>>(d, g.bl);
-      ++n;
-    }
-  for (const PassGroup& g : x)
-    if (g.bl.blocks > 0) {
-      set(g)->bx_green<<<g.bl.blocks, set(g)->threads_x, g.smem_a, st>>>(d, g.bl);
-      ++n;
-    }
-  for (const PassGroup& g : y)
-    if (g.bl.blocks > 0) {
-      set(g)->by_inv<<<g.bl.blocks, set(g)->threads, g.smem_a, st>>>(d, g.bl);
-      ++n;
-    }
-  for (const PassGroup& g : z)
-    if (g.bl.blocks > 0) {
-      set(g)->bz_c2r<<<g.bl.blocks, set(g)->threads, g.smem_b, st>>>(d, g.bl);
-      ++n;
-    }
-  return n;
+int launch_spectral_chain(const SlotDesc<S>* d, const PassChain& c, cudaStream_t st) {
+  if (c.z.blocks <= 0) return 0;
+  const PassSet<S>* Z = static_cast<const PassSet<S>*>(c.set_z);
+  const PassSet<S>* Y = static_cast<const PassSet<S>*>(c.set_y);
+  const PassSet<S>* X = static_cast<const PassSet<S>*>(c.set_x);
+  Z->bz_r2c<<<c.z.blocks, Z->threads, c.smem_z_r2c, st>>>(d, c.z);
+  Y->by_fwd<<<c.y.blocks, Y->threads, c.smem_y, st>>>(d, c.y);
+  X->bx_green<<<c.x.blocks, X->threads_x, c.smem_x, st>>>(d, c.x);
+  Y->by_inv<<<c.y.blocks, Y->threads, c.smem_y, st>>>(d, c.y);
+  Z->bz_c2r<<<c.z.blocks, Z->threads, c.smem_z_c2r, st>>>(d, c.z);
+  return 5;
 }
 
 template SpectralShape spectral_shape<double>(const Spectral<double>&, int);
 template SpectralShape spectral_shape<float>(const Spectral<float>&, int);
-template int launch_spectral_batch<double>(const SlotDesc<double>*, const std::vector<PassGroup>&,
-                                           const std::vector<PassGroup>&,
-                                           const std::vector<PassGroup>&, cudaStream_t);
-template int launch_spectral_batch<float>(const SlotDesc<float>*, const std::vector<PassGroup>&,
-                                          const std::vector<PassGroup>&,
-                                          const std::vector<PassGroup>&, cudaStream_t);
+template int launch_spectral_chain<double>(const SlotDesc<double>*, const PassChain&,
+                                           cudaStream_t);
+template int launch_spectral_chain<float>(const SlotDesc<float>*, const PassChain&, cudaStream_t);
 template int launch_spectral_iteration<double>(const Spectral<double>&, const GreenParams<double>&,
                                                double*, const IterCtrl*, cudaStream_t, int,
                                                cudaEvent_t*);

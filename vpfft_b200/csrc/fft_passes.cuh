@@ -32,15 +32,16 @@ namespace fft {
 
 // Lines per block and threads per block of an engine.  Fixed engines of
 // length >= 64 hold about 2048 (FP32) or 1024 (FP64) complex values per
-// ping-pong buffer; shorter lines take 512 so that a small grid still spreads
-// over many blocks.  The z and y passes run 256 (FP32) or 128 (FP64) threads
+// ping-pong buffer; shorter lines take 512 so that a small single grid still
+// spreads over many blocks.  The z and y passes run 256 (FP32) or 128 (FP64) threads
 // per block, the x pass (two transforms and the Green operator) 128 threads,
 // the settings measured fastest at 256^3.  The generic engine keeps 256
 // threads and its short tiles.
-template <typename S, class E>
+// A batch always takes the long tiles: its launches have blocks enough.
+template <typename S, class E, bool kBatch = false>
 struct Tiles {
   static constexpr bool kF32 = sizeof(S) == 4;
-  static constexpr int kElems = E::kN >= 64 ? (kF32 ? 2048 : 1024) : 512;
+  static constexpr int kElems = (E::kN >= 64 || kBatch) ? (kF32 ? 2048 : 1024) : 512;
   static constexpr int kThreads = E::kN ? (kF32 ? 256 : 128) : 256;  // z and y passes
   static constexpr int kThreadsX = E::kN ? 128 : 256;                // x pass
   static constexpr int cmax(int a, int b) { return a > b ? a : b; }
@@ -100,14 +101,14 @@ __device__ __forceinline__ void copy_short_rows(int nrows, G get, P put) {
 
 // ---------------------------------------------------------------- z, forward
 // Tile bt of component c: real lines f = bt TZ ... (f = x ny + y).
-template <typename S, class E>
+template <typename S, class E, class TL>
 __device__ __forceinline__ void pass_z_r2c_body(const S* __restrict__ W,
                                                 typename CX<S>::T* __restrict__ A,
                                                 const LinePlan& pl, const FastDiv& dny,
                                                 const typename CX<S>::T* __restrict__ twg, int nx,
                                                 int ny, int nh, int bt, int c) {
   using T = typename CX<S>::T;
-  constexpr int TZ = Tiles<S, E>::kZ;
+  constexpr int TZ = TL::kZ;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nz = E::n(pl), ls = line_stride(nz);
   T* tw = reinterpret_cast<T*>(smraw);
@@ -151,14 +152,14 @@ __device__ __forceinline__ void pass_z_r2c_body(const S* __restrict__ W,
 }
 
 // ---------------------------------------------------------------- z, inverse
-template <typename S, class E>
+template <typename S, class E, class TL>
 __device__ __forceinline__ void pass_z_c2r_body(const typename CX<S>::T* __restrict__ A,
                                                 S* __restrict__ W, const LinePlan& pl,
                                                 const FastDiv& dny,
                                                 const typename CX<S>::T* __restrict__ twg, int nx,
                                                 int ny, int nh, S scale, int bt, int c) {
   using T = typename CX<S>::T;
-  constexpr int TZ = Tiles<S, E>::kZ;
+  constexpr int TZ = TL::kZ;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nz = E::n(pl), ls = line_stride(nz);
   // a: (TZ/2) packed lines; b: the tile's half spectra first (TZ x (nh+1)),
@@ -215,14 +216,14 @@ __device__ __forceinline__ void pass_z_c2r_body(const typename CX<S>::T* __restr
 // ---------------------------------------------------------------- y passes
 // Lines g = kz nx + x of component c.  Forward: A[c][x][kz][y] ->
 // B[c][kz][ky][x]; inverse: B -> A.
-template <int SIGN, typename S, class E>
+template <int SIGN, typename S, class E, class TL>
 __device__ __forceinline__ void pass_y_body(const typename CX<S>::T* __restrict__ in,
                                             typename CX<S>::T* __restrict__ out,
                                             const LinePlan& pl, const FastDiv& dnx,
                                             const typename CX<S>::T* __restrict__ twg, int nx,
                                             int nh, int bt, int c) {
   using T = typename CX<S>::T;
-  constexpr int TY = Tiles<S, E>::kY;
+  constexpr int TY = TL::kY;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int ny = E::n(pl), ls = line_stride(ny);
   T* tw = reinterpret_cast<T*>(smraw);
@@ -273,14 +274,14 @@ __device__ __forceinline__ void pass_y_body(const typename CX<S>::T* __restrict_
 // ---------------------------------------------------------------- x pass
 // In place on B[c][kz][ky][x], lines f = kz ny + ky of all ncomp components:
 // MODE 0 forward, 1 inverse, 2 forward + Green + inverse.
-template <int MODE, typename S, class E>
+template <int MODE, typename S, class E, class TL>
 __device__ __forceinline__ void pass_x_body(typename CX<S>::T* __restrict__ B, const LinePlan& pl,
                                             const FastDiv& dny,
                                             const typename CX<S>::T* __restrict__ twg,
                                             const GreenParams<S>& gp, int ny, int nh, int ncomp,
                                             int bt) {
   using T = typename CX<S>::T;
-  constexpr int TK = Tiles<S, E>::kX;
+  constexpr int TK = TL::kX;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nx = E::n(pl), ls = line_stride(nx);
   T* tw = reinterpret_cast<T*>(smraw);
@@ -342,7 +343,7 @@ __global__ void __launch_bounds__(Tiles<S, E>::kThreads)
                  FastDiv dny, const typename CX<S>::T* __restrict__ twg, int nx, int ny, int nh,
                  const IterCtrl* ctrl) {
   if (ctrl && ctrl->done) return;
-  pass_z_r2c_body<S, E>(W, A, pl, dny, twg, nx, ny, nh, blockIdx.x, blockIdx.y);
+  pass_z_r2c_body<S, E, Tiles<S, E>>(W, A, pl, dny, twg, nx, ny, nh, blockIdx.x, blockIdx.y);
 }
 template <typename S, class E>
 __global__ void __launch_bounds__(Tiles<S, E>::kThreads)
@@ -350,7 +351,8 @@ __global__ void __launch_bounds__(Tiles<S, E>::kThreads)
                  FastDiv dny, const typename CX<S>::T* __restrict__ twg, int nx, int ny, int nh,
                  S scale, const IterCtrl* ctrl) {
   if (ctrl && ctrl->done) return;
-  pass_z_c2r_body<S, E>(A, W, pl, dny, twg, nx, ny, nh, scale, blockIdx.x, blockIdx.y);
+  pass_z_c2r_body<S, E, Tiles<S, E>>(A, W, pl, dny, twg, nx, ny, nh, scale, blockIdx.x,
+                                     blockIdx.y);
 }
 template <int SIGN, typename S, class E>
 __global__ void __launch_bounds__(Tiles<S, E>::kThreads)
@@ -358,7 +360,7 @@ __global__ void __launch_bounds__(Tiles<S, E>::kThreads)
              LinePlan pl, FastDiv dnx, const typename CX<S>::T* __restrict__ twg, int nx, int nh,
              const IterCtrl* ctrl) {
   if (ctrl && ctrl->done) return;
-  pass_y_body<SIGN, S, E>(in, out, pl, dnx, twg, nx, nh, blockIdx.x, blockIdx.y);
+  pass_y_body<SIGN, S, E, Tiles<S, E>>(in, out, pl, dnx, twg, nx, nh, blockIdx.x, blockIdx.y);
 }
 template <int MODE, typename S, class E>
 __global__ void __launch_bounds__(Tiles<S, E>::kThreadsX, 512 / Tiles<S, E>::kThreadsX)
@@ -366,85 +368,93 @@ __global__ void __launch_bounds__(Tiles<S, E>::kThreadsX, 512 / Tiles<S, E>::kTh
              const typename CX<S>::T* __restrict__ twg, GreenParams<S> gp, int ny, int nh,
              int ncomp, const IterCtrl* ctrl) {
   if (ctrl && ctrl->done) return;
-  pass_x_body<MODE, S, E>(B, pl, dny, twg, gp, ny, nh, ncomp, blockIdx.x);
+  pass_x_body<MODE, S, E, Tiles<S, E>>(B, pl, dny, twg, gp, ny, nh, ncomp, blockIdx.x);
 }
 
 // Batched passes of the fixed-point iteration (5 components): block -> slot,
-// then the slot's tile from the local block index.
+// then the slot's tile from the local block index.  A block copies the slot's
+// FFT fields (FftSlot, and the Green constants for the x pass) to shared
+// memory; the runtime line plan of the generic engine is read in place.
 template <typename S>
-struct SlotSpectral {
-  Spectral<S> sp;
+struct SlotFft {
+  FftSlot<S> fs;
   GreenParams<S> gp;
 };
 template <typename S>
 __device__ __forceinline__ const SlotDesc<S>* batch_pass_setup(const SlotDesc<S>* desc,
                                                                const BatchLaunch& bl, bool green,
-                                                               SlotSpectral<S>* sm, int* lb) {
+                                                               SlotFft<S>* sm, int* lb) {
   const SlotDesc<S>* d = &desc[batch_slot(bl, blockIdx.x, lb)];
   if (d->ctrl->done) return nullptr;
-  copy_struct(&sm->sp, &d->sp);
+  copy_struct(&sm->fs, &d->fs);
   if (green) copy_struct(&sm->gp, &d->gp);
   __syncthreads();
   return d;
 }
 
 template <typename S, class E>
-__global__ void __launch_bounds__(Tiles<S, E>::kThreads)
+__global__ void __launch_bounds__(Tiles<S, E, true>::kThreads)
     k_pass_z_r2c_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
   using T = typename CX<S>::T;
-  __shared__ SlotSpectral<S> sm;
+  using TL = Tiles<S, E, true>;
+  __shared__ SlotFft<S> sm;
   int lb;
   const SlotDesc<S>* d = batch_pass_setup(desc, bl, false, &sm, &lb);
   if (!d) return;
-  const Spectral<S>& sp = sm.sp;
-  const int gt = (sp.nx * sp.ny + Tiles<S, E>::kZ - 1) / Tiles<S, E>::kZ;
+  const FftSlot<S>& fs = sm.fs;
+  const int gt = (fs.nx * fs.ny + TL::kZ - 1) / TL::kZ;
   const int c = lb / gt;
-  pass_z_r2c_body<S, E>(d->f.work, reinterpret_cast<T*>(sp.X), sp.pz, sp.py.by_n,
-                        reinterpret_cast<const T*>(sp.twz), sp.nx, sp.ny, sp.nh, lb - c * gt, c);
+  pass_z_r2c_body<S, E, TL>(fs.work, reinterpret_cast<T*>(fs.X), d->sp.pz, fs.dny,
+                            reinterpret_cast<const T*>(fs.twz), fs.nx, fs.ny, fs.nh, lb - c * gt,
+                            c);
 }
 template <typename S, class E>
-__global__ void __launch_bounds__(Tiles<S, E>::kThreads)
+__global__ void __launch_bounds__(Tiles<S, E, true>::kThreads)
     k_pass_z_c2r_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
   using T = typename CX<S>::T;
-  __shared__ SlotSpectral<S> sm;
+  using TL = Tiles<S, E, true>;
+  __shared__ SlotFft<S> sm;
   int lb;
   const SlotDesc<S>* d = batch_pass_setup(desc, bl, false, &sm, &lb);
   if (!d) return;
-  const Spectral<S>& sp = sm.sp;
-  const int gt = (sp.nx * sp.ny + Tiles<S, E>::kZ - 1) / Tiles<S, E>::kZ;
+  const FftSlot<S>& fs = sm.fs;
+  const int gt = (fs.nx * fs.ny + TL::kZ - 1) / TL::kZ;
   const int c = lb / gt;
-  const S scale = S(1.0 / ((double)sp.nx * sp.ny * sp.nz));
-  pass_z_c2r_body<S, E>(reinterpret_cast<const T*>(sp.X), d->f.work, sp.pz, sp.py.by_n,
-                        reinterpret_cast<const T*>(sp.twz), sp.nx, sp.ny, sp.nh, scale,
-                        lb - c * gt, c);
+  const S scale = S(1.0 / ((double)fs.nx * fs.ny * fs.nz));
+  pass_z_c2r_body<S, E, TL>(reinterpret_cast<const T*>(fs.X), fs.work, d->sp.pz, fs.dny,
+                            reinterpret_cast<const T*>(fs.twz), fs.nx, fs.ny, fs.nh, scale,
+                            lb - c * gt, c);
 }
 template <int SIGN, typename S, class E>
-__global__ void __launch_bounds__(Tiles<S, E>::kThreads)
+__global__ void __launch_bounds__(Tiles<S, E, true>::kThreads)
     k_pass_y_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
   using T = typename CX<S>::T;
-  __shared__ SlotSpectral<S> sm;
+  using TL = Tiles<S, E, true>;
+  __shared__ SlotFft<S> sm;
   int lb;
   const SlotDesc<S>* d = batch_pass_setup(desc, bl, false, &sm, &lb);
   if (!d) return;
-  const Spectral<S>& sp = sm.sp;
-  const int gt = (sp.nh * sp.nx + Tiles<S, E>::kY - 1) / Tiles<S, E>::kY;
+  const FftSlot<S>& fs = sm.fs;
+  const int gt = (fs.nh * fs.nx + TL::kY - 1) / TL::kY;
   const int c = lb / gt;
-  const T* in = reinterpret_cast<const T*>(SIGN < 0 ? sp.X : sp.X2);
-  T* out = reinterpret_cast<T*>(SIGN < 0 ? sp.X2 : sp.X);
-  pass_y_body<SIGN, S, E>(in, out, sp.py, sp.px.by_n, reinterpret_cast<const T*>(sp.twy), sp.nx,
-                          sp.nh, lb - c * gt, c);
+  const T* in = reinterpret_cast<const T*>(SIGN < 0 ? fs.X : fs.X2);
+  T* out = reinterpret_cast<T*>(SIGN < 0 ? fs.X2 : fs.X);
+  pass_y_body<SIGN, S, E, TL>(in, out, d->sp.py, fs.dnx, reinterpret_cast<const T*>(fs.twy),
+                              fs.nx, fs.nh, lb - c * gt, c);
 }
 template <typename S, class E>
-__global__ void __launch_bounds__(Tiles<S, E>::kThreadsX, 512 / Tiles<S, E>::kThreadsX)
+__global__ void __launch_bounds__(Tiles<S, E, true>::kThreadsX,
+                                  512 / Tiles<S, E, true>::kThreadsX)
     k_pass_x_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
   using T = typename CX<S>::T;
-  __shared__ SlotSpectral<S> sm;
+  using TL = Tiles<S, E, true>;
+  __shared__ SlotFft<S> sm;
   int lb;
   const SlotDesc<S>* d = batch_pass_setup(desc, bl, true, &sm, &lb);
   if (!d) return;
-  const Spectral<S>& sp = sm.sp;
-  pass_x_body<2, S, E>(reinterpret_cast<T*>(sp.X2), sp.px, sp.py.by_n,
-                       reinterpret_cast<const T*>(sp.twx), sm.gp, sp.ny, sp.nh, 5, lb);
+  const FftSlot<S>& fs = sm.fs;
+  pass_x_body<2, S, E, TL>(reinterpret_cast<T*>(fs.X2), d->sp.px, fs.dny,
+                           reinterpret_cast<const T*>(fs.twx), sm.gp, fs.ny, fs.nh, 5, lb);
 }
 
 // ---------------------------------------------------------------- entry table
@@ -452,7 +462,8 @@ template <typename S>
 struct PassSet {
   using T = typename CX<S>::T;
   int threads, threads_x;  // z and y passes, x pass
-  int tz, ty, tk;  // real z-lines, y-lines and ky-lines (per component) per block
+  int tz, ty, tk;     // real z-lines, y-lines and ky-lines (per component) per block
+  int btz, bty, btk;  // the same for the batched kernels
   void (*z_r2c)(const S*, T*, LinePlan, FastDiv, const T*, int, int, int, const IterCtrl*);
   void (*z_c2r)(const T*, S*, LinePlan, FastDiv, const T*, int, int, int, S, const IterCtrl*);
   void (*y_fwd)(const T*, T*, LinePlan, FastDiv, const T*, int, int, const IterCtrl*);
@@ -486,6 +497,12 @@ PassSet<S> make_pass_set() {
   p.tz = Ti::kZ;
   p.ty = Ti::kY;
   p.tk = Ti::kX;
+  p.btz = Tiles<S, E, true>::kZ;
+  p.bty = Tiles<S, E, true>::kY;
+  p.btk = Tiles<S, E, true>::kX;
+  static_assert(Tiles<S, E, true>::kThreads == Ti::kThreads &&
+                    Tiles<S, E, true>::kThreadsX == Ti::kThreadsX,
+                "batched and single kernels share the thread counts");
   p.z_r2c = k_pass_z_r2c<S, E>;
   p.z_c2r = k_pass_z_c2r<S, E>;
   p.y_fwd = k_pass_y<-1, S, E>;

@@ -151,6 +151,20 @@ template <typename S>
 int launch_fft3d(const Spectral<S>& sp, S* real, int ncomp, int mode, cudaStream_t st);
 
 // --- batches of RVEs ---------------------------------------------------------
+// The fields of an RVE that the batched FFT passes read (each block copies them
+// to shared memory).
+template <typename S>
+struct FftSlot {
+  int nx, ny, nz, nh;
+  FastDiv dnx, dny;  // division by nx and ny
+  const void* twx;
+  const void* twy;
+  const void* twz;
+  void* X;
+  void* X2;
+  S* work;
+};
+
 // One RVE ("slot") of a batch: everything a batched kernel needs, resident in
 // device memory so that one launch per phase serves RVEs of different sizes.
 template <typename S>
@@ -161,6 +175,7 @@ struct SlotDesc {
   PostParams post;       // texture and hardening update
   GreenParams<S> gp;
   Spectral<S> sp;
+  FftSlot<S> fs;         // copy of the fields of sp (and f.work) the batched passes use
   FieldPtrs<S> f;
   S* crss_out;           // per-voxel CRSS written by the post kernel
   double* partials;      // block partial sums (reference medium, loop reductions)
@@ -200,7 +215,7 @@ int launch_ref_medium_batch(const SlotDesc<S>* d, const BatchLaunch& bl,
 template <typename S>
 int launch_post_batch(const SlotDesc<S>* d, const BatchLaunch& bl, cudaStream_t st);
 // Blocks, dynamic shared memory and line engine ("pass set", chosen by the
-// axis length) of the five FFT passes of one RVE.
+// axis length) of the five batched FFT passes of one RVE.
 struct SpectralShape {
   int blocks_z, blocks_y, blocks_x;
   size_t smem_z_r2c, smem_z_c2r, smem_y, smem_x;
@@ -210,20 +225,18 @@ struct SpectralShape {
 };
 template <typename S>
 SpectralShape spectral_shape(const Spectral<S>& sp, int ncomp);
-// The RVEs of one batched pass that share a line engine: their blocks and the
-// largest dynamic shared memory among them (smem_a: r2c / forward / x pass,
-// smem_b: c2r).
-struct PassGroup {
-  const void* set;
-  BatchLaunch bl;
-  size_t smem_a, smem_b;
+// The RVEs of a batch whose three axes have the same line engines: one launch
+// per pass over all of them (the largest shared memory among them).  Chains
+// of different classes are independent and may run on different streams.
+struct PassChain {
+  const void* set_z;
+  const void* set_y;
+  const void* set_x;
+  BatchLaunch z, y, x;
+  size_t smem_z_r2c, smem_z_c2r, smem_y, smem_x;
 };
-// The five passes of one iteration over a batch, one launch per pass and
-// engine group.
 template <typename S>
-int launch_spectral_batch(const SlotDesc<S>* d, const std::vector<PassGroup>& z,
-                          const std::vector<PassGroup>& y, const std::vector<PassGroup>& x,
-                          cudaStream_t st);
+int launch_spectral_chain(const SlotDesc<S>* d, const PassChain& c, cudaStream_t st);
 
 // --- batched solver entry points for testing (double, voxel-major) ---------
 int launch_solvers_constrained(int n, const double* s0, const double* schmid, const double* crss,
