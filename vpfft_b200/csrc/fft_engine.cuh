@@ -14,11 +14,12 @@
 //                       padded offset is a compile-time constant and each
 //                       thread holds a whole radix-16 butterfly in registers.
 //
-// Both engines use the same twiddle table tw[i] = exp(-2 pi i i / n) (i in
-// [0, n)) and give the unnormalised DFT with exponent sign SIGN.  Everything
-// here is __host__ __device__ so that a host build can run a block's work
-// sequentially (thread 0 of a 1-thread block) and check it against a direct
-// DFT.
+// Both engines start from the twiddle table exp(-2 pi i i / n) (i in [0, n)),
+// which load_tw stages in shared memory (the fixed engine as per-stage tables
+// read without bank conflicts), and give the unnormalised DFT with exponent
+// sign SIGN.  Everything here is __host__ __device__ so that a host build can
+// run a block's work sequentially (thread 0 of a 1-thread block) and check it
+// against a direct DFT.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -255,6 +256,11 @@ template <bool B16>
 struct GenericEngine {
   static constexpr int kN = 0;
   VPFFT_HD static int n(const LinePlan& p) { return p.n; }
+  // shared-memory twiddles: the table itself (n entries)
+  template <typename T>
+  VPFFT_HD static void load_tw(T* tw, const T* twg, int n, int tid, int nthr) {
+    for (int i = tid; i < n; i += nthr) tw[i] = twg[i];
+  }
   VPFFT_HD static int div_n(int i, const LinePlan& p) { return (int)fast_div((uint32_t)i, p.by_n); }
   // B16: whether the plan may contain a radix-16 stage (kernels without it
   // keep a smaller register footprint for lines that never use one).
@@ -305,11 +311,12 @@ template <> struct FixedPlan<256> { using type = Radices<16, 16>; };
 template <> struct FixedPlan<384> { using type = Radices<16, 12, 2>; };
 template <> struct FixedPlan<512> { using type = Radices<16, 16, 2>; };
 
-// The same stage with every size a compile-time constant.
+// The same stage with every size a compile-time constant.  tws: the stage's
+// own twiddles, tws[(r - 1) NS + j mod NS] = W_N^(r (j mod NS) N / (NS RADIX)),
+// so that the threads of a warp (consecutive j) read consecutive entries.
 template <int N, int RADIX, int NS, int SIGN, typename T>
-VPFFT_HD void fixed_stage(const T* a, T* b, const T* tw, int nlines, int ls, int tid, int nthr) {
+VPFFT_HD void fixed_stage(const T* a, T* b, const T* tws, int nlines, int ls, int tid, int nthr) {
   constexpr int NB = N / RADIX;
-  constexpr int TWS = N / (NS * RADIX);
   static_assert(N % (NS * RADIX) == 0, "plan does not divide N");
   const int total = NB * nlines;
   for (int t = tid; t < total; t += nthr) {
@@ -325,10 +332,9 @@ VPFFT_HD void fixed_stage(const T* a, T* b, const T* tw, int nlines, int ls, int
       v[r] = in[sw(j + r * NB)];
     });
     if constexpr (NS > 1) {
-      const int e = jm * TWS;
       static_for<1, RADIX>([&](auto rc) {
         constexpr int r = decltype(rc)::value;
-        v[r] = tw_mul<SIGN>(v[r], tw[r * e]);
+        v[r] = tw_mul<SIGN>(v[r], tws[(r - 1) * NS + jm]);
       });
     }
     dft<RADIX, SIGN>(v);
@@ -339,16 +345,40 @@ VPFFT_HD void fixed_stage(const T* a, T* b, const T* tw, int nlines, int ls, int
   }
 }
 
-template <int N, int SIGN, int NS, typename T>
+// Offset of the next stage's twiddles: stages with a span NS > 1 keep
+// (R - 1) NS entries (at most N in all).
+template <int NS, int R>
+constexpr int stage_tw_size() {
+  return NS > 1 ? (R - 1) * NS : 0;
+}
+
+template <int N, int SIGN, int NS, int OFF, typename T>
 VPFFT_HD T* fixed_stages(T* a, T*, const T*, int, int, int, int, Radices<>) {
   return a;
 }
-template <int N, int SIGN, int NS, typename T, int R, int... Rest>
+template <int N, int SIGN, int NS, int OFF, typename T, int R, int... Rest>
 VPFFT_HD T* fixed_stages(T* a, T* b, const T* tw, int nlines, int ls, int tid, int nthr,
                          Radices<R, Rest...>) {
-  fixed_stage<N, R, NS, SIGN>(a, b, tw, nlines, ls, tid, nthr);
+  fixed_stage<N, R, NS, SIGN>(a, b, tw + OFF, nlines, ls, tid, nthr);
   block_sync();
-  return fixed_stages<N, SIGN, NS * R>(b, a, tw, nlines, ls, tid, nthr, Radices<Rest...>{});
+  return fixed_stages<N, SIGN, NS * R, OFF + stage_tw_size<NS, R>()>(b, a, tw, nlines, ls, tid,
+                                                                    nthr, Radices<Rest...>{});
+}
+
+// The stage twiddle tables from the table twg[i] = exp(-2 pi i i / N).
+template <int N, int NS, int OFF, typename T>
+VPFFT_HD void fixed_tw_build(T*, const T*, int, int, Radices<>) {}
+template <int N, int NS, int OFF, typename T, int R, int... Rest>
+VPFFT_HD void fixed_tw_build(T* tw, const T* twg, int tid, int nthr, Radices<R, Rest...>) {
+  if constexpr (NS > 1) {
+    constexpr int TWS = N / (NS * R);
+    for (int i = tid; i < (R - 1) * NS; i += nthr) {
+      const int r = i / NS + 1, jm = i - (r - 1) * NS;
+      tw[OFF + i] = twg[r * jm * TWS];
+    }
+  }
+  fixed_tw_build<N, NS * R, OFF + stage_tw_size<NS, R>()>(tw, twg, tid, nthr,
+                                                          Radices<Rest...>{});
 }
 
 template <int N>
@@ -356,10 +386,16 @@ struct FixedEngine {
   static constexpr int kN = N;
   VPFFT_HD static constexpr int n(const LinePlan&) { return N; }
   VPFFT_HD static int div_n(int i, const LinePlan&) { return i / N; }
+  // shared-memory twiddles: the per-stage tables (at most N entries)
+  template <typename T>
+  VPFFT_HD static void load_tw(T* tw, const T* twg, int, int tid, int nthr) {
+    fixed_tw_build<N, 1, 0>(tw, twg, tid, nthr, typename FixedPlan<N>::type{});
+  }
   template <int SIGN, typename T>
   VPFFT_HD static T* fft(T* a, T* b, const T* tw, const LinePlan&, int nlines, int ls, int tid,
                          int nthr) {
-    return fixed_stages<N, SIGN, 1>(a, b, tw, nlines, ls, tid, nthr, typename FixedPlan<N>::type{});
+    return fixed_stages<N, SIGN, 1, 0>(a, b, tw, nlines, ls, tid, nthr,
+                                       typename FixedPlan<N>::type{});
   }
 };
 

@@ -50,10 +50,6 @@ struct Tiles {
   static constexpr int kX = E::kN ? cmax(1, kElems / (5 * E::kN)) : (sizeof(S) == 4 ? 4 : 2);
 };
 
-template <typename T>
-__device__ __forceinline__ void load_twiddles(T* tw, const T* twg, int n) {
-  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = twg[i];
-}
 
 // Copy of nrows rows of len elements: warp w takes rows w, w + nwarps, ...;
 // lanes stride 32 along the row with kU independent loads in flight per lane
@@ -114,7 +110,7 @@ __device__ __forceinline__ void pass_z_r2c_body(const S* __restrict__ W,
   T* tw = reinterpret_cast<T*>(smraw);
   T* a = tw + nz;
   T* b = a + (TZ / 2) * ls;
-  load_twiddles(tw, twg, nz);
+  E::load_tw(tw, twg, nz, threadIdx.x, blockDim.x);
   const int nxy = nx * ny;
   const int f0 = bt * TZ;
   const int nf = min(TZ, nxy - f0);
@@ -167,7 +163,7 @@ __device__ __forceinline__ void pass_z_c2r_body(const typename CX<S>::T* __restr
   T* tw = reinterpret_cast<T*>(smraw);
   T* a = tw + nz;
   T* b = a + (TZ / 2) * ls;
-  load_twiddles(tw, twg, nz);
+  E::load_tw(tw, twg, nz, threadIdx.x, blockDim.x);
   const int nxy = nx * ny;
   const int f0 = bt * TZ;
   const int nf = min(TZ, nxy - f0);
@@ -229,7 +225,7 @@ __device__ __forceinline__ void pass_y_body(const typename CX<S>::T* __restrict_
   T* tw = reinterpret_cast<T*>(smraw);
   T* a = tw + ny;
   T* b = a + TY * ls;
-  load_twiddles(tw, twg, ny);
+  E::load_tw(tw, twg, ny, threadIdx.x, blockDim.x);
   const int g0 = bt * TY;
   const int ng = min(TY, nh * nx - g0);
   // component base (offsets inside a component are < 2^31 for dimensions <= 512)
@@ -287,7 +283,7 @@ __device__ __forceinline__ void pass_x_body(typename CX<S>::T* __restrict__ B, c
   T* tw = reinterpret_cast<T*>(smraw);
   T* a = tw + nx;
   T* b = a + ncomp * TK * ls;
-  load_twiddles(tw, twg, nx);
+  E::load_tw(tw, twg, nx, threadIdx.x, blockDim.x);
   const int f0 = bt * TK;
   const int nfk = min(TK, nh * ny - f0);
   // component stride and the block's offset: < 2^31 for dimensions <= 512
