@@ -18,6 +18,8 @@
 //   ConstructGreensOperator     MaterialGrid.cpp:583-615 (+ Symmetrize/projection 717)
 #pragma once
 
+#include <type_traits>
+
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -54,6 +56,52 @@ __host__ __device__ constexpr int slip_n(int s, int i) {
                   : ((s < 6) ? -1 : 1);
 }
 
+// c0 x0 + c1 x1 + c2 x2 for compile-time coefficients in {-1, 0, 1}, summed in
+// index order: the same roundings as the multiply-add chain over the integer
+// slip vectors, without the multiplications by 0 and 1.
+template <int C0, int C1, int C2, typename T>
+__host__ __device__ __forceinline__ T signed_sum3(T x0, T x1, T x2) {
+  static_assert(C0 != 0 || C1 != 0 || C2 != 0, "zero vector");
+  static_assert(C0 >= -1 && C0 <= 1 && C1 >= -1 && C1 <= 1 && C2 >= -1 && C2 <= 1, "signs");
+  auto term = [](auto c, T x) { return c < 0 ? -x : x; };
+  if constexpr (C0 != 0) {
+    T r = term(C0, x0);
+    if constexpr (C1 > 0) r = r + x1;
+    if constexpr (C1 < 0) r = r - x1;
+    if constexpr (C2 > 0) r = r + x2;
+    if constexpr (C2 < 0) r = r - x2;
+    return r;
+  } else if constexpr (C1 != 0) {
+    T r = term(C1, x1);
+    if constexpr (C2 > 0) r = r + x2;
+    if constexpr (C2 < 0) r = r - x2;
+    return r;
+  } else {
+    return term(C2, x2);
+  }
+}
+
+template <int I, int N, typename F>
+__host__ __device__ __forceinline__ void static_for_s(F&& f) {
+  if constexpr (I < N) {
+    f(std::integral_constant<int, I>{});
+    static_for_s<I + 1, N>(f);
+  }
+}
+
+// Rotated slip direction b' = R b and plane normal n' = R n of system S (R
+// row-major), from the integer vectors of slip_b / slip_n.
+template <int S, typename T>
+__host__ __device__ __forceinline__ void rotated_slip(const T R[9], T b[3], T n[3]) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    b[i] = signed_sum3<slip_b(S, 0), slip_b(S, 1), slip_b(S, 2)>(R[3 * i], R[3 * i + 1],
+                                                                 R[3 * i + 2]);
+    n[i] = signed_sum3<slip_n(S, 0), slip_n(S, 1), slip_n(S, 2)>(R[3 * i], R[3 * i + 1],
+                                                                 R[3 * i + 2]);
+  }
+}
+
 // 1/(2 sqrt 3) and 1/6: the coefficients that map q_ij = b'_i n'_j (rotated
 // vectors) to the 5 deviatoric-basis components of sym(b' (x) n')/(2 sqrt 6).
 #define VPFFT_INV_2SQRT3 0.28867513459481288225
@@ -66,21 +114,17 @@ __host__ __device__ constexpr int slip_n(int s, int i) {
 //   m0 = (S11 - S00)/sqrt2, m1 = (2 S22 - S00 - S11)/sqrt6,
 //   m2 = sqrt2 S12, m3 = sqrt2 S02, m4 = sqrt2 S01.
 __device__ __forceinline__ void schmid_from_R(const double R[9], double m[kNS][5]) {
-#pragma unroll
-  for (int s = 0; s < kNS; ++s) {
+  static_for_s<0, kNS>([&](auto sc) {
+    constexpr int s = decltype(sc)::value;
     double b[3], n[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      b[i] = R[3 * i + 0] * slip_b(s, 0) + R[3 * i + 1] * slip_b(s, 1) + R[3 * i + 2] * slip_b(s, 2);
-      n[i] = R[3 * i + 0] * slip_n(s, 0) + R[3 * i + 1] * slip_n(s, 1) + R[3 * i + 2] * slip_n(s, 2);
-    }
+    rotated_slip<s>(R, b, n);
     const double q00 = b[0] * n[0], q11 = b[1] * n[1], q22 = b[2] * n[2];
     m[s][0] = (q11 - q00) * VPFFT_INV_2SQRT3;
     m[s][1] = (2.0 * q22 - q00 - q11) * (1.0 / 6.0);
     m[s][2] = (b[1] * n[2] + b[2] * n[1]) * VPFFT_INV_2SQRT3;
     m[s][3] = (b[0] * n[2] + b[2] * n[0]) * VPFFT_INV_2SQRT3;
     m[s][4] = (b[0] * n[1] + b[1] * n[0]) * VPFFT_INV_2SQRT3;
-  }
+  });
 }
 
 // Plastic spin of MaterialGrid::ShearRate (MaterialGrid.cpp:1098-1119) and

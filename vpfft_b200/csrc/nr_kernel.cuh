@@ -169,14 +169,10 @@ struct SL<float> {
 // computed in the staging precision MS (FP64 path: double; mixed: float).
 template <typename MS>
 __device__ __forceinline__ void schmid_to_smem(const MS R[9], MS* msm, int bs) {
-#pragma unroll
-  for (int s = 0; s < kNS; ++s) {
+  static_for_s<0, kNS>([&](auto sc) {
+    constexpr int s = decltype(sc)::value;
     MS b[3], n[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      b[i] = R[3 * i + 0] * slip_b(s, 0) + R[3 * i + 1] * slip_b(s, 1) + R[3 * i + 2] * slip_b(s, 2);
-      n[i] = R[3 * i + 0] * slip_n(s, 0) + R[3 * i + 1] * slip_n(s, 1) + R[3 * i + 2] * slip_n(s, 2);
-    }
+    rotated_slip<s>(R, b, n);
     const MS q00 = b[0] * n[0], q11 = b[1] * n[1], q22 = b[2] * n[2];
     const MS c23 = (MS)VPFFT_INV_2SQRT3, c6 = (MS)(1.0 / 6.0);
     msm[SL<MS>::m(s, 0, bs)] = (q11 - q00) * c23;
@@ -184,7 +180,7 @@ __device__ __forceinline__ void schmid_to_smem(const MS R[9], MS* msm, int bs) {
     msm[SL<MS>::m(s, 2, bs)] = (b[1] * n[2] + b[2] * n[1]) * c23;
     msm[SL<MS>::m(s, 3, bs)] = (b[0] * n[2] + b[2] * n[0]) * c23;
     msm[SL<MS>::m(s, 4, bs)] = (b[0] * n[1] + b[1] * n[0]) * c23;
-  }
+  });
 }
 
 template <typename MS>
