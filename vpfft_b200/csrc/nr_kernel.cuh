@@ -19,6 +19,7 @@
 // back to complete pivoting when K is singular (systems with r_s snapped to 0).
 #pragma once
 
+#include <cfloat>
 #include "device_math.cuh"
 
 namespace vpfft {
@@ -189,6 +190,19 @@ __device__ __forceinline__ void load_m(const MS* msm, int bs, int s, double m[5]
   for (int c = 0; c < 5; ++c) m[c] = (double)msm[SL<MS>::m(s, c, bs)];
 }
 
+// 1/x: IEEE division in FP64; in FP32 (the Newton predictor, which the FP64
+// step polishes) the fast reciprocal intrinsic.
+__device__ __forceinline__ double recip(double x) { return 1.0 / x; }
+__device__ __forceinline__ float recip(float x) { return __fdividef(1.f, x); }
+
+// |delta| / |avg| < eps for the squared norms dn = |delta|^2, an = |avg|^2,
+// compared as dn < eps^2 an; *bad when a norm is not finite or |avg| = 0
+// (where the quotient would not be finite).
+__device__ __forceinline__ bool small_step_f32(float dn, float an, float eps, bool* bad) {
+  *bad = !(dn <= FLT_MAX) || !(an > 0.f) || !(an <= FLT_MAX);
+  return dn < eps * eps * an;
+}
+
 // LDL^T solve of a symmetric positive-definite 5x5 A (packed upper) x = b.
 // Returns false when a pivot is not positive (A not numerically SPD).
 template <typename T>
@@ -202,7 +216,7 @@ __device__ __forceinline__ bool ldlt5_solve(const T A[15], const T b[5], T x[5])
     for (int k = 0; k < j; ++k) dj -= L[j][k] * L[j][k] * d[k];
     ok = ok && (dj > T(0));
     d[j] = dj;
-    id[j] = T(1) / dj;
+    id[j] = recip(dj);
 #pragma unroll
     for (int i = j + 1; i < 5; ++i) {
       T a = A[sym5(j, i)];
@@ -410,9 +424,10 @@ __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, in
       an += av * av;
       cur[c] = nw;
     }
-    const float rel = sqrtf(dn) / sqrtf(an);
-    if (!isfinite(rel)) return false;
-    if (rel < p.eps_f) {
+    bool bad;
+    const bool small = small_step_f32(dn, an, p.eps_f, &bad);
+    if (bad) return false;
+    if (small) {
 #pragma unroll
       for (int c = 0; c < 5; ++c) s_io[c] = (double)cur[c];
       return true;
@@ -622,9 +637,11 @@ __device__ __forceinline__ bool nr_predict_unconstrained_fp32(const MS* msm, con
       sn += sm * sm;
       cur[c] = nw;
     }
-    const float rel = 2.f * sqrtf(dn) / sqrtf(sn);
-    if (!isfinite(rel)) return false;
-    if (rel < p.eps_f) {
+    // 2 |delta| / |sum| < eps
+    bool bad;
+    const bool small = small_step_f32(4.f * dn, sn, p.eps_f, &bad);
+    if (bad) return false;
+    if (small) {
 #pragma unroll
       for (int c = 0; c < 5; ++c) s_io[c] = (double)cur[c];
       return true;
