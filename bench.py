@@ -61,9 +61,13 @@ SEED = 2024
 RATE_SENS = 20
 VEL_GRAD = np.diag([1.0, 0.0, -1.0])
 
-WORKLOAD = ("256^3 periodic Voronoi polycrystal, 1000 grains, uniform SO(3) orientations, "
+def workload(n: int) -> str:
+    return (f"{n}^3 periodic Voronoi polycrystal, 1000 grains, uniform SO(3) orientations, "
             "FCC 12 {111}<110>, n=20, gdot0=1, CRSS=1, plane-strain diag(1,0,-1), one "
             "fixed-point iteration per step")
+
+
+WORKLOAD = workload(256)
 
 
 def peaks():
@@ -594,9 +598,11 @@ def main(argv=None):
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 fields/FFT + f64 NR" if args.precision == "mixed" else "f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "grid": [args.grid] * 3, "grains": N_GRAINS,
+        "config": {"workload": workload(args.grid), "grid": [args.grid] * 3, "grains": N_GRAINS,
                    "seed": SEED, "precision": args.precision,
-                   "l2": "inputs larger than L2 (resident fields of the 256^3 grid)",
+                   "l2": (f"inputs larger than L2 (resident fields of the {args.grid}^3 grid)"
+                          if args.grid >= 128 else
+                          f"resident fields of the {args.grid}^3 grid (smaller than L2)"),
                    "parallelism": f"replicas x{ws}"},
         "roofline": roofline,
         "kernels": kernels,
