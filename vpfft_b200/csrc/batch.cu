@@ -680,6 +680,13 @@ vpfft_status vpfft_batch_create(vpfft_precision precision, const vpfft_material*
   if ((e = cudaMallocHost(&b->h_ctrl, sizeof(IterCtrl) * ms)) != cudaSuccess) return bail(e, "pinned");
   if ((e = cudaMallocHost(&b->h_sum25, sizeof(double) * 25 * ms)) != cudaSuccess)
     return bail(e, "pinned");
+  // block lists sized for a full batch (a tick then never allocates)
+  for (DeviceLists* dl : {&b->setup_lists, &b->iter_lists}) {
+    const int cap = 16 * ms + 64;
+    if ((e = cudaMalloc(&dl->d, sizeof(int) * cap)) != cudaSuccess) return bail(e, "lists");
+    if ((e = cudaMallocHost(&dl->h, sizeof(int) * cap)) != cudaSuccess) return bail(e, "pinned");
+    dl->cap = cap;
+  }
   std::memset(b->h_ctrl, 0, sizeof(IterCtrl) * ms);
   if ((e = cudaMemset(b->d_ctrl, 0, sizeof(IterCtrl) * ms)) != cudaSuccess) return bail(e, "ctrl");
   if ((e = cudaMallocHost(&b->h_desc, desc_bytes * ms)) != cudaSuccess) return bail(e, "pinned");

@@ -608,6 +608,12 @@ vpfft_status vpfft_grid_create(int nx, int ny, int nz, const vpfft_material* mat
   CKC(cudaMalloc(&g->lambda, es * n * 5));
   CKC(cudaMalloc(&g->work, es * n * 5));
   if (g->keep_d) CKC(cudaMalloc(&g->dkeep, es * n * 5));
+  // the per-voxel CRSS (written by the first hardening update) and the
+  // iteration history are allocated here, so that no solve -- in particular
+  // no batch request -- allocates device memory
+  CKC(cudaMalloc(&g->crss, es * n * kNS));
+  CKC(cudaMalloc(&g->hist, sizeof(double) * 12 * 128));
+  g->hist_cap = 128;
   CKC(cudaMalloc(&g->acc, sizeof(double) * n));
   const size_t nparts = (size_t)std::max(nr_blocks(g->n), ref_medium_blocks(g->n));
   CKC(cudaMalloc(&g->partials, sizeof(double) * nparts * 25));

@@ -438,17 +438,23 @@ __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, in
 
 // SolveConstrainedConstitutiveEquations (Solvers.cpp:111-222).  ed = Edot + d~.
 // Returns the Newton steps taken; *capped when the iteration budget ran out.
+// The stopping test |delta| / |avg| < eps is taken on the squared norms
+// (|delta|^2 < eps^2 |avg|^2); *rel_out (optional) gets the last step's ratio,
+// *tight (optional) whether it was below 1e-5.
 template <int NEXP, bool kTauSmem, typename MS, class C = ParamConsts>
 __device__ __forceinline__ int nr_constrained_smem(const MS* msm, const MS* tsm, int bs,
                                                    const NRParams& p, const C& cs,
                                                    const double lam[5],
                                                    const double ed[5], double s_io[5],
                                                    double* rel_out, bool* capped,
-                                                   double* e_lin = nullptr) {
+                                                   double* e_lin = nullptr,
+                                                   bool* tight = nullptr) {
   double cur[5], saved[5], nw[5] = {-1.0, -3.0, -7.0, -9.0, -11.0};
 #pragma unroll
   for (int c = 0; c < 5; ++c) cur[c] = saved[c] = s_io[c];
-  double rel = 1e5;
+  const double eps2 = p.eps * p.eps;
+  double dn = 1e10, an = 1.0;  // a ratio of 1e5 before the first step
+  bool conv = false;
   int remaining = p.max_iter, steps = 0;
   *capped = false;
   while (remaining > 0) {
@@ -464,7 +470,8 @@ __device__ __forceinline__ int nr_constrained_smem(const MS* msm, const MS* tsm,
       remaining--;
       if (remaining < 0) {
         *capped = true;
-        *rel_out = rel;
+        if (rel_out) *rel_out = sqrt(dn) / sqrt(an);
+        if (tight) *tight = false;
 #pragma unroll
         for (int c = 0; c < 5; ++c) s_io[c] = cur[c];
         return steps;
@@ -486,7 +493,8 @@ __device__ __forceinline__ int nr_constrained_smem(const MS* msm, const MS* tsm,
     for (int k = 0; k < 15; ++k) K[k] += cs.L0inv(k);
     double delta[5];
     ldlt5_solve<double>(K, y, delta);
-    double dn = 0.0, an = 0.0;
+    dn = 0.0;
+    an = 0.0;
 #pragma unroll
     for (int c = 0; c < 5; ++c) {
       saved[c] = cur[c];
@@ -497,12 +505,13 @@ __device__ __forceinline__ int nr_constrained_smem(const MS* msm, const MS* tsm,
       an += av * av;
       cur[c] = nw[c];
     }
-    rel = sqrt(dn) / sqrt(an);
     steps++;
-    if (rel < p.eps) break;
+    conv = dn < eps2 * an;
+    if (conv) break;
   }
-  *rel_out = rel;
-  *capped = !(rel < p.eps);
+  if (rel_out) *rel_out = sqrt(dn) / sqrt(an);
+  if (tight) *tight = dn < 1e-10 * an;
+  *capped = !conv;
 #pragma unroll
   for (int c = 0; c < 5; ++c) s_io[c] = nw[c];
   if (e_lin) {
@@ -580,9 +589,9 @@ __device__ __forceinline__ int nr_unconstrained_smem(const MS* msm, const MS* ts
       sn += sm * sm;
       cur[c] = nw[c];
     }
-    const double rel = 2.0 * sqrt(dn) / sqrt(sn);
     steps++;
-    if (rel < p.eps) {
+    // 2 |delta| / |new + old| < eps, on the squared norms
+    if (4.0 * dn < p.eps * p.eps * sn) {
       conv = true;
       break;
     }

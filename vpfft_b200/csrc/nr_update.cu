@@ -145,7 +145,7 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const C& cs, l
     double ed[5];
 #pragma unroll
     for (int c = 0; c < 5; ++c) ed[c] = cs.edot(c) + d[c];
-    double rel, e[5];
+    double e[5];
     bool capped;
     if constexpr (sizeof(S) == 4) {
       // mixed precision: an FP32 Newton predictor from the previous stress,
@@ -165,8 +165,10 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const C& cs, l
         for (int c = 0; c < 5; ++c) s[c] = s0[c] / mx;
       }
       double el[5];
-      nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, cs, lam, ed, s, &rel, &capped, el);
-      if (!capped && rel < 1e-5) {
+      bool tight;
+      nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, cs, lam, ed, s, nullptr, &capped, el,
+                                          &tight);
+      if (!capped && tight) {
 #pragma unroll
         for (int c = 0; c < 5; ++c) e[c] = el[c];
       } else {
@@ -177,7 +179,7 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const C& cs, l
       if (mx < 1e-10) status |= kStatusMaxRssTiny;
 #pragma unroll
       for (int c = 0; c < 5; ++c) s[c] /= mx;
-      nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, cs, lam, ed, s, &rel, &capped);
+      nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, cs, lam, ed, s, nullptr, &capped);
       apply_smem<NEXP, kTauSmem>(msm, tsm, bs, p, s, e);
     }
     capped_count += capped ? 1 : 0;
