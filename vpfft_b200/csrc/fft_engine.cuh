@@ -52,6 +52,24 @@ template <typename T>
 VPFFT_HD T sub(T a, T b) {
   return T{a.x - b.x, a.y - b.y};
 }
+// FP32 complex add and subtract as one paired instruction each on sm_100
+// (a - b as fma(b, -1, a): one rounding, the same value as a - b).
+template <>
+VPFFT_HD float2 add(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+  return __fadd2_rn(a, b);
+#else
+  return float2{a.x + b.x, a.y + b.y};
+#endif
+}
+template <>
+VPFFT_HD float2 sub(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+  return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+#else
+  return float2{a.x - b.x, a.y - b.y};
+#endif
+}
 template <typename T, typename R>
 VPFFT_HD T scl(T a, R s) {
   return T{a.x * s, a.y * s};
