@@ -297,6 +297,7 @@ void free_grid_buffers(vpfft_grid* g) {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (g->h_ctrl) cudaFreeHost(g->h_ctrl);
+  if (g->loop_graph) cudaGraphExecDestroy(g->loop_graph);
   for (cudaEvent_t e : g->ev) cudaEventDestroy(e);
   g->ev.clear();
   if (g->stream) cudaStreamDestroy(g->stream);
@@ -399,14 +400,51 @@ vpfft_status do_fixed_point(vpfft_grid* g, const double edot[5], int max_iter, d
       g->ev.push_back(e);
     }
   }
-  int done_before = 0;
-  for (;;) {
+  // The first chunk runs eagerly; when the loop goes on, the chunk is captured
+  // once into a CUDA graph (updating the grid's executable graph in place when
+  // only the parameters changed) and replayed: the kernels return at once when
+  // the device-side control block says the loop is done.  Profiling keeps the
+  // eager launches (events between the kernels).
+  auto enqueue_chunk = [&](bool profiled) {
+    int n = 0;
     for (int b = 0; b < batch; ++b) {
-      cudaEvent_t* e = g->profile ? &g->ev[(size_t)b * kEv] : nullptr;
-      g->launches += launch_spectral_iteration<S>(sp, gp, (S*)g->work, g->ctrl, g->stream, 5, e);
-      g->launches += launch_nr_update<S>(p, f, g->partials, g->ctrl, g->hist, g->stream,
-                                         e ? e + 6 : nullptr);
+      cudaEvent_t* e = profiled ? &g->ev[(size_t)b * kEv] : nullptr;
+      n += launch_spectral_iteration<S>(sp, gp, (S*)g->work, g->ctrl, g->stream, 5, e);
+      n += launch_nr_update<S>(p, f, g->partials, g->ctrl, g->hist, g->stream,
+                               e ? e + 6 : nullptr);
     }
+    return n;
+  };
+  int done_before = 0, chunk = 0, chunk_launches = 0;
+  bool graph_ready = false;
+  for (;;) {
+    if (g->profile || chunk == 0) {
+      chunk_launches = enqueue_chunk(g->profile);
+    } else {
+      if (!graph_ready) {
+        cudaGraph_t graph = nullptr;
+        CK(g, cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_chunk(false);
+        CK(g, cudaStreamEndCapture(g->stream, &graph));
+        bool updated = false;
+        if (g->loop_graph) {
+          cudaGraphExecUpdateResultInfo info;
+          updated = cudaGraphExecUpdate(g->loop_graph, graph, &info) == cudaSuccess;
+          if (!updated) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(g->loop_graph);
+            g->loop_graph = nullptr;
+          }
+        }
+        cudaError_t e = updated ? cudaSuccess : cudaGraphInstantiate(&g->loop_graph, graph, 0);
+        cudaGraphDestroy(graph);
+        CK(g, e);
+        graph_ready = true;
+      }
+      CK(g, cudaGraphLaunch(g->loop_graph, g->stream));
+    }
+    g->launches += chunk_launches;
+    ++chunk;
     CKL(g);
     CK(g, cudaMemcpyAsync(g->h_ctrl, g->ctrl, sizeof(IterCtrl), cudaMemcpyDeviceToHost, g->stream));
     CK(g, cudaStreamSynchronize(g->stream));

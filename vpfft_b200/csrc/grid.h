@@ -60,6 +60,9 @@ struct vpfft_grid {
   double phase_ms[VPFFT_NUM_PHASES] = {0};
   int64_t phase_n[VPFFT_NUM_PHASES] = {0};
   bool in_batch = false;      // a batch request owns the grid until it completes
+  // the fixed-point loop's chunk of iterations as a CUDA graph (re-captured for
+  // each loop, replayed for its chunks after the first)
+  cudaGraphExec_t loop_graph = nullptr;
   std::string err;
 };
 
