@@ -18,7 +18,11 @@ from vpfft_b200 import capi, fixtures
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-12
-DIMS = [(16, 16, 16), (12, 10, 8), (24, 20, 18), (32, 32, 32), (8, 8, 8)]
+# cubic and non-cubic RVEs: compile-time line engines (16, 32, 48, 64), the
+# runtime-plan engine (8, 10, 12, 18, 20, 24) and both on different axes, so
+# the batch forms several size classes whose pass chains run concurrently
+DIMS = [(16, 16, 16), (12, 10, 8), (24, 20, 18), (32, 32, 32), (8, 8, 8), (48, 16, 20),
+        (16, 64, 32)]
 
 
 def material():
