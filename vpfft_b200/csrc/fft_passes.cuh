@@ -44,6 +44,9 @@ struct Tiles {
   static constexpr int kElems = (E::kN >= 64 || kBatch) ? (kF32 ? 2048 : 1024) : 512;
   static constexpr int kThreads = E::kN ? (kF32 ? 256 : 128) : 256;  // z and y passes
   static constexpr int kThreadsX = E::kN ? 128 : 256;                // x pass
+  // x-pass blocks per SM the registers are capped for: FP32 at 6 (85
+  // registers; measured 15 % faster than 4), FP64 at 4 (more would spill)
+  static constexpr int kMinBlocksX = (E::kN && kF32) ? 6 : 512 / kThreadsX;
   static constexpr int cmax(int a, int b) { return a > b ? a : b; }
   static constexpr int kZ = E::kN ? cmax(2, 2 * (kElems / E::kN)) : 16;  // real z-lines
   static constexpr int kY = E::kN ? cmax(1, kElems / E::kN) : (sizeof(S) == 4 ? 16 : 8);
@@ -359,7 +362,7 @@ __global__ void __launch_bounds__(Tiles<S, E>::kThreads)
   pass_y_body<SIGN, S, E, Tiles<S, E>>(in, out, pl, dnx, twg, nx, nh, blockIdx.x, blockIdx.y);
 }
 template <int MODE, typename S, class E>
-__global__ void __launch_bounds__(Tiles<S, E>::kThreadsX, 512 / Tiles<S, E>::kThreadsX)
+__global__ void __launch_bounds__(Tiles<S, E>::kThreadsX, Tiles<S, E>::kMinBlocksX)
     k_pass_x(typename CX<S>::T* __restrict__ B, LinePlan pl, FastDiv dny,
              const typename CX<S>::T* __restrict__ twg, GreenParams<S> gp, int ny, int nh,
              int ncomp, const IterCtrl* ctrl) {
