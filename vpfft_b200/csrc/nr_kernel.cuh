@@ -320,7 +320,10 @@ __device__ __forceinline__ float2 cpow2(float2 x) {
 // of every float2 carries system q, lane 1 system q+1 (FFMA2/FMUL2 issue two
 // FMAs per instruction); the two partial sums of S and K are added at the end.
 // Compile-time rate exponent NEXP > 1 (the power branch of Solvers.cpp:177).
-template <int NEXP, bool kTauSmem>
+// kFull: the pass over the 6 pairs fully unrolled (the single-grid kernel,
+// which has the registers for it: measured 3 % faster) or by 2 (the batched
+// kernel at 4 blocks per SM, where the full unroll spills).
+template <int NEXP, bool kTauSmem, bool kFull = true>
 __device__ __forceinline__ bool accumulate_pairs(const float* msm, const float* tsm, int bs,
                                                  const NRParams& p, const float s[5], float S[5],
                                                  float K[15], float* rmax) {
@@ -339,10 +342,7 @@ __device__ __forceinline__ bool accumulate_pairs(const float* msm, const float* 
   const float mr = p.max_rss_f;
   bool adm = true;
   float rm = 0.f;
-  // fully unrolled over the 6 pairs (measured 3 % faster than unrolling by 2;
-  // the FP64 pass over the 12 systems stays unrolled by 2)
-#pragma unroll
-  for (int pq = 0; pq < kNS / 2; ++pq) {
+  auto pair = [&](int pq) {
     float2 m[5];
 #pragma unroll
     for (int c = 0; c < 5; ++c) m[c] = m2p[(pq * 5 + c) * bs];
@@ -369,6 +369,13 @@ __device__ __forceinline__ bool accumulate_pairs(const float* msm, const float* 
 #pragma unroll
       for (int j = i; j < 5; ++j) K2[sym5(i, j)] = __ffma2_rn(mw, m[j], K2[sym5(i, j)]);
     }
+  };
+  if constexpr (kFull) {
+#pragma unroll
+    for (int pq = 0; pq < kNS / 2; ++pq) pair(pq);
+  } else {
+#pragma unroll 2
+    for (int pq = 0; pq < kNS / 2; ++pq) pair(pq);
   }
 #pragma unroll
   for (int c = 0; c < 5; ++c) S[c] = S2[c].x + S2[c].y;
@@ -383,7 +390,7 @@ __device__ __forceinline__ bool accumulate_pairs(const float* msm, const float* 
 // true and the iterate in s_io when it converged with finite values; the
 // caller then takes the accepted step with FP64 residual and Jacobian.
 // *rmax0 gets max_s |r_s| at the starting point.
-template <int NEXP, bool kTauSmem, typename MS, class C>
+template <int NEXP, bool kTauSmem, bool kFull = true, typename MS, class C>
 __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, int bs,
                                                 const NRParams& p, const C& cs,
                                                 const double lam[5], const double ed[5],
@@ -400,7 +407,7 @@ __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, in
     float S[5], K[15], rm;
     bool adm;
     if constexpr (NEXP > 1 && sizeof(MS) == 4)
-      adm = accumulate_pairs<NEXP, kTauSmem>(msm, tsm, bs, p, cur, S, K, &rm);
+      adm = accumulate_pairs<NEXP, kTauSmem, kFull>(msm, tsm, bs, p, cur, S, K, &rm);
     else
       adm = accumulate<NEXP, false, kTauSmem, float, MS, true>(msm, tsm, bs, p, cur, S, K, &rm);
     if (it == 0) *rmax0 = rm;

@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_batch_min_blocks<MS>())
 // voxels averages out instead of idling warps at a barrier.
 // p: the material and solver constants; cs: the RVE's strain rate and
 // reference medium; n: its voxel count.
-template <typename S, typename MS, int NEXP, bool kTauSmem, class C>
+template <typename S, typename MS, int NEXP, bool kTauSmem, bool kFull, class C>
 __device__ __forceinline__ void nr_update_body(const NRParams& p, const C& cs, long long n,
                                                const FieldPtrs<S>& f, double* partials,
                                                IterCtrl* ctrl, int blk, int nblk, MS* msm,
@@ -168,7 +168,8 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const C& cs, l
       double s0[5];
 #pragma unroll
       for (int c = 0; c < 5; ++c) s0[c] = s[c];
-      const bool ok = nr_predict_fp32<NEXP, kTauSmem>(msm, tsm, bs, p, cs, lam, ed, s, 8, &mx0);
+      const bool ok =
+          nr_predict_fp32<NEXP, kTauSmem, kFull>(msm, tsm, bs, p, cs, lam, ed, s, 8, &mx0);
       if (mx0 < 1e-10f) status |= kStatusMaxRssTiny;
       if (!ok) {
         const double mx = max_resolved<kTauSmem>(msm, tsm, bs, p, s0);
@@ -236,8 +237,8 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_loop_min_blocks<MS>())
   extern __shared__ __align__(16) unsigned char nr_smem[];
   MS* msm = reinterpret_cast<MS*>(nr_smem) + SL<MS>::kThreadStride * threadIdx.x;
   MS* tsm = msm + 60 * kVoxelBlock;
-  nr_update_body<S, MS, NEXP, kTauSmem>(p, ParamConsts{p}, p.n, f, partials, ctrl, blockIdx.x,
-                                        gridDim.x, msm, tsm);
+  nr_update_body<S, MS, NEXP, kTauSmem, true>(p, ParamConsts{p}, p.n, f, partials, ctrl,
+                                              blockIdx.x, gridDim.x, msm, tsm);
 }
 
 template <typename S, typename MS, int NEXP, bool kTauSmem>
@@ -257,8 +258,8 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_loop_batch_min_blocks<MS>())
   MS* tsm = msm + 60 * kVoxelBlock;
   // material and solver constants (the same for every RVE of a batch) from the
   // kernel parameter; the slot's strain rate and reference medium from shared memory
-  nr_update_body<S, MS, NEXP, kTauSmem>(pm, SharedConsts{&sp}, sp.n, sf, d.partials, d.ctrl, lb,
-                                        d.nr_blocks, msm, tsm);
+  nr_update_body<S, MS, NEXP, kTauSmem, false>(pm, SharedConsts{&sp}, sp.n, sf, d.partials,
+                                               d.ctrl, lb, d.nr_blocks, msm, tsm);
 }
 
 
