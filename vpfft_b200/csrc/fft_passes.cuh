@@ -119,9 +119,15 @@ __device__ __forceinline__ void pass_z_r2c_body(const S* __restrict__ W,
   const int nf = min(TZ, nxy - f0);
   const int npair = (nf + 1) / 2;
   const S* src = W + ((long long)c * nxy + f0) * nz;
-  copy_rows<S>(
-      2 * npair, nz, [&](int l, int z) { return l < nf ? src[l * nz + z] : S(0); },
-      [&](int l, int z, S v) { reinterpret_cast<S*>(&a[(l >> 1) * ls + sw(z)])[l & 1] = v; });
+  // rows 2q and 2q+1 packed as line q: each lane reads both rows' element and
+  // stores one complex value
+  copy_rows<T>(
+      npair, nz,
+      [&](int q, int z) {
+        const int l = 2 * q;
+        return T{l < nf ? src[l * nz + z] : S(0), l + 1 < nf ? src[(l + 1) * nz + z] : S(0)};
+      },
+      [&](int q, int z, T v) { a[q * ls + sw(z)] = v; });
   __syncthreads();
   const T* r = E::template fft<-1>(a, b, tw, pl, npair, ls, threadIdx.x, blockDim.x);
   T* dst = A + (long long)c * nx * nh * ny;
@@ -203,13 +209,13 @@ __device__ __forceinline__ void pass_z_c2r_body(const typename CX<S>::T* __restr
   __syncthreads();
   const T* r = E::template fft<1>(a, b, tw, pl, npair, ls, threadIdx.x, blockDim.x);
   S* dst = W + ((long long)c * nxy + f0) * nz;
-  copy_rows<S>(
-      nf, nz,
-      [&](int l, int z) {
-        const T Z = r[(l >> 1) * ls + sw(z)];
-        return ((l & 1) ? Z.y : Z.x) * scale;
-      },
-      [&](int l, int z, S v) { dst[l * nz + z] = v; });
+  // line q holds rows 2q (real part) and 2q+1 (imaginary part)
+  copy_rows<T>(
+      npair, nz, [&](int q, int z) { return r[q * ls + sw(z)]; },
+      [&](int q, int z, T v) {
+        dst[2 * q * nz + z] = v.x * scale;
+        if (2 * q + 1 < nf) dst[(2 * q + 1) * nz + z] = v.y * scale;
+      });
 }
 
 // ---------------------------------------------------------------- y passes
