@@ -636,7 +636,12 @@ __device__ __forceinline__ void green_apply(const GreenParams<R>& gp, int ix, in
     V[0][2] = R(0);      V[1][2] = k2 * is2;  V[2][2] = k1 * is2;
     V[0][3] = k2 * is2;  V[1][3] = R(0);      V[2][3] = k0 * is2;
     V[0][4] = k1 * is2;  V[1][4] = k0 * is2;  V[2][4] = R(0);
-    // A = V L0 V^T
+    // A = V L0 V^T.  The four structural zeros of V (vz) are skipped: adding
+    // 0 * x to a sum leaves it unchanged for finite x, so the results are the
+    // same as with the full products.
+    auto vz = [](int i, int a) {
+      return (i == 0 && a == 2) || (i == 1 && a == 3) || (i == 2 && (a == 0 || a == 4));
+    };
     R VL[3][5];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -644,7 +649,8 @@ __device__ __forceinline__ void green_apply(const GreenParams<R>& gp, int ix, in
       for (int b = 0; b < 5; ++b) {
         R acc = R(0);
 #pragma unroll
-        for (int a = 0; a < 5; ++a) acc += V[i][a] * gp.L0[b * 5 + a];
+        for (int a = 0; a < 5; ++a)
+          if (!vz(i, a)) acc += V[i][a] * gp.L0[b * 5 + a];
         VL[i][b] = acc;
       }
     R A[3][3];
@@ -654,7 +660,8 @@ __device__ __forceinline__ void green_apply(const GreenParams<R>& gp, int ix, in
       for (int k = 0; k < 3; ++k) {
         R acc = R(0);
 #pragma unroll
-        for (int b = 0; b < 5; ++b) acc += VL[i][b] * V[k][b];
+        for (int b = 0; b < 5; ++b)
+          if (!vz(k, b)) acc += VL[i][b] * V[k][b];
         A[i][k] = acc;
       }
     // A^-1 by the adjugate
@@ -688,6 +695,7 @@ __device__ __forceinline__ void green_apply(const GreenParams<R>& gp, int ix, in
       R ar = R(0), ai = R(0);
 #pragma unroll
       for (int b = 0; b < 5; ++b) {
+        if (vz(i, b)) continue;
         ar += V[i][b] * pre[b];
         ai += V[i][b] * pim[b];
       }
