@@ -300,7 +300,14 @@ typedef struct {
   int32_t iterations_per_tick;  /* fixed-point iterations enqueued per tick (default 8) */
   int64_t hbm_budget_bytes;     /* device memory for in-flight spectra (default 8 GiB) */
   int32_t use_graphs;           /* replay the tick's iterations from a CUDA graph (default 1) */
-  int32_t pad_;
+  int32_t fft_tiles;            /* tile family of the batched FFT passes: 0, 1, 2 = tiles of
+                                   about 512, 1024, 2048 complex values per buffer (clamped per
+                                   axis to the longest its line engine has; default 2, the
+                                   same results bit for bit as the single-grid path); -1 =
+                                   autotuned per RVE size (vpfft_batch_get_tunings).  FP64
+                                   results are the same bit for bit in every family; FP32
+                                   passes of different families are separately compiled
+                                   kernels whose last bits can differ. */
 } vpfft_batch_options;
 typedef struct {
   int64_t request_id;
@@ -343,6 +350,25 @@ vpfft_status vpfft_batch_poll(vpfft_batch *b, vpfft_batch_result *out, int cap, 
  * Both complete with status VPFFT_ERR_CANCELLED. */
 vpfft_status vpfft_batch_cancel(vpfft_batch *b, int64_t request_id);
 vpfft_status vpfft_batch_get_info(const vpfft_batch *b, vpfft_batch_info *info);
+/* Autotuner of the batched FFT passes.  The first tick that admits an RVE of a
+ * size new to the process times the five-pass chain of every tile family over
+ * the RVEs of that size admitted in that tick (one warm-up, three timed, CUDA
+ * events on the batch's stream, before their initialisation rewrites the field
+ * the chain writes) and keeps the fastest; later batches of the process reuse
+ * the choice.  One entry per size this batch has admitted, in order of first
+ * admission.  No reference counterpart (the reference plans its FFTs with
+ * FFTW_ESTIMATE, MaterialGrid.cpp:344-376). */
+typedef struct {
+  int32_t nx, ny, nz;
+  int32_t fft_tiles;            /* family in use (0, 1, 2 as in vpfft_batch_options) */
+  int32_t families;             /* families the size's line engines offer (1: no choice) */
+  int32_t source;               /* 0 set by the options, 1 one family only, 2 timed earlier in
+                                   this process, 3 timed by this batch */
+  double ms_per_chain[3];       /* mean time of the five passes per family (0: not timed) */
+} vpfft_tile_tuning;
+/* Copies min(cap, count) entries; *n_out = count. */
+vpfft_status vpfft_batch_get_tunings(const vpfft_batch *b, vpfft_tile_tuning *out, int cap,
+                                     int *n_out);
 const char *vpfft_batch_last_error(const vpfft_batch *b);
 
 /* ------------------------------------------------------------------ text I/O

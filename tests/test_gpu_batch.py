@@ -185,3 +185,62 @@ def test_submit_rejects_mismatched_grid(lib):
         g2 = vp.MaterialGrid(8, 8, 8, material=vp.material(), precision="mixed")
         with pytest.raises(capi.VpfftError):
             b.submit(g2, edot_for(0))
+
+
+# edges with several batched tile families (compile-time engines up to 96
+# points), one axis with the runtime-plan engine, and a 96-point axis
+TILE_DIMS = [(16, 16, 16), (32, 48, 16), (64, 32, 48), (24, 16, 32), (96, 16, 16)]
+# Mixed precision: the FP32 passes of different tile families are separately
+# compiled kernels whose last bits can differ, and the reference's fixed point
+# (which runs to its iteration cap here) carries such differences along; one
+# case measured 1.2e-9 on <sigma> and 2.2e-5 on the stress field.
+TILE_TOL_MIXED = {"avg": 1e-7, "field": 1e-4}
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_fft_tile_families_and_autotuner(lib, precision):
+    """Forced tile families and the autotuned choice: FP64 results are the same
+    bit for bit in every family, mixed results within TILE_TOL_MIXED; the
+    tuning record lists each admitted size once, in admission order, with the
+    timed chain of every family and the fastest one chosen."""
+    runs = {}
+    for tiles in (2, -1, 0, 1):
+        with vp.Batch(precision, material=material(), iterations_per_tick=4,
+                      fft_tiles=tiles) as b:
+            grids, ids = [], []
+            for i, d in enumerate(TILE_DIMS):
+                g = make_grid(d, i, precision, b.new_grid)
+                grids.append(g)
+                ids.append(b.submit(g, edot_for(i), 100, 0.005, 1e-5))
+            b.run()
+            res = {r.request_id: r for r in b.poll()}
+            tun = b.tunings()
+            runs[tiles] = [(res[ids[i]], fields(grids[i])) for i in range(len(TILE_DIMS))]
+        assert [t["dims"] for t in tun] == TILE_DIMS
+        for t in tun:
+            assert 0 <= t["fft_tiles"] < t["families"]
+            if tiles >= 0:
+                assert t["source"] == "options"
+                assert t["fft_tiles"] == min(tiles, t["families"] - 1)
+            else:
+                assert t["source"] in ("timed", "cached")
+                ms = t["ms_per_chain"]
+                assert len(ms) == t["families"] and min(ms) > 0
+                assert t["fft_tiles"] == int(np.argmin(ms))
+        # fixed engines up to 96 points: three families in FP32, two in FP64
+        fams = {t["dims"]: t["families"] for t in tun}
+        assert fams[(16, 16, 16)] == (3 if precision == "mixed" else 2)
+    worst = {}
+    for tiles in (-1, 0, 1):
+        for i, d in enumerate(TILE_DIMS):
+            (ra, fa), (rb, fb) = runs[2][i], runs[tiles][i]
+            assert ra.status == capi.OK and rb.status == capi.OK
+            assert ra.iterations == rb.iterations, (tiles, d)
+            worst[(tiles, d, "avg")] = rel(rb.avg_stress, ra.avg_stress)
+            for k in fa:
+                worst[(tiles, d, k)] = rel(fb[k], fa[k])
+    if precision == "fp64":
+        assert max(worst.values()) == 0.0, max(worst.items(), key=lambda kv: kv[1])
+    else:
+        for key, v in worst.items():
+            assert v <= TILE_TOL_MIXED["avg" if key[2] == "avg" else "field"], (key, v)

@@ -37,7 +37,7 @@ class Batch:
     def __init__(self, precision: str = "mixed", material: capi.Material | None = None,
                  options: capi.SolverOptions | None = None, max_slots: int = 256,
                  iterations_per_tick: int = 8, hbm_budget_bytes: int = 8 << 30,
-                 use_graphs: bool = True):
+                 use_graphs: bool = True, fft_tiles: int = 2):
         lib = capi.load()
         bo = capi.BatchOptions()
         lib.vpfft_batch_options_default(C.byref(bo))
@@ -45,6 +45,7 @@ class Batch:
         bo.iterations_per_tick = iterations_per_tick
         bo.hbm_budget_bytes = hbm_budget_bytes
         bo.use_graphs = int(bool(use_graphs))
+        bo.fft_tiles = int(fft_tiles)
         prec = {"fp64": capi.PREC_FP64, "mixed": capi.PREC_MIXED}[precision]
         h = C.c_void_p()
         self._lib = lib
@@ -123,3 +124,18 @@ class Batch:
         i = capi.BatchInfo()
         self._check(self._lib.vpfft_batch_get_info(self._h, C.byref(i)), self._h)
         return {name: int(getattr(i, name)) for name, _ in capi.BatchInfo._fields_}
+
+    def tunings(self) -> list[dict]:
+        """Tile family of the batched FFT passes per RVE size admitted so far
+        (vpfft_batch_get_tunings): the family used, how many the size offers,
+        how it was chosen and the timed five-pass chain per family (ms)."""
+        n = C.c_int()
+        self._check(self._lib.vpfft_batch_get_tunings(self._h, None, 0, C.byref(n)), self._h)
+        buf = (capi.TileTuning * max(1, n.value))()
+        self._check(self._lib.vpfft_batch_get_tunings(self._h, buf, n.value, C.byref(n)),
+                    self._h)
+        src = {0: "options", 1: "single family", 2: "cached", 3: "timed"}
+        return [{"dims": (int(t.nx), int(t.ny), int(t.nz)), "fft_tiles": int(t.fft_tiles),
+                 "families": int(t.families), "source": src.get(int(t.source), "?"),
+                 "ms_per_chain": [float(v) for v in t.ms_per_chain[: int(t.families)]]}
+                for t in buf[: n.value]]

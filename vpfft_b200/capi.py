@@ -121,7 +121,19 @@ class BatchOptions(C.Structure):
         ("iterations_per_tick", C.c_int32),
         ("hbm_budget_bytes", C.c_int64),
         ("use_graphs", C.c_int32),
-        ("pad_", C.c_int32),
+        ("fft_tiles", C.c_int32),
+    ]
+
+
+class TileTuning(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32),
+        ("ny", C.c_int32),
+        ("nz", C.c_int32),
+        ("fft_tiles", C.c_int32),
+        ("families", C.c_int32),
+        ("source", C.c_int32),
+        ("ms_per_chain", C.c_double * 3),
     ]
 
 
@@ -216,6 +228,8 @@ _PROTOS = {
     "vpfft_batch_poll": (C.c_int, [_G, C.POINTER(BatchResult), C.c_int, C.POINTER(C.c_int)]),
     "vpfft_batch_cancel": (C.c_int, [_G, C.c_int64]),
     "vpfft_batch_get_info": (C.c_int, [_G, C.POINTER(BatchInfo)]),
+    "vpfft_batch_get_tunings": (C.c_int, [_G, C.POINTER(TileTuning), C.c_int,
+                                          C.POINTER(C.c_int)]),
     "vpfft_batch_last_error": (C.c_char_p, [_G]),
     "vpfft_print_field": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, _D, _D]),
     "vpfft_grid_print": (C.c_int, [_G, C.c_int, C.c_char_p]),

@@ -26,7 +26,9 @@
 #include <cstring>
 #include <deque>
 #include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "grid.h"
@@ -95,6 +97,7 @@ struct Active {
   size_t off = 0;  // arena offset of X (X2 follows)
   Phase phase = kInit;
   bool tau = false;  // per-voxel CRSS
+  int fam = -1;      // tile family of the batched FFT passes
 };
 
 // Host mirror of one device block list: slots and cumulative block counts.
@@ -157,6 +160,10 @@ struct vpfft_batch {
   cudaStream_t aux[kAux] = {};
   cudaEvent_t ev_fork = nullptr;
   cudaEvent_t ev_join[kAux] = {};
+  // FFT tile families: per RVE size, in order of first admission
+  std::map<std::tuple<int, int, int>, int> fam_of;
+  std::vector<vpfft_tile_tuning> tunings;
+  cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;  // autotuner timing
   std::string err;
 };
 
@@ -326,6 +333,116 @@ vpfft_status admit(vpfft_batch* b, std::vector<int>& admitted) {
   return VPFFT_OK;
 }
 
+// ---- autotuner of the batched FFT passes' tile family (vpfft_batch_options
+// fft_tiles = -1).  A family only regroups lines into blocks: FP64 results
+// are the same bit for bit, FP32 ones can differ in the last bits.
+struct TileChoice {
+  int fam;
+  double ms[3];
+};
+std::mutex g_tile_mu;
+std::map<std::tuple<int, int, int, int, int>, TileChoice> g_tiles;  // (device, bytes, nx, ny, nz)
+
+// Mean time of the five passes in family fam over the slots of active[idxs]
+// (all of one size): one warm-up chain, then three timed.
+template <typename S>
+vpfft_status time_chain(vpfft_batch* b, const std::vector<int>& idxs, int fam, double* ms) {
+  HostList z, y, x;
+  SpectralShape sh{};
+  size_t s_zr = 0, s_zc = 0, s_y = 0, s_x = 0;
+  for (int idx : idxs) {
+    const Active& a = b->active[idx];
+    sh = spectral_shape<S>(host_desc<S>(b, a.slot)->sp, 5, fam);
+    z.add(a.slot, sh.blocks_z);
+    y.add(a.slot, sh.blocks_y);
+    x.add(a.slot, sh.blocks_x);
+    s_zr = std::max(s_zr, sh.smem_z_r2c);
+    s_zc = std::max(s_zc, sh.smem_z_c2r);
+    s_y = std::max(s_y, sh.smem_y);
+    s_x = std::max(s_x, sh.smem_x);
+  }
+  std::vector<BatchLaunch> bl;
+  if (vpfft_status s = upload_lists(b, b->setup_lists, {&z, &y, &x}, bl)) return s;
+  const PassChain c{sh.set_z, sh.set_y, sh.set_x, bl[0], bl[1], bl[2], s_zr, s_zc, s_y, s_x,
+                    sh.fam_z, sh.fam_y, sh.fam_x};
+  constexpr int kReps = 3;
+  b->launches += launch_spectral_chain<S>(dev_desc<S>(b), c, b->stream);
+  BCK(b, cudaEventRecord(b->ev_t0, b->stream));
+  for (int r = 0; r < kReps; ++r) b->launches += launch_spectral_chain<S>(dev_desc<S>(b), c, b->stream);
+  BCK(b, cudaEventRecord(b->ev_t1, b->stream));
+  BCK(b, cudaGetLastError());
+  // the timed chains also finish before the host stages the next lists
+  BCK(b, cudaEventSynchronize(b->ev_t1));
+  float t = 0.f;
+  BCK(b, cudaEventElapsedTime(&t, b->ev_t0, b->ev_t1));
+  *ms = (double)t / kReps;
+  return VPFFT_OK;
+}
+
+// Tile family of every newly admitted slot.  Runs before the slots'
+// initialisation, which rewrites the real field (work) the chain's last pass
+// writes; the chain's other outputs are the slots' spectrum buffers.
+template <typename S>
+vpfft_status assign_tiles(vpfft_batch* b, const std::vector<int>& admitted) {
+  // sizes in order of admission, each with its slots
+  std::vector<std::pair<std::tuple<int, int, int>, std::vector<int>>> groups;
+  for (int idx : admitted) {
+    const vpfft_grid* g = b->active[idx].r.g;
+    const auto key = std::make_tuple(g->nx, g->ny, g->nz);
+    auto it = std::find_if(groups.begin(), groups.end(),
+                           [&](const auto& e) { return e.first == key; });
+    if (it == groups.end()) it = groups.insert(groups.end(), {key, {}});
+    it->second.push_back(idx);
+  }
+  for (auto& kv : groups) {
+    auto it = b->fam_of.find(kv.first);
+    if (it == b->fam_of.end()) {
+      vpfft_tile_tuning t{};
+      std::tie(t.nx, t.ny, t.nz) = kv.first;
+      const int nf = spectral_shape<S>(host_desc<S>(b, b->active[kv.second[0]].slot)->sp, 5)
+                         .families;
+      t.families = nf;
+      int fam = nf - 1;
+      if (b->bopt.fft_tiles >= 0) {
+        fam = std::min(b->bopt.fft_tiles, nf - 1);
+        t.source = 0;
+      } else if (nf == 1) {
+        t.source = 1;
+      } else {
+        const auto key = std::make_tuple(b->device, (int)sizeof(S), t.nx, t.ny, t.nz);
+        bool cached = false;
+        {
+          std::lock_guard<std::mutex> lk(g_tile_mu);
+          auto c = g_tiles.find(key);
+          if (c != g_tiles.end()) {
+            fam = c->second.fam;
+            for (int f = 0; f < 3; ++f) t.ms_per_chain[f] = c->second.ms[f];
+            cached = true;
+          }
+        }
+        if (cached) {
+          t.source = 2;
+        } else {
+          for (int f = 0; f < nf; ++f)
+            if (vpfft_status s = time_chain<S>(b, kv.second, f, &t.ms_per_chain[f])) return s;
+          fam = 0;
+          for (int f = 1; f < nf; ++f)
+            if (t.ms_per_chain[f] < t.ms_per_chain[fam]) fam = f;
+          TileChoice ch{fam, {t.ms_per_chain[0], t.ms_per_chain[1], t.ms_per_chain[2]}};
+          std::lock_guard<std::mutex> lk(g_tile_mu);
+          g_tiles.emplace(key, ch);
+          t.source = 3;
+        }
+      }
+      t.fft_tiles = fam;
+      b->tunings.push_back(t);
+      it = b->fam_of.emplace(kv.first, fam).first;
+    }
+    for (int idx : kv.second) b->active[idx].fam = it->second;
+  }
+  return VPFFT_OK;
+}
+
 // After the INIT tick: L0 and the loop constants of an admitted slot.
 template <typename S>
 vpfft_status start_loop(vpfft_batch* b, Active& a) {
@@ -350,6 +467,7 @@ struct ClassList {
   const void* set_z;
   const void* set_y;
   const void* set_x;
+  int fam_z, fam_y, fam_x;
   HostList z, y, x;
   size_t smem_z_r2c = 0, smem_z_c2r = 0, smem_y = 0, smem_x = 0;
 };
@@ -363,12 +481,15 @@ void build_iter_lists(vpfft_batch* b, IterLists& L) {
   for (const Active& a : b->active) {
     if (a.phase != kIter) continue;
     const SlotDesc<S>& d = *host_desc<S>(b, a.slot);
-    const SpectralShape sh = spectral_shape<S>(d.sp, 5);
+    const SpectralShape sh = spectral_shape<S>(d.sp, 5, a.fam);
     ClassList* c = nullptr;
     for (ClassList& e : L.cls)
-      if (e.set_z == sh.set_z && e.set_y == sh.set_y && e.set_x == sh.set_x) c = &e;
+      if (e.set_z == sh.set_z && e.set_y == sh.set_y && e.set_x == sh.set_x &&
+          e.fam_z == sh.fam_z && e.fam_y == sh.fam_y && e.fam_x == sh.fam_x)
+        c = &e;
     if (!c) {
-      L.cls.push_back(ClassList{sh.set_z, sh.set_y, sh.set_x, {}, {}, {}});
+      L.cls.push_back(ClassList{sh.set_z, sh.set_y, sh.set_x, sh.fam_z, sh.fam_y, sh.fam_x,
+                                {}, {}, {}});
       c = &L.cls.back();
     }
     c->z.add(a.slot, sh.blocks_z);
@@ -391,7 +512,8 @@ int enqueue_iterations(vpfft_batch* b, const std::vector<BatchLaunch>& bl, const
   size_t k = 0;
   for (const ClassList& c : L.cls) {
     chains.push_back(PassChain{c.set_z, c.set_y, c.set_x, bl[k], bl[k + 1], bl[k + 2],
-                               c.smem_z_r2c, c.smem_z_c2r, c.smem_y, c.smem_x});
+                               c.smem_z_r2c, c.smem_z_c2r, c.smem_y, c.smem_x, c.fam_z, c.fam_y,
+                               c.fam_x});
     k += 3;
   }
   // material and solver constants: those of any iterating slot (a batch admits
@@ -505,6 +627,7 @@ vpfft_status tick(vpfft_batch* b) {
   // 1. admission and the initialisation of the new slots
   std::vector<int> admitted;
   if (vpfft_status s = admit<S>(b, admitted)) return s;
+  if (vpfft_status s = assign_tiles<S>(b, admitted)) return s;
   if (!admitted.empty()) {
     HostList init[2], rm, rms;
     for (int idx : admitted) {
@@ -598,6 +721,8 @@ void free_batch(vpfft_batch* b) {
     if (b->ev_join[a]) cudaEventDestroy(b->ev_join[a]);
   }
   if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+  if (b->ev_t0) cudaEventDestroy(b->ev_t0);
+  if (b->ev_t1) cudaEventDestroy(b->ev_t1);
 }
 
 }  // namespace
@@ -610,7 +735,7 @@ void vpfft_batch_options_default(vpfft_batch_options* o) {
   o->iterations_per_tick = 8;
   o->hbm_budget_bytes = 8LL << 30;
   o->use_graphs = 1;
-  o->pad_ = 0;
+  o->fft_tiles = 2;
 }
 
 vpfft_status vpfft_batch_create(vpfft_precision precision, const vpfft_material* material,
@@ -640,7 +765,8 @@ vpfft_status vpfft_batch_create(vpfft_precision precision, const vpfft_material*
     b->bopt = *bopt;
   else
     vpfft_batch_options_default(&b->bopt);
-  if (b->bopt.max_slots < 1 || b->bopt.max_slots > 65536 || b->bopt.hbm_budget_bytes < 0) {
+  if (b->bopt.max_slots < 1 || b->bopt.max_slots > 65536 || b->bopt.hbm_budget_bytes < 0 ||
+      b->bopt.fft_tiles < -1 || b->bopt.fft_tiles > 2) {
     delete b;
     return bfail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "bad batch options");
   }
@@ -670,6 +796,8 @@ vpfft_status vpfft_batch_create(vpfft_precision precision, const vpfft_material*
   }
   if ((e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming)) != cudaSuccess)
     return bail(e, "event");
+  if ((e = cudaEventCreate(&b->ev_t0)) != cudaSuccess) return bail(e, "event");
+  if ((e = cudaEventCreate(&b->ev_t1)) != cudaSuccess) return bail(e, "event");
   if (b->bopt.hbm_budget_bytes > 0 &&
       (e = cudaMalloc(&b->arena_base, (size_t)b->bopt.hbm_budget_bytes)) != cudaSuccess)
     return bail(e, "arena");
@@ -786,6 +914,16 @@ vpfft_status vpfft_batch_get_info(const vpfft_batch* b, vpfft_batch_info* info) 
   info->arena_bytes_in_use = (int64_t)b->arena.in_use();
   info->arena_bytes = (int64_t)b->arena.size();
   info->admissions_deferred_for_memory = b->deferred;
+  return VPFFT_OK;
+}
+
+vpfft_status vpfft_batch_get_tunings(const vpfft_batch* b, vpfft_tile_tuning* out, int cap,
+                                     int* n_out) {
+  if (!b || !n_out || cap < 0 || (cap > 0 && !out))
+    return bfail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "bad arguments");
+  const int n = std::min(cap, (int)b->tunings.size());
+  for (int i = 0; i < n; ++i) out[i] = b->tunings[i];
+  *n_out = (int)b->tunings.size();
   return VPFFT_OK;
 }
 

@@ -131,15 +131,23 @@ int launch_fft3d(const Spectral<S>& sp, S* real, int ncomp, int mode, cudaStream
 }
 
 template <typename S>
-SpectralShape spectral_shape(const Spectral<S>& sp, int ncomp) {
+SpectralShape spectral_shape(const Spectral<S>& sp, int ncomp, int fam) {
   const PassSet<S>& Z = pass_set<S>(sp.pz);
   const PassSet<S>& Y = pass_set<S>(sp.py);
   const PassSet<S>& X = pass_set<S>(sp.px);
-  const PassSmem<S> sm = pass_smem(sp, Z.btz, Y.bty, X.btk, ncomp);
+  // each axis takes the requested family, or its longest tile
+  auto pick = [fam](const PassSet<S>& P) { return (fam < 0 || fam >= P.nfam) ? P.nfam - 1 : fam; };
   SpectralShape r;
-  r.blocks_z = cdiv(sp.nx * sp.ny, Z.btz) * ncomp;
-  r.blocks_y = cdiv(sp.nh * sp.nx, Y.bty) * ncomp;
-  r.blocks_x = cdiv(sp.nh * sp.ny, X.btk);
+  r.fam_z = pick(Z);
+  r.fam_y = pick(Y);
+  r.fam_x = pick(X);
+  const BatchPasses<S>& bz = Z.fam[r.fam_z];
+  const BatchPasses<S>& by = Y.fam[r.fam_y];
+  const BatchPasses<S>& bx = X.fam[r.fam_x];
+  const PassSmem<S> sm = pass_smem(sp, bz.tz, by.ty, bx.tk, ncomp);
+  r.blocks_z = cdiv(sp.nx * sp.ny, bz.tz) * ncomp;
+  r.blocks_y = cdiv(sp.nh * sp.nx, by.ty) * ncomp;
+  r.blocks_x = cdiv(sp.nh * sp.ny, bx.tk);
   r.smem_z_r2c = sm.z_r2c;
   r.smem_z_c2r = sm.z_c2r;
   r.smem_y = sm.y;
@@ -147,25 +155,29 @@ SpectralShape spectral_shape(const Spectral<S>& sp, int ncomp) {
   r.set_z = &Z;
   r.set_y = &Y;
   r.set_x = &X;
+  r.families = std::max(Z.nfam, std::max(Y.nfam, X.nfam));
   return r;
 }
 
 template <typename S>
 int launch_spectral_chain(const SlotDesc<S>* d, const PassChain& c, cudaStream_t st) {
   if (c.z.blocks <= 0) return 0;
-  const PassSet<S>* Z = static_cast<const PassSet<S>*>(c.set_z);
-  const PassSet<S>* Y = static_cast<const PassSet<S>*>(c.set_y);
-  const PassSet<S>* X = static_cast<const PassSet<S>*>(c.set_x);
-  Z->bz_r2c<<<c.z.blocks, Z->threads, c.smem_z_r2c, st>>>(d, c.z);
-  Y->by_fwd<<<c.y.blocks, Y->threads, c.smem_y, st>>>(d, c.y);
-  X->bx_green<<<c.x.blocks, X->threads_x, c.smem_x, st>>>(d, c.x);
-  Y->by_inv<<<c.y.blocks, Y->threads, c.smem_y, st>>>(d, c.y);
-  Z->bz_c2r<<<c.z.blocks, Z->threads, c.smem_z_c2r, st>>>(d, c.z);
+  const BatchPasses<S>& Z = static_cast<const PassSet<S>*>(c.set_z)->fam[c.fam_z];
+  const BatchPasses<S>& Y = static_cast<const PassSet<S>*>(c.set_y)->fam[c.fam_y];
+  const BatchPasses<S>& X = static_cast<const PassSet<S>*>(c.set_x)->fam[c.fam_x];
+  const int tzy = static_cast<const PassSet<S>*>(c.set_z)->threads;
+  const int tyy = static_cast<const PassSet<S>*>(c.set_y)->threads;
+  const int txx = static_cast<const PassSet<S>*>(c.set_x)->threads_x;
+  Z.z_r2c<<<c.z.blocks, tzy, c.smem_z_r2c, st>>>(d, c.z);
+  Y.y_fwd<<<c.y.blocks, tyy, c.smem_y, st>>>(d, c.y);
+  X.x_green<<<c.x.blocks, txx, c.smem_x, st>>>(d, c.x);
+  Y.y_inv<<<c.y.blocks, tyy, c.smem_y, st>>>(d, c.y);
+  Z.z_c2r<<<c.z.blocks, tzy, c.smem_z_c2r, st>>>(d, c.z);
   return 5;
 }
 
-template SpectralShape spectral_shape<double>(const Spectral<double>&, int);
-template SpectralShape spectral_shape<float>(const Spectral<float>&, int);
+template SpectralShape spectral_shape<double>(const Spectral<double>&, int, int);
+template SpectralShape spectral_shape<float>(const Spectral<float>&, int, int);
 template int launch_spectral_chain<double>(const SlotDesc<double>*, const PassChain&,
                                            cudaStream_t);
 template int launch_spectral_chain<float>(const SlotDesc<float>*, const PassChain&, cudaStream_t);

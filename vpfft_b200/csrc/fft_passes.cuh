@@ -37,11 +37,17 @@ namespace fft {
 // per block, the x pass (two transforms and the Green operator) 128 threads,
 // the settings measured fastest at 256^3.  The generic engine keeps 256
 // threads and its short tiles.
-// A batch always takes the long tiles: its launches have blocks enough.
-template <typename S, class E, bool kBatch = false>
+// kEl != 0 selects a batched tile family: about kEl complex values per buffer
+// (512, 1024 or 2048, at most the long tile), chosen by the batch's options or
+// its autotuner.  A tile only groups lines: every line goes through the same
+// arithmetic whatever the family (FP64 results are the same bit for bit; the
+// FP32 kernels of different families are compiled separately and their last
+// bits can differ).
+template <typename S, class E, int kEl = 0>
 struct Tiles {
   static constexpr bool kF32 = sizeof(S) == 4;
-  static constexpr int kElems = (E::kN >= 64 || kBatch) ? (kF32 ? 2048 : 1024) : 512;
+  static constexpr int kLong = kF32 ? 2048 : 1024;
+  static constexpr int kElems = kEl ? (kEl < kLong ? kEl : kLong) : (E::kN >= 64 ? kLong : 512);
   static constexpr int kThreads = E::kN ? (kF32 ? 256 : 128) : 256;  // z and y passes
   static constexpr int kThreadsX = E::kN ? 128 : 256;                // x pass
   // x-pass blocks per SM the registers are capped for: FP32 at 6 (85
@@ -52,6 +58,18 @@ struct Tiles {
   static constexpr int kY = E::kN ? cmax(1, kElems / E::kN) : (sizeof(S) == 4 ? 16 : 8);
   static constexpr int kX = E::kN ? cmax(1, kElems / (5 * E::kN)) : (sizeof(S) == 4 ? 4 : 2);
 };
+// Batched tile families of an engine: 512, 1024 (and 2048 in FP32) complex
+// values per buffer for the fixed engines up to 96 points; one (the long
+// tile) for longer lines and for the generic engine, whose tiles do not
+// depend on it.
+template <typename S, class E>
+constexpr int batch_families() {
+  return (E::kN == 0 || E::kN > 96) ? 1 : (sizeof(S) == 4 ? 3 : 2);
+}
+template <typename S, class E>
+constexpr int batch_family_elems(int f) {
+  return batch_families<S, E>() == 1 ? Tiles<S, E>::kLong : (512 << f);
+}
 
 
 // Copy of nrows rows of len elements: warp w takes rows w, w + nwarps, ...;
@@ -397,11 +415,11 @@ __device__ __forceinline__ const SlotDesc<S>* batch_pass_setup(const SlotDesc<S>
   return d;
 }
 
-template <typename S, class E>
-__global__ void __launch_bounds__(Tiles<S, E, true>::kThreads)
+template <typename S, class E, int kEl>
+__global__ void __launch_bounds__(Tiles<S, E, kEl>::kThreads)
     k_pass_z_r2c_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
   using T = typename CX<S>::T;
-  using TL = Tiles<S, E, true>;
+  using TL = Tiles<S, E, kEl>;
   __shared__ SlotFft<S> sm;
   int lb;
   const SlotDesc<S>* d = batch_pass_setup(desc, bl, false, &sm, &lb);
@@ -413,11 +431,11 @@ __global__ void __launch_bounds__(Tiles<S, E, true>::kThreads)
                             reinterpret_cast<const T*>(fs.twz), fs.nx, fs.ny, fs.nh, lb - c * gt,
                             c);
 }
-template <typename S, class E>
-__global__ void __launch_bounds__(Tiles<S, E, true>::kThreads)
+template <typename S, class E, int kEl>
+__global__ void __launch_bounds__(Tiles<S, E, kEl>::kThreads)
     k_pass_z_c2r_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
   using T = typename CX<S>::T;
-  using TL = Tiles<S, E, true>;
+  using TL = Tiles<S, E, kEl>;
   __shared__ SlotFft<S> sm;
   int lb;
   const SlotDesc<S>* d = batch_pass_setup(desc, bl, false, &sm, &lb);
@@ -430,11 +448,11 @@ __global__ void __launch_bounds__(Tiles<S, E, true>::kThreads)
                             reinterpret_cast<const T*>(fs.twz), fs.nx, fs.ny, fs.nh, scale,
                             lb - c * gt, c);
 }
-template <int SIGN, typename S, class E>
-__global__ void __launch_bounds__(Tiles<S, E, true>::kThreads)
+template <int SIGN, typename S, class E, int kEl>
+__global__ void __launch_bounds__(Tiles<S, E, kEl>::kThreads)
     k_pass_y_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
   using T = typename CX<S>::T;
-  using TL = Tiles<S, E, true>;
+  using TL = Tiles<S, E, kEl>;
   __shared__ SlotFft<S> sm;
   int lb;
   const SlotDesc<S>* d = batch_pass_setup(desc, bl, false, &sm, &lb);
@@ -447,12 +465,11 @@ __global__ void __launch_bounds__(Tiles<S, E, true>::kThreads)
   pass_y_body<SIGN, S, E, TL>(in, out, d->sp.py, fs.dnx, reinterpret_cast<const T*>(fs.twy),
                               fs.nx, fs.nh, lb - c * gt, c);
 }
-template <typename S, class E>
-__global__ void __launch_bounds__(Tiles<S, E, true>::kThreadsX,
-                                  512 / Tiles<S, E, true>::kThreadsX)
+template <typename S, class E, int kEl>
+__global__ void __launch_bounds__(Tiles<S, E, kEl>::kThreadsX, 512 / Tiles<S, E, kEl>::kThreadsX)
     k_pass_x_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
   using T = typename CX<S>::T;
-  using TL = Tiles<S, E, true>;
+  using TL = Tiles<S, E, kEl>;
   __shared__ SlotFft<S> sm;
   int lb;
   const SlotDesc<S>* d = batch_pass_setup(desc, bl, true, &sm, &lb);
@@ -463,12 +480,21 @@ __global__ void __launch_bounds__(Tiles<S, E, true>::kThreadsX,
 }
 
 // ---------------------------------------------------------------- entry table
+// The batched passes of one tile family.
+template <typename S>
+struct BatchPasses {
+  int tz, ty, tk;  // real z-lines, y-lines and ky-lines (per component) per block
+  void (*z_r2c)(const SlotDesc<S>*, const BatchLaunch);
+  void (*z_c2r)(const SlotDesc<S>*, const BatchLaunch);
+  void (*y_fwd)(const SlotDesc<S>*, const BatchLaunch);
+  void (*y_inv)(const SlotDesc<S>*, const BatchLaunch);
+  void (*x_green)(const SlotDesc<S>*, const BatchLaunch);
+};
 template <typename S>
 struct PassSet {
   using T = typename CX<S>::T;
   int threads, threads_x;  // z and y passes, x pass
   int tz, ty, tk;     // real z-lines, y-lines and ky-lines (per component) per block
-  int btz, bty, btk;  // the same for the batched kernels
   void (*z_r2c)(const S*, T*, LinePlan, FastDiv, const T*, int, int, int, const IterCtrl*);
   void (*z_c2r)(const T*, S*, LinePlan, FastDiv, const T*, int, int, int, S, const IterCtrl*);
   void (*y_fwd)(const T*, T*, LinePlan, FastDiv, const T*, int, int, const IterCtrl*);
@@ -477,11 +503,8 @@ struct PassSet {
   void (*x_inv)(T*, LinePlan, FastDiv, const T*, GreenParams<S>, int, int, int, const IterCtrl*);
   void (*x_green)(T*, LinePlan, FastDiv, const T*, GreenParams<S>, int, int, int,
                   const IterCtrl*);
-  void (*bz_r2c)(const SlotDesc<S>*, const BatchLaunch);
-  void (*bz_c2r)(const SlotDesc<S>*, const BatchLaunch);
-  void (*by_fwd)(const SlotDesc<S>*, const BatchLaunch);
-  void (*by_inv)(const SlotDesc<S>*, const BatchLaunch);
-  void (*bx_green)(const SlotDesc<S>*, const BatchLaunch);
+  int nfam;                // batched tile families; the last is the long tile
+  BatchPasses<S> fam[3];
 };
 
 // Dynamic shared memory limit = the opt-in maximum minus the kernel's static part.
@@ -493,6 +516,30 @@ inline void optin_rest(K kern, int total) {
                        total - (int)a.sharedSizeBytes);
 }
 
+template <typename S, class E, int kEl>
+BatchPasses<S> make_batch_passes(int smem) {
+  using TL = Tiles<S, E, kEl>;
+  static_assert(TL::kThreads == Tiles<S, E>::kThreads &&
+                    TL::kThreadsX == Tiles<S, E>::kThreadsX,
+                "batched and single kernels share the thread counts");
+  BatchPasses<S> q;
+  q.tz = TL::kZ;
+  q.ty = TL::kY;
+  q.tk = TL::kX;
+  q.z_r2c = k_pass_z_r2c_batch<S, E, kEl>;
+  q.z_c2r = k_pass_z_c2r_batch<S, E, kEl>;
+  q.y_fwd = k_pass_y_batch<-1, S, E, kEl>;
+  q.y_inv = k_pass_y_batch<1, S, E, kEl>;
+  q.x_green = k_pass_x_batch<S, E, kEl>;
+  // the batched kernels hold the slot's descriptor in static shared memory
+  optin_rest(q.z_r2c, smem);
+  optin_rest(q.z_c2r, smem);
+  optin_rest(q.y_fwd, smem);
+  optin_rest(q.y_inv, smem);
+  optin_rest(q.x_green, smem);
+  return q;
+}
+
 template <typename S, class E>
 PassSet<S> make_pass_set() {
   using Ti = Tiles<S, E>;
@@ -502,12 +549,6 @@ PassSet<S> make_pass_set() {
   p.tz = Ti::kZ;
   p.ty = Ti::kY;
   p.tk = Ti::kX;
-  p.btz = Tiles<S, E, true>::kZ;
-  p.bty = Tiles<S, E, true>::kY;
-  p.btk = Tiles<S, E, true>::kX;
-  static_assert(Tiles<S, E, true>::kThreads == Ti::kThreads &&
-                    Tiles<S, E, true>::kThreadsX == Ti::kThreadsX,
-                "batched and single kernels share the thread counts");
   p.z_r2c = k_pass_z_r2c<S, E>;
   p.z_c2r = k_pass_z_c2r<S, E>;
   p.y_fwd = k_pass_y<-1, S, E>;
@@ -515,11 +556,6 @@ PassSet<S> make_pass_set() {
   p.x_fwd = k_pass_x<0, S, E>;
   p.x_inv = k_pass_x<1, S, E>;
   p.x_green = k_pass_x<2, S, E>;
-  p.bz_r2c = k_pass_z_r2c_batch<S, E>;
-  p.bz_c2r = k_pass_z_c2r_batch<S, E>;
-  p.by_fwd = k_pass_y_batch<-1, S, E>;
-  p.by_inv = k_pass_y_batch<1, S, E>;
-  p.bx_green = k_pass_x_batch<S, E>;
   const int s = 227 * 1024;
   optin_rest(p.z_r2c, s);
   optin_rest(p.z_c2r, s);
@@ -528,12 +564,11 @@ PassSet<S> make_pass_set() {
   optin_rest(p.x_fwd, s);
   optin_rest(p.x_inv, s);
   optin_rest(p.x_green, s);
-  // the batched kernels hold the slot's descriptor in static shared memory
-  optin_rest(p.bz_r2c, s);
-  optin_rest(p.bz_c2r, s);
-  optin_rest(p.by_fwd, s);
-  optin_rest(p.by_inv, s);
-  optin_rest(p.bx_green, s);
+  constexpr int nf = batch_families<S, E>();
+  p.nfam = nf;
+  p.fam[0] = make_batch_passes<S, E, batch_family_elems<S, E>(0)>(s);
+  if constexpr (nf > 1) p.fam[1] = make_batch_passes<S, E, batch_family_elems<S, E>(1)>(s);
+  if constexpr (nf > 2) p.fam[2] = make_batch_passes<S, E, batch_family_elems<S, E>(2)>(s);
   return p;
 }
 

@@ -214,26 +214,32 @@ int launch_ref_medium_batch(const SlotDesc<S>* d, const BatchLaunch& bl,
                             const BatchLaunch& bl_slots, cudaStream_t st);
 template <typename S>
 int launch_post_batch(const SlotDesc<S>* d, const BatchLaunch& bl, cudaStream_t st);
-// Blocks, dynamic shared memory and line engine ("pass set", chosen by the
-// axis length) of the five batched FFT passes of one RVE.
+// Blocks, dynamic shared memory, line engine ("pass set", chosen by the axis
+// length) and tile family of the five batched FFT passes of one RVE.  fam:
+// the tile family (0, 1, 2: about 512, 1024, 2048 complex values per buffer),
+// clamped per axis to the families its engine has; -1 = the longest tiles.
 struct SpectralShape {
   int blocks_z, blocks_y, blocks_x;
   size_t smem_z_r2c, smem_z_c2r, smem_y, smem_x;
   const void* set_z;
   const void* set_y;
   const void* set_x;
+  int fam_z, fam_y, fam_x;
+  int families;  // distinct families over the three axes (the candidates worth timing)
 };
 template <typename S>
-SpectralShape spectral_shape(const Spectral<S>& sp, int ncomp);
-// The RVEs of a batch whose three axes have the same line engines: one launch
-// per pass over all of them (the largest shared memory among them).  Chains
-// of different classes are independent and may run on different streams.
+SpectralShape spectral_shape(const Spectral<S>& sp, int ncomp, int fam = -1);
+// The RVEs of a batch whose three axes have the same line engines and tile
+// families: one launch per pass over all of them (the largest shared memory
+// among them).  Chains of different classes are independent and may run on
+// different streams.
 struct PassChain {
   const void* set_z;
   const void* set_y;
   const void* set_x;
   BatchLaunch z, y, x;
   size_t smem_z_r2c, smem_z_c2r, smem_y, smem_x;
+  int fam_z, fam_y, fam_x;
 };
 template <typename S>
 int launch_spectral_chain(const SlotDesc<S>* d, const PassChain& c, cudaStream_t st);
