@@ -24,7 +24,12 @@ The metric is voxel-iterations per second (voxels x iterations / time).
             copied back inside the timed region;
   fp64   -- the all-FP64 GPU path on the same workload;
   cpu_baseline -- the reference's own code (oracle/_ref, else the C
-            restatement) on a bounded sample of the same workload on the host.
+            restatement) on a bounded sample of the same workload on the host;
+  batched / serving -- 256 RVEs of 16-64^3 in one batch, and a Poisson
+            request stream served by continuous batching (host wall clock:
+            the batch synchronises every tick), each with a cpu_baseline of
+            the reference on every host core, modelled from its measured
+            per-edge increment costs (full CPU solves would take hours).
 
 Multi-GPU: one process per GPU (torchrun); every rank solves its own replica
 RVE (weak scaling, no collective in the data path); the elapsed time is the
@@ -341,6 +346,8 @@ def batched_arm(n_rves: int) -> dict:
         "timing": "host wall clock around submit + run (the batch synchronises every tick)",
         "config": ("edges uniform {16,32,48,64}, grains uniform [8,200], random traceless L, "
                    "n=10, gdot0=1, CRSS=1, max 100 iterations, eps 1e-5, dt 0.005"),
+        # for the CPU comparison (removed before printing)
+        "_cpu_model": {"edges": [e for e, _ in specs], "iters": [int(i) for i in iters]},
     }
 
 
@@ -353,9 +360,10 @@ def serving_arm(n_requests: int) -> dict:
     from vpfft_b200 import serving
 
     budget = 2 << 30
+    sizes, weights = [32, 48, 64, 96], [0.4, 0.3, 0.2, 0.1]
     b = vp.Batch("mixed", material=material_n10(), max_slots=64, iterations_per_tick=4,
                  hbm_budget_bytes=budget)
-    pool = serving.rve_pool(b, [32, 48, 64, 96], [0.4, 0.3, 0.2, 0.1], 64, SEED)
+    pool = serving.rve_pool(b, sizes, weights, 64, SEED)
     serving.serve(b, pool, serving.poisson_trace(32, 500.0, len(pool), SEED + 1))  # warm-up
     trace = serving.poisson_trace(n_requests, 500.0, len(pool), SEED + 2)
     r = serving.serve(b, pool, trace)
@@ -376,6 +384,11 @@ def serving_arm(n_requests: int) -> dict:
         "config": ("Poisson arrivals mean 500/s, pool of 64 RVEs, edges {32,48,64,96} weights "
                    "0.4/0.3/0.2/0.1, grains uniform [8,200], random traceless L per request, "
                    "n=10, mixed, max 100 iterations, eps 1e-5, dt 0.005"),
+        # for the CPU comparison (removed before printing)
+        "_cpu_model": {"trace": trace,
+                       "edges": [e for e, _ in serving.pool_specs(sizes, weights, 64, SEED)],
+                       "iters": [res.iterations if res is not None else 100
+                                 for res in r["results"]]},
     }
 
 
@@ -436,6 +449,124 @@ def cpu_baseline_ours():
             "sample": (f"{n_side}^3 sample of the workload (same grain size and material), "
                        f"{timed} timed fixed-point iterations after {warm} warm-up, one "
                        "single-threaded process")}
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_increment_costs(edges, k_iters: int = 2):
+    """The reference's cost of one increment (RunSingleStrainStep) of one RVE
+    per edge length on the host: one single-threaded process per edge, run
+    concurrently, each with eps = 0 so that it takes exactly k_iters
+    fixed-point iterations (the batched/serving material, n = 10, and a
+    random traceless velocity gradient).  Returns {edge: (fixed_s, iter_s)}:
+    iter_s = the last iteration's time (from the harness's timestamps at each
+    iteration's forward FFT), fixed_s = the increment's time outside its
+    iterations (initialisation, reference medium, texture and hardening)."""
+    import shutil
+
+    from oracle import refio
+    from vpfft_b200 import fixtures
+
+    binary, kind = ref_binary()
+    m = refio.Material.uniform(1.0, 10, 1.0, 0.5, 20.0, 1.0)
+    rng = np.random.default_rng(SEED + 9)
+    tmp = tempfile.mkdtemp(prefix="vpfft_cpu_rve_")
+    runs = []
+    try:
+        for e in edges:
+            R = fixtures.polycrystal(e, e, e, 104, SEED + 11 * e)
+            ed = fixtures.edot_from_matrix(fixtures.random_traceless_velocity_gradient(rng))
+            case = refio.Case((e,) * 3, R, np.zeros((e ** 3, 5)), np.ones(12), m, ed, nsteps=1,
+                              max_iter=k_iters, dt=0.005, eps=0.0)
+            d = os.path.join(tmp, str(e))
+            os.makedirs(d)
+            refio.write_input(os.path.join(d, "input.bin"), case)
+            runs.append((e, d, subprocess.Popen([binary, os.path.join(d, "input.bin"), d,
+                                                 "--quiet"], stdout=subprocess.DEVNULL,
+                                                stderr=subprocess.PIPE)))
+        costs = {}
+        for e, d, pr in runs:
+            _, err = pr.communicate()
+            if pr.returncode != 0:
+                raise RuntimeError(f"reference failed at {e}^3: {err.decode()[-300:]}")
+            t_inc = float(np.fromfile(os.path.join(d, "step_seconds.bin"))[0])
+            ft = np.fromfile(os.path.join(d, "fwd_times.bin"))
+            t_it = float(ft[k_iters] - ft[k_iters - 1])
+            costs[e] = (max(0.0, t_inc - k_iters * t_it), t_it)
+    finally:
+        for _, _, pr in runs:
+            if pr.poll() is None:
+                pr.kill()
+        shutil.rmtree(tmp, ignore_errors=True)
+    return costs, kind, binary
+
+
+def lpt_makespan(times, workers: int) -> float:
+    """Makespan of independent jobs on `workers` identical workers, longest
+    job first onto the least-loaded worker."""
+    import heapq
+
+    loads = [0.0] * max(1, int(workers))
+    for t in sorted(times, reverse=True):
+        heapq.heapreplace(loads, loads[0] + t)
+    return max(loads)
+
+
+def cpu_rve_baselines(models: dict) -> dict:
+    """The reference on the host cores beside the batched and serving arms.
+    Full solves of every RVE would take hours of CPU time (a 96^3 increment of
+    100 iterations takes ~10 min on one core), so each solve's time is formed
+    from measured per-edge costs: fixed_s + iterations x iter_s, with the
+    iteration count of the same solve on the GPU.  Batched: the solves as
+    independent single-threaded processes on every host core (longest first,
+    makespan).  Serving: the same Poisson trace replayed through a FIFO pool of
+    one single-threaded solver per core (serving.fifo_replay)."""
+    from vpfft_b200 import serving
+
+    edges = sorted({int(e) for mdl in models.values() for e in mdl["edges"]})
+    k_iters = 2
+    costs, kind, binary = cpu_increment_costs(edges, k_iters)
+    cores = host_cores()
+
+    def solve_s(e, iters):
+        fixed, it = costs[int(e)]
+        return fixed + iters * it
+
+    how = (f"the reference ({os.path.relpath(binary, ROOT)}) timed per RVE edge: one increment "
+           f"of one RVE per edge {edges} with {k_iters} fixed-point iterations (eps 0), one "
+           "single-threaded process per edge, run concurrently; a solve's time = the measured "
+           "cost outside the iterations + its iteration count (that of the same solve on the "
+           "GPU) x the measured iteration time")
+    per_edge = {str(e): {"fixed_s": c[0], "iteration_s": c[1]} for e, c in costs.items()}
+    out = {}
+    if "batched" in models:
+        bm = models["batched"]
+        times = [solve_s(e, it) for e, it in zip(bm["edges"], bm["iters"])]
+        mk = lpt_makespan(times, cores)
+        out["batched"] = {
+            "value": len(times) / mk, "unit": "solves/s", "cores": cores, "kind": kind,
+            "method": "modelled from measured per-edge costs",
+            "sample": how + f"; {len(times)} solves on {cores} cores, longest first (makespan "
+                            f"{mk:.1f} s)",
+            "per_edge": per_edge}
+    if "serving" in models:
+        sm = models["serving"]
+        trace = sm["trace"]
+        svc = [solve_s(sm["edges"][req.rve], it) for req, it in zip(trace, sm["iters"])]
+        rep = serving.fifo_replay(trace, svc, cores)
+        out["serving"] = {
+            "value": rep["throughput"], "unit": "solves/s", "cores": cores, "kind": kind,
+            "latency_p50_s": rep["latency_p50_s"], "latency_p99_s": rep["latency_p99_s"],
+            "method": "modelled from measured per-edge costs",
+            "sample": how + f"; the same {len(trace)}-request trace through a FIFO pool of "
+                            f"{cores} single-threaded solvers",
+            "per_edge": per_edge}
+    return out
 
 
 # ------------------------------------------------------------------ distributed helpers
@@ -653,8 +784,16 @@ def main(argv=None):
         line["batched"] = batched_arm(args.batch_rves)
     if ws == 1 and not args.no_serving:
         line["serving"] = serving_arm(args.serve_requests)
+    models = {k: line[k].pop("_cpu_model") for k in ("batched", "serving") if k in line}
     if rank == 0 and ws == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline_ours()
+        if models:
+            try:
+                for k, v in cpu_rve_baselines(models).items():
+                    line[k]["cpu_baseline"] = v
+            except (RuntimeError, OSError, ValueError) as exc:
+                for k in models:
+                    line[k]["cpu_baseline"] = {"unavailable": f"{type(exc).__name__}: {exc}"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if _dist is not None:

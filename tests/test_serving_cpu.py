@@ -1,4 +1,6 @@
-"""Host logic of the serving loop (no GPU): the synthetic arrival trace."""
+"""Host logic of the serving loop and of the CPU comparison (no GPU): the
+synthetic arrival trace, the RVE pool draws, the FIFO replay and the
+longest-first packing of independent solves."""
 import numpy as np
 
 from vpfft_b200 import fixtures, serving
@@ -21,3 +23,38 @@ def test_poisson_trace_statistics(lib):
     # seeded: the same trace twice
     tr2 = serving.poisson_trace(4000, 500.0, 64, seed=3)
     assert all(a.t_arrival == b.t_arrival and a.rve == b.rve for a, b in zip(tr, tr2))
+
+
+def test_pool_specs_seeded_and_weighted(lib):
+    a = serving.pool_specs([32, 48, 64, 96], [0.4, 0.3, 0.2, 0.1], 2000, seed=5)
+    assert a == serving.pool_specs([32, 48, 64, 96], [0.4, 0.3, 0.2, 0.1], 2000, seed=5)
+    edges = np.array([e for e, _ in a])
+    grains = np.array([g for _, g in a])
+    for e, w in ((32, 0.4), (48, 0.3), (64, 0.2), (96, 0.1)):
+        assert abs(np.mean(edges == e) - w) < 0.04
+    assert grains.min() >= 8 and grains.max() <= 200
+
+
+def test_fifo_replay_hand_case(lib):
+    def req(t, rve):
+        return serving.Request(t, rve, np.zeros((3, 3)))
+
+    # two workers, unit service times; the third request waits for its RVE's
+    # first increment and for a free worker
+    tr = [req(0.0, 0), req(0.1, 1), req(0.2, 0), req(0.3, 2)]
+    r = serving.fifo_replay(tr, [1.0, 1.0, 1.0, 1.0], 2)
+    np.testing.assert_allclose(r["latency_max_s"], 1.8)
+    np.testing.assert_allclose(r["latency_p50_s"], np.quantile([1.0, 1.0, 1.8, 1.8], 0.5))
+    np.testing.assert_allclose(r["throughput"], 4 / 2.1)
+    # the same RVE twice: the second increment starts when the first ends,
+    # even with a worker free
+    r = serving.fifo_replay([req(0.0, 3), req(0.0, 3)], [1.0, 1.0], 2)
+    np.testing.assert_allclose(r["latency_max_s"], 2.0)
+
+
+def test_lpt_makespan(lib):
+    import bench
+
+    assert bench.lpt_makespan([4.0, 3.0, 2.0, 1.0], 2) == 5.0
+    assert bench.lpt_makespan([1.0] * 10, 3) == 4.0
+    assert bench.lpt_makespan([2.0, 7.0], 16) == 7.0

@@ -39,18 +39,56 @@ def poisson_trace(n: int, rate: float, n_rves: int, seed: int) -> list[Request]:
     return out
 
 
+def pool_specs(sizes, weights, n: int, seed: int, grains=(8, 200)) -> list[tuple[int, int]]:
+    """(edge, grain count) of the n RVEs of a pool: edges drawn from `sizes`
+    with `weights`, grain counts uniform in `grains` (seeded)."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for _ in range(n):
+        s = int(rng.choice(sizes, p=np.asarray(weights) / np.sum(weights)))
+        ng = int(rng.integers(grains[0], grains[1] + 1))
+        specs.append((s, ng))
+    return specs
+
+
 def rve_pool(batch: Batch, sizes, weights, n: int, seed: int, grains=(8, 200)):
     """n grids with sizes drawn from `sizes` (edge lengths) with `weights`,
     seeded Voronoi microstructures with a grain count uniform in `grains`."""
-    rng = np.random.default_rng(seed)
     pool = []
-    for k in range(n):
-        s = int(rng.choice(sizes, p=np.asarray(weights) / np.sum(weights)))
-        ng = int(rng.integers(grains[0], grains[1] + 1))
+    for k, (s, ng) in enumerate(pool_specs(sizes, weights, n, seed, grains)):
         g = batch.new_grid(s, s, s)
         g.SendDataAndInitialize(fixtures.polycrystal(s, s, s, ng, seed * 1000 + k))
         pool.append(g)
     return pool
+
+
+def fifo_replay(trace: list[Request], service_s, workers: int) -> dict:
+    """Latency and throughput of a trace served by `workers` single-threaded
+    solvers taking requests in arrival order, each request on the earliest
+    free worker but not before the previous request on its RVE has finished
+    (an RVE's state carries from one increment to the next).  service_s[k]
+    is request k's solve time in seconds."""
+    import heapq
+
+    free = [0.0] * max(1, int(workers))
+    rve_free: dict[int, float] = {}
+    latency = np.zeros(len(trace))
+    last = 0.0
+    for k, r in enumerate(trace):
+        w = heapq.heappop(free)
+        start = max(r.t_arrival, w, rve_free.get(r.rve, 0.0))
+        done = start + float(service_s[k])
+        heapq.heappush(free, done)
+        rve_free[r.rve] = done
+        latency[k] = done - r.t_arrival
+        last = max(last, done)
+    span = last - trace[0].t_arrival
+    return {
+        "throughput": len(trace) / span if span > 0 else float("inf"),
+        "latency_p50_s": float(np.quantile(latency, 0.5)),
+        "latency_p99_s": float(np.quantile(latency, 0.99)),
+        "latency_max_s": float(latency.max()),
+    }
 
 
 def serve(batch: Batch, pool, trace: list[Request], max_iter: int = 100, dt: float = 0.005,
