@@ -226,7 +226,9 @@ vpfft_status vpfft_solve_constrained_constitutive(int n, const double *stress0,
  * as long as the library; larger n returns VPFFT_ERR_UNSUPPORTED_SIZE.  The
  * first call on each device looks up that array's address: make it before any
  * stream capture begins.  Calls share the array, so they are serialised by a
- * process-wide lock (overlapping calls would otherwise race on it).
+ * process-wide lock (overlapping calls would otherwise race on it).  A call
+ * waits for its own work on the legacy default stream, not for the whole
+ * device.
  * not_converged (may be NULL) gets the number of points whose NR error is not
  * below eps. */
 #define VPFFT_NOALLOC_MAX_POINTS 4096

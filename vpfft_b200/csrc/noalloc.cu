@@ -20,7 +20,12 @@
 //    in time would race on it: the entry point holds a process-wide lock for
 //    the whole call, and concurrent callers run one after another;
 //  * the array keeps the previous call's contents; the only value that must
-//    start at zero (the count of non-converged points) is cleared each call.
+//    start at zero (the count of non-converged points) is cleared each call;
+//  * the call waits for its own work on the legacy default stream, not for
+//    the whole device; it does not return until the results are on the host.
+//  * the looked-up address belongs to the device's primary context: after a
+//    cudaDeviceReset the library (its grids, batches and this entry point)
+//    must not be used again in the process.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -146,7 +151,9 @@ extern "C" vpfft_status vpfft_solve_constrained_constitutive_noalloc(
   NA_CK(cudaGetLastError());
   k_count_not_converged<<<(n + 255) / 256, 256>>>(d_err, n, eps, d_count);
   NA_CK(cudaGetLastError());
-  NA_CK(cudaDeviceSynchronize());
+  // the copies, the solve and the count all ran on the legacy default stream:
+  // wait for that stream only, not for the caller's own (non-blocking) streams
+  NA_CK(cudaStreamSynchronize(0));
   NA_CK(cudaMemcpy(out, d_out, b5, cudaMemcpyDeviceToHost));
   if (nr_error) NA_CK(cudaMemcpy(nr_error, d_err, sizeof(double) * n, cudaMemcpyDeviceToHost));
   if (not_converged) {
