@@ -464,13 +464,13 @@ int launch_crss_broadcast(S* dst, long long n, const double crss[kNS], cudaStrea
 }
 
 // ============================================================== Solvers batch (testing)
-__device__ __forceinline__ void load_schmid(const double* schmid, int v, double m[kNS][5]) {
+__device__ __forceinline__ void load_schmid(const double* schmid, long long v, double m[kNS][5]) {
 #pragma unroll
   for (int k = 0; k < kNS; ++k)
 #pragma unroll
     for (int c = 0; c < 5; ++c) m[k][c] = schmid[(long long)v * 60 + k * 5 + c];
 }
-__device__ __forceinline__ void load_crss_v(const double* crss, int v, double tau[kNS]) {
+__device__ __forceinline__ void load_crss_v(const double* crss, long long v, double tau[kNS]) {
 #pragma unroll
   for (int k = 0; k < kNS; ++k) tau[k] = crss[(long long)v * kNS + k];
 }
@@ -483,7 +483,7 @@ struct Mat25 {
 
 __global__ void k_solvers_apply(int n, const double* s_in, const double* schmid,
                                 const double* crss, MaterialParams mp, double* out) {
-  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= n) return;
   double m[kNS][5], tau[kNS], s[5], e[5];
   load_schmid(schmid, v, m);
@@ -494,7 +494,7 @@ __global__ void k_solvers_apply(int n, const double* s_in, const double* schmid,
 }
 __global__ void k_solvers_sachs(int n, const double* schmid, const double* crss, Vec5 edot,
                                 double* out) {
-  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= n) return;
   double m[kNS][5], tau[kNS], g[5];
   load_schmid(schmid, v, m);
@@ -503,7 +503,7 @@ __global__ void k_solvers_sachs(int n, const double* schmid, const double* crss,
   for (int c = 0; c < 5; ++c) out[v * 5 + c] = g[c];
 }
 __global__ void k_solvers_schmid(int n, const double* R, double* out) {
-  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= n) return;
   double r[9], m[kNS][5];
   for (int k = 0; k < 9; ++k) r[k] = R[(long long)v * 9 + k];
@@ -514,7 +514,7 @@ __global__ void k_solvers_schmid(int n, const double* R, double* out) {
 template <typename R>
 __global__ void k_green_batch(int n, const int32_t* kidx, GreenParams<R> gp, const double* phat,
                               double* dhat) {
-  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= n) return;
   R pre[5], pim[5];
   for (int c = 0; c < 5; ++c) {

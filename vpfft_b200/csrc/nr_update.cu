@@ -451,10 +451,10 @@ __global__ void __launch_bounds__(kVoxelBlock, 3)
   constexpr int bs = kVoxelBlock;  // every launch of these kernels uses kVoxelBlock threads
   double* msm = reinterpret_cast<double*>(nr_smem) + threadIdx.x;
   double* tsm = msm + 60 * bs;
-  const int v = blockIdx.x * bs + threadIdx.x;
+  const long long v = (long long)blockIdx.x * bs + threadIdx.x;  // 64-bit: v * 60 below
   if (v >= n) return;
-  for (int k = 0; k < 60; ++k) msm[k * bs] = schmid[(long long)v * 60 + k];
-  for (int q = 0; q < kNS; ++q) tsm[q * bs] = 1.0 / crss[(long long)v * kNS + q];
+  for (int k = 0; k < 60; ++k) msm[k * bs] = schmid[v * 60 + k];
+  for (int q = 0; q < kNS; ++q) tsm[q * bs] = 1.0 / crss[v * kNS + q];
   double s[5];
   for (int c = 0; c < 5; ++c) s[c] = s0[v * 5 + c];
   bool capped;
