@@ -722,6 +722,23 @@ def main(argv=None):
                       "achieved_gbs": it_bytes / (ms / args.steps * 1e-3) / 1e9,
                       "frac": it_bytes / (ms / args.steps * 1e-3) / 1e9 / hbm},
     }
+    if (args.precision, dom) in WARP_INST_PER_VOXEL:
+        # the bound the NR sweep actually meets: instruction issue (four
+        # schedulers per SM, one warp instruction per cycle each)
+        import torch
+
+        sms = torch.cuda.get_device_properties(0).multi_processor_count
+        clk = main_res["clocks"].get("sm_mhz") or main_res["clocks"].get("sm_max_mhz") or 1965.0
+        wpv = WARP_INST_PER_VOXEL[(args.precision, dom)]
+        achieved_i = wpv * N / (kernels[dom]["avg_ms"] * 1e-3)
+        peak_i = sms * 4 * clk * 1e6
+        roofline["issue"] = {
+            "bound": "instruction issue", "achieved": achieved_i / 1e9, "peak": peak_i / 1e9,
+            "unit": "G warp-instructions/s", "frac": achieved_i / peak_i,
+            "warp_instructions_per_voxel": wpv, "sm_mhz": clk, "sms": sms,
+            "source": ("smsp__inst_executed.sum of one launch at 192^3 per voxel (ncu), x the "
+                       "voxel count, / the kernel's CUDA-event duration; peak = SMs x 4 "
+                       "schedulers x the sampled SM clock")}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -806,6 +823,10 @@ def main(argv=None):
 # profiles/k_nr_update_192cubed_mixed.md; the kernel's traffic is proportional to
 # the voxel count (it streams each voxel's fields once), so it scales to 256^3.
 TRAFFIC_PER_VOXEL: dict = {("mixed", "nr_update"): (680.249088e6 + 380.631808e6) / 192 ** 3}
+# Warp instructions per voxel of one launch (smsp__inst_executed.sum divided by
+# the voxel count) from the same capture; the per-voxel instruction count does
+# not depend on the grid size (each voxel's solve is independent of it).
+WARP_INST_PER_VOXEL: dict = {("mixed", "nr_update"): 0.774e9 / 192 ** 3}
 
 
 if __name__ == "__main__":
