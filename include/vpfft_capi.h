@@ -149,6 +149,19 @@ vpfft_status vpfft_grid_set_crss(vpfft_grid *g, const double *crss);
 vpfft_status vpfft_grid_get_field(vpfft_grid *g, vpfft_field which, double *dst);
 /* Write a field from a host buffer (snapshot/restore). */
 vpfft_status vpfft_grid_set_field(vpfft_grid *g, vpfft_field which, const double *src);
+/* Checkpoint of a whole grid.  The reference's MaterialGrid has none: its only
+ * saved state is the text pair WriteRandomMaterial / ReadRandomMaterial
+ * (UnitTester.cpp:116-167: orientation and stress).  A snapshot holds every
+ * state a later call reads -- stress, Lagrange multiplier, orientation,
+ * polarization, accumulated shear, per-voxel CRSS once hardening has run,
+ * voxel lengths, L0 and the last macroscopic strain rate -- as FP64 (FP32
+ * fields widen exactly), so a grid restored from it continues bit for bit as
+ * the original would.  vpfft_grid_snapshot_size gives the bytes (a header plus
+ * 25 or 37 doubles per voxel); vpfft_grid_restore accepts a snapshot of a
+ * grid of the same dimensions and precision only. */
+vpfft_status vpfft_grid_snapshot_size(const vpfft_grid *g, size_t *bytes);
+vpfft_status vpfft_grid_snapshot(vpfft_grid *g, void *buf, size_t cap);
+vpfft_status vpfft_grid_restore(vpfft_grid *g, const void *buf, size_t size);
 
 /* RunSingleStrainStep(Edot, NumMaxIterations, TimeStep, ConvergenceEpsilon) -> <sigma>
  * (MaterialGrid.cpp:897-1084).  stats may be NULL. */

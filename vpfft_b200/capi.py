@@ -183,6 +183,9 @@ _PROTOS = {
     "vpfft_grid_set_crss": (C.c_int, [_G, _D]),
     "vpfft_grid_get_field": (C.c_int, [_G, C.c_int, _D]),
     "vpfft_grid_set_field": (C.c_int, [_G, C.c_int, _D]),
+    "vpfft_grid_snapshot_size": (C.c_int, [_G, C.POINTER(C.c_size_t)]),
+    "vpfft_grid_snapshot": (C.c_int, [_G, C.c_void_p, C.c_size_t]),
+    "vpfft_grid_restore": (C.c_int, [_G, C.c_void_p, C.c_size_t]),
     "vpfft_run_single_strain_step": (C.c_int, [_G, _D, C.c_int, C.c_double, C.c_double, _D,
                                                C.POINTER(Stats)]),
     "vpfft_run": (C.c_int, [_G, _D, C.c_int, C.c_int, C.c_double, C.c_double, C.c_char_p,

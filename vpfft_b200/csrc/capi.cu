@@ -202,6 +202,19 @@ vpfft_status grid_fail(vpfft_grid* g, vpfft_status s, const std::string& msg) {
   return fail(g, s, msg);
 }
 
+// The operators formed from L0: inverse(-L0) for the Nyquist planes
+// (StrainRateEvolutionWithFFT, MaterialGrid.cpp:628-632) and the symmetric
+// part of L0^-1 for the Newton step.
+void derive_L0_inverses(vpfft_grid* g) {
+  double negL[25];
+  for (int k = 0; k < 25; ++k) negL[k] = -g->L0[k];
+  inverse5_host(negL, g->Linv);
+  double inv[25];
+  inverse5_host(g->L0, inv);
+  for (int i = 0; i < 5; ++i)
+    for (int j = i; j < 5; ++j) g->L0inv_sym[sym5(i, j)] = 0.5 * (inv[j * 5 + i] + inv[i * 5 + j]);
+}
+
 vpfft_status finish_ref_medium(vpfft_grid* g, const double sums[25]) {
   const double N = (double)g->n;
   for (int k = 0; k < 25; ++k) {
@@ -213,13 +226,7 @@ vpfft_status finish_ref_medium(vpfft_grid* g, const double sums[25]) {
   for (int k = 0; k < 25; ++k)
     if (!std::isfinite(g->L0[k]))
       return fail(g, VPFFT_ERR_NONFINITE, "reference medium is not finite (singular voxel compliance)");
-  double negL[25];
-  for (int k = 0; k < 25; ++k) negL[k] = -g->L0[k];
-  inverse5_host(negL, g->Linv);  // StrainRateEvolutionWithFFT, MaterialGrid.cpp:628-632
-  double inv[25];
-  inverse5_host(g->L0, inv);
-  for (int i = 0; i < 5; ++i)
-    for (int j = i; j < 5; ++j) g->L0inv_sym[sym5(i, j)] = 0.5 * (inv[j * 5 + i] + inv[i * 5 + j]);
+  derive_L0_inverses(g);
   g->have_L0 = true;
   return VPFFT_OK;
 }
@@ -847,6 +854,115 @@ vpfft_status vpfft_grid_set_field(vpfft_grid* g, vpfft_field which, const double
                                               : set_field_impl<float>(g, which, src);
   if (s == VPFFT_OK && which == VPFFT_FIELD_ORIENTATION) g->fields_set = true;
   return s;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Binary snapshot of a grid: this header, then FP64 voxel-major fields in the
+// order stress (5), Lagrange multiplier (5), orientation (9), polarization /
+// work field (5), accumulated shear (1) and, when the CRSS is per voxel, the
+// CRSS (12).
+struct SnapshotHeader {
+  char magic[8];
+  int32_t version, precision, nx, ny, nz, flags, pad;
+  double h[3];
+  double L0[25];
+  double last_edot[5];
+};
+constexpr char kSnapMagic[8] = {'V', 'P', 'F', 'F', 'T', 'S', 'N', '1'};
+constexpr int32_t kSnapFieldsSet = 1, kSnapCrssPerVoxel = 2, kSnapHaveL0 = 4;
+
+size_t snapshot_bytes(long long n, bool crss_per_voxel) {
+  const size_t per = 5 + 5 + 9 + 5 + 1 + (crss_per_voxel ? kNS : 0);
+  return sizeof(SnapshotHeader) + sizeof(double) * per * (size_t)n;
+}
+
+struct SnapField {
+  vpfft_field f;
+  int width;
+};
+constexpr SnapField kSnapFields[] = {{VPFFT_FIELD_STRESS, 5},
+                                     {VPFFT_FIELD_LAGRANGE, 5},
+                                     {VPFFT_FIELD_ORIENTATION, 9},
+                                     {VPFFT_FIELD_POLARIZATION, 5},
+                                     {VPFFT_FIELD_ACCUMULATED_SHEAR, 1},
+                                     {VPFFT_FIELD_CRSS, kNS}};
+
+}  // namespace
+
+extern "C" {
+
+vpfft_status vpfft_grid_snapshot_size(const vpfft_grid* g, size_t* bytes) {
+  if (!g || !bytes) return VPFFT_ERR_INVALID_ARGUMENT;
+  *bytes = snapshot_bytes(g->n, g->crss_per_voxel);
+  return VPFFT_OK;
+}
+
+vpfft_status vpfft_grid_snapshot(vpfft_grid* g, void* buf, size_t cap) {
+  if (g && g->in_batch) return busy(g);
+  if (!g || !buf) return VPFFT_ERR_INVALID_ARGUMENT;
+  const size_t need = snapshot_bytes(g->n, g->crss_per_voxel);
+  if (cap < need)
+    return fail(g, VPFFT_ERR_INVALID_ARGUMENT,
+                "snapshot buffer too small: " + std::to_string(need) + " bytes needed");
+  SnapshotHeader hd{};
+  std::memcpy(hd.magic, kSnapMagic, sizeof(kSnapMagic));
+  hd.version = 1;
+  hd.precision = (int32_t)g->prec;
+  hd.nx = g->nx;
+  hd.ny = g->ny;
+  hd.nz = g->nz;
+  hd.flags = (g->fields_set ? kSnapFieldsSet : 0) | (g->crss_per_voxel ? kSnapCrssPerVoxel : 0) |
+             (g->have_L0 ? kSnapHaveL0 : 0);
+  std::memcpy(hd.h, g->h, sizeof(hd.h));
+  std::memcpy(hd.L0, g->L0, sizeof(hd.L0));
+  std::memcpy(hd.last_edot, g->last_edot, sizeof(hd.last_edot));
+  unsigned char* out = static_cast<unsigned char*>(buf);
+  std::memcpy(out, &hd, sizeof(hd));
+  double* d = reinterpret_cast<double*>(out + sizeof(hd));
+  for (const SnapField& sf : kSnapFields) {
+    if (sf.f == VPFFT_FIELD_CRSS && !g->crss_per_voxel) continue;
+    if (vpfft_status s = vpfft_grid_get_field(g, sf.f, d)) return s;
+    d += (size_t)sf.width * (size_t)g->n;
+  }
+  return VPFFT_OK;
+}
+
+vpfft_status vpfft_grid_restore(vpfft_grid* g, const void* buf, size_t size) {
+  if (g && g->in_batch) return busy(g);
+  if (!g || !buf) return VPFFT_ERR_INVALID_ARGUMENT;
+  SnapshotHeader hd{};
+  if (size < sizeof(hd)) return fail(g, VPFFT_ERR_INVALID_ARGUMENT, "snapshot truncated");
+  std::memcpy(&hd, buf, sizeof(hd));
+  if (std::memcmp(hd.magic, kSnapMagic, sizeof(kSnapMagic)) != 0 || hd.version != 1)
+    return fail(g, VPFFT_ERR_INVALID_ARGUMENT, "not a vpfft grid snapshot");
+  if (hd.precision != (int32_t)g->prec || hd.nx != g->nx || hd.ny != g->ny || hd.nz != g->nz)
+    return fail(g, VPFFT_ERR_INVALID_ARGUMENT,
+                "snapshot of a grid of other dimensions or precision");
+  const bool crss_pv = (hd.flags & kSnapCrssPerVoxel) != 0;
+  if (size != snapshot_bytes(g->n, crss_pv))
+    return fail(g, VPFFT_ERR_INVALID_ARGUMENT, "snapshot size does not match its header");
+  if (!(hd.h[0] > 0) || !(hd.h[1] > 0) || !(hd.h[2] > 0))
+    return fail(g, VPFFT_ERR_INVALID_ARGUMENT, "snapshot voxel lengths must be > 0");
+  const double* d =
+      reinterpret_cast<const double*>(static_cast<const unsigned char*>(buf) + sizeof(hd));
+  for (const SnapField& sf : kSnapFields) {
+    if (sf.f == VPFFT_FIELD_CRSS) {
+      if (vpfft_status s = vpfft_grid_set_crss(g, crss_pv ? d : nullptr)) return s;
+    } else if (vpfft_status s = vpfft_grid_set_field(g, sf.f, d)) {
+      return s;
+    }
+    if (sf.f != VPFFT_FIELD_CRSS || crss_pv) d += (size_t)sf.width * (size_t)g->n;
+  }
+  std::memcpy(g->h, hd.h, sizeof(g->h));
+  std::memcpy(g->L0, hd.L0, sizeof(g->L0));
+  std::memcpy(g->last_edot, hd.last_edot, sizeof(g->last_edot));
+  g->have_L0 = (hd.flags & kSnapHaveL0) != 0;
+  if (g->have_L0) derive_L0_inverses(g);
+  g->fields_set = (hd.flags & kSnapFieldsSet) != 0;
+  return VPFFT_OK;
 }
 
 vpfft_status vpfft_run_single_strain_step(vpfft_grid* g, const double edot[5], int max_iter,

@@ -160,6 +160,20 @@ class MaterialGrid:
         a = f64(values, (self.N * w,))
         check(self._lib.vpfft_grid_set_field(self._h, which, dptr(a)), self._h)
 
+    # ---------------------------------------------------------------- checkpoint
+    def snapshot(self) -> bytes:
+        """The grid's whole state (vpfft_grid_snapshot) as bytes."""
+        n = C.c_size_t(0)
+        check(self._lib.vpfft_grid_snapshot_size(self._h, C.byref(n)), self._h)
+        buf = C.create_string_buffer(n.value)
+        check(self._lib.vpfft_grid_snapshot(self._h, buf, n.value), self._h)
+        return buf.raw
+
+    def restore(self, data: bytes) -> None:
+        """Continue from a snapshot of a grid of the same dimensions and
+        precision (vpfft_grid_restore)."""
+        check(self._lib.vpfft_grid_restore(self._h, data, len(data)), self._h)
+
     def Stress(self) -> np.ndarray:
         return self.field(capi.FIELD_STRESS)
 
