@@ -120,6 +120,20 @@ class MaterialGrid {
   void PrintLagrangeMultiplier(const std::string& f) { print(VPFFT_PRINT_LAGRANGE, f); }
   void PrintPolarization(const std::string& f) { print(VPFFT_PRINT_POLARIZATION, f); }
 
+  // Checkpoint of the whole grid (vpfft_grid_snapshot / vpfft_grid_restore; the
+  // reference has none): a grid of the same dimensions and precision restored
+  // from it continues bit for bit.
+  std::vector<unsigned char> Snapshot() {
+    size_t n = 0;
+    detail::check(vpfft_grid_snapshot_size(g_, &n), g_);
+    std::vector<unsigned char> b(n);
+    detail::check(vpfft_grid_snapshot(g_, b.data(), b.size()), g_);
+    return b;
+  }
+  void Restore(const std::vector<unsigned char>& b) {
+    detail::check(vpfft_grid_restore(g_, b.data(), b.size()), g_);
+  }
+
   vpfft_grid* handle() { return g_; }
 
  private:
