@@ -66,6 +66,33 @@ def test_port_matches_reference_build_on_random_case(port):
         assert np.array_equal(ra[k], rb[k]), k
 
 
+@pytest.mark.skipif(not os.path.exists(refio.REF_BIN), reason="reference build not present")
+def test_port_matches_reference_build_on_the_seed_sweep(port, lib):
+    """The ten seeded 12^3 cases the device parity sweep (test_gpu_seeds.py)
+    checks against the restatement: the restatement and the reference build
+    agree bit for bit on each."""
+    import concurrent.futures as cf
+
+    from vpfft_b200 import fixtures
+
+    dims = (12, 12, 12)
+    n = int(np.prod(dims))
+    edot = fixtures.edot_from_matrix(np.diag([1.0, -0.5, -0.5]))
+    mat = refio.Material.uniform(1.0, 10, 1.0, 0.5, 20.0, 1.0)
+    cases = {s: refio.Case(dims, fixtures.polycrystal(*dims, 8, s), np.zeros((n, 5)), np.ones(12),
+                           mat, edot, nsteps=1, max_iter=100, dt=0.005, eps=1e-5)
+             for s in range(1, 11)}
+    with tempfile.TemporaryDirectory() as tmp, \
+            cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+        runs = {(s, b): ex.submit(refio.run, b, c, os.path.join(tmp, f"{s}_{i}"))
+                for s, c in cases.items() for i, b in enumerate((refio.REF_BIN, refio.PORT_BIN))}
+        out = {k: f.result() for k, f in runs.items()}
+    for s in cases:
+        ra, rb = out[(s, refio.REF_BIN)], out[(s, refio.PORT_BIN)]
+        for k in ("iters", "avg_stress", "allreduce", "sigma", "lambda", "R", "crss", "accshear"):
+            assert np.array_equal(ra[k], rb[k]), (s, k)
+
+
 def test_dft_matches_numpy(port):
     rng = np.random.default_rng(1)
     for shape in [(8, 6, 5), (16, 12, 10), (3, 7, 4)]:
