@@ -27,3 +27,27 @@ def test_increment_costs_and_rve_baselines(lib, port):
     assert np.isfinite(s["value"]) and s["value"] > 0
     assert 0 < s["latency_p50_s"] <= s["latency_p99_s"]
     assert set(b["per_edge"]) == {"6", "8"}
+
+
+def test_reference_arm_prints_its_json_line(port):
+    """bench.py --impl reference: the reference's CPU solve on the host cores,
+    one JSON line with the bench keys, impl "reference", its cpu_baseline and
+    an e2e without host-device copies."""
+    import json
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference",
+                        "--steps", "1", "--warmup", "1"], capture_output=True, text=True,
+                       timeout=600, cwd=root)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+              "higher_is_better", "config", "cpu_baseline", "e2e"):
+        assert k in line, k
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] in ("reference", "port")
+    assert line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
