@@ -404,51 +404,91 @@ def ref_binary():
     return refio.PORT_BIN, "port"
 
 
-def cpu_samples(n_side, procs, warm, timed):
-    """Run `procs` concurrent single-threaded oracle processes, each solving its
-    own n_side^3 sample of the workload (same grain size and material) for
-    warm + timed fixed-point iterations with eps = 0; returns the summed
-    voxel-iters/s over the timed iterations (from the oracle's per-iteration
-    timestamps) and per-process rates."""
-    from oracle import refio
-    from vpfft_b200 import fixtures
+def mem_available_bytes() -> int:
+    try:
+        with open("/proc/meminfo") as fh:
+            for line in fh:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
+# Host memory of the reference per voxel: its fields (orientation, stress,
+# Lagrange multiplier, per-system Schmid tensors and CRSS in nested vectors,
+# accumulated shear; MaterialGrid.cpp:312-394), its ten complex FFT buffers,
+# and the send buffers of the input distribution (orientation + stress).
+REF_BYTES_PER_VOXEL = 1300
+
+
+def reference_solve(n_side, grains, seed, warm, timed, ranks):
+    """The reference's own solve of the workload (n_side^3, `grains` grains,
+    the fixture seed, n = 20, plane strain) on the host: the reference build
+    (oracle/_ref/vpfft_ref) run as `ranks` MPI ranks over the multi-process
+    stand-ins (its FFTW-MPI slab decomposition, one single-threaded process
+    per core), which generates the polycrystal itself (oracle/common/
+    polycrystal.c, bit-identical to the product's fixture); one increment of
+    warm + timed fixed-point iterations with eps = 0.  Returns the rate over
+    the timed iterations (from rank 0's timestamps at each iteration's forward
+    FFT) and the share of that time inside the FFT stand-in."""
+    from oracle import portlib, refio
 
     binary, kind = ref_binary()
-    grains = max(1, round(N_GRAINS * (n_side / N_GRID) ** 3))
-    edot = fixtures.edot_from_matrix(VEL_GRAD)
+    edot = refio.edot_from_matrix(VEL_GRAD)
     m = refio.Material.uniform(1.0, RATE_SENS, 1.0, 0.5, 20.0, 1.0)
-    tmp = tempfile.mkdtemp(prefix="vpfft_cpu_")
-    runs = []
-    for p in range(procs):
-        R = fixtures.polycrystal(n_side, n_side, n_side, grains, SEED + p)
-        case = refio.Case((n_side,) * 3, R, np.zeros((n_side ** 3, 5)), np.ones(12), m, edot,
-                          nsteps=1, max_iter=warm + timed, dt=0.005, eps=0.0)
-        d = os.path.join(tmp, str(p))
-        os.makedirs(d)
-        refio.write_input(os.path.join(d, "input.bin"), case)
-        runs.append(d)
-    procs_ = [subprocess.Popen([binary, os.path.join(d, "input.bin"), d, "--quiet"],
-                               stdout=subprocess.DEVNULL, stderr=subprocess.PIPE) for d in runs]
-    rates = []
-    for pr, d in zip(procs_, runs):
-        _, err = pr.communicate()
-        if pr.returncode != 0:
-            raise RuntimeError(f"oracle failed: {err.decode()[-500:]}")
-        ft = np.fromfile(os.path.join(d, "fwd_times.bin"))
-        # ft[k] is taken at the start of iteration k+1's forward FFT; the last
-        # one starts the post-loop orientation update
-        span = ft[warm + timed] - ft[warm]
-        rates.append(n_side ** 3 * timed / span)
-    return float(sum(rates)), rates, kind, binary
+    tmp = tempfile.mkdtemp(prefix="vpfft_ref_")
+    n = n_side ** 3
+    try:
+        if kind == "reference":
+            case = refio.Case((n_side,) * 3, None, None, np.ones(12), m, edot, nsteps=1,
+                              max_iter=warm + timed, dt=0.005, eps=0.0)
+            extra = ["--generate", grains, seed, "--ranks", ranks, "--timing-only"]
+        else:  # the C restatement has no MPI: one process
+            ranks = 1
+            case = refio.Case((n_side,) * 3, portlib.polycrystal(n_side, n_side, n_side, grains,
+                                                                 seed, threads=host_cores()),
+                              np.zeros((n, 5)), np.ones(12), m, edot, nsteps=1,
+                              max_iter=warm + timed, dt=0.005, eps=0.0)
+            extra = []
+        t0 = time.time()
+        out = refio.run(binary, case, tmp, extra_args=extra)
+        wall = time.time() - t0
+    finally:
+        import shutil
+
+        shutil.rmtree(tmp, ignore_errors=True)
+    ft, fs = out["fwd_times"], out["fwd_fft_seconds"]
+    # ft[k]: start of iteration k's forward FFT; ft[warm + timed] starts the
+    # post-loop orientation update
+    span = float(ft[warm + timed] - ft[warm])
+    fft_share = (float(fs[warm + timed] - fs[warm]) / span) if fs is not None else None
+    return {"rate": n * timed / span, "iter_s": span / timed, "fft_share": fft_share,
+            "setup_s": wall - float(ft[-1] - ft[0]),
+            "wall_s": wall, "ranks": ranks, "kind": kind, "binary": binary}
 
 
-def cpu_baseline_ours():
-    n_side, warm, timed = 48, 1, 6
-    total, rates, kind, _ = cpu_samples(n_side, 1, warm, timed)
-    return {"value": total, "unit": UNIT, "cores": 1, "kind": kind,
-            "sample": (f"{n_side}^3 sample of the workload (same grain size and material), "
-                       f"{timed} timed fixed-point iterations after {warm} warm-up, one "
-                       "single-threaded process")}
+def reference_sample_text(r, n_side, grains, warm, timed) -> str:
+    return (f"the reference's own code ({os.path.relpath(r['binary'], ROOT)}: Src/*.cpp "
+            f"compiled unmodified against the project's MPI/FFTW/Eigen stand-ins) on the full "
+            f"{n_side}^3 workload ({grains} grains, same seed, material and strain rate), run as "
+            f"{r['ranks']} MPI ranks (FFTW-MPI slab decomposition, one single-threaded process "
+            f"per core); {warm} warm-up + {timed} timed fixed-point iterations of one increment; "
+            f"{r['fft_share'] * 100:.1f} % of the timed time inside the FFT stand-in"
+            if r.get("fft_share") is not None else "")
+
+
+def cpu_baseline_ours(n_side=N_GRID):
+    warm, timed = 1, 2
+    cores = host_cores()
+    need = REF_BYTES_PER_VOXEL * n_side ** 3
+    if mem_available_bytes() < 1.2 * need:
+        return {"unavailable": f"the reference needs ~{need / 2**30:.0f} GiB of host memory at "
+                               f"{n_side}^3; {mem_available_bytes() / 2**30:.0f} GiB available"}
+    r = reference_solve(n_side, N_GRAINS, SEED, warm, timed, cores)
+    return {"value": r["rate"], "unit": UNIT, "cores": r["ranks"], "kind": r["kind"],
+            "seconds_per_iteration": r["iter_s"], "fft_share": r["fft_share"],
+            "sample": reference_sample_text(r, n_side, N_GRAINS, warm, timed)}
 
 
 def host_cores() -> int:
@@ -469,7 +509,7 @@ def cpu_increment_costs(edges, k_iters: int = 2):
     iterations (initialisation, reference medium, texture and hardening)."""
     import shutil
 
-    from oracle import refio
+    from oracle import portlib, refio
     from vpfft_b200 import fixtures
 
     binary, kind = ref_binary()
@@ -479,7 +519,7 @@ def cpu_increment_costs(edges, k_iters: int = 2):
     runs = []
     try:
         for e in edges:
-            R = fixtures.polycrystal(e, e, e, 104, SEED + 11 * e)
+            R = portlib.polycrystal(e, e, e, 104, SEED + 11 * e)
             ed = fixtures.edot_from_matrix(fixtures.random_traceless_velocity_gradient(rng))
             case = refio.Case((e,) * 3, R, np.zeros((e ** 3, 5)), np.ones(12), m, ed, nsteps=1,
                               max_iter=k_iters, dt=0.005, eps=0.0)
@@ -622,31 +662,39 @@ def whole_job_rate(units_per_rank: float, world_size: int, seconds_max: float) -
 
 # ------------------------------------------------------------------ main
 def run_reference_arm(args, rank, ws):
+    """The reference's CPU solve of the headline workload on the host cores
+    (rank 0 only), printed as the reference arm's JSON line."""
     if rank != 0:
         return 0
-    procs = os.cpu_count() or 1
-    # per-process sample sized so that warm-up + steps iterations stay ~1 minute
-    n_side = 32 if args.steps + args.warmup > 20 else 48
-    total, rates, kind, binary = cpu_samples(n_side, procs, args.warmup, args.steps)
-    per_iter_ms = 1e3 * (n_side ** 3) / (total / procs)
-    line = {
-        "metric": METRIC, "value": total, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": per_iter_ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "impl": "reference",
-        "config": {"workload": WORKLOAD, "grid": [n_side] * 3, "grains_scaled": True,
-                   "step": "one fixed-point iteration of each process's sample",
-                   "processes": procs},
-        "cpu_baseline": {"value": total, "unit": UNIT, "cores": procs, "kind": kind,
-                         "sample": (f"{procs} concurrent single-threaded processes of the "
-                                    f"reference ({os.path.relpath(binary, ROOT)}), each on its "
-                                    f"own {n_side}^3 sample of the workload (same grain size, "
-                                    f"material and strain rate), {args.warmup} warm-up + "
-                                    f"{args.steps} timed fixed-point iterations; the reference "
-                                    "has no threaded region and its MPI transport is replaced "
-                                    "by a single-rank stand-in")},
-        "e2e": {"value": total, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
+    n_side = args.grid
+    grains = N_GRAINS if n_side == N_GRID else max(1, round(N_GRAINS * (n_side / N_GRID) ** 3))
+    cores = host_cores()
+    need = REF_BYTES_PER_VOXEL * n_side ** 3
+    base = {"metric": METRIC, "impl": "reference", "unit": UNIT}
+    if mem_available_bytes() < 1.2 * need:
+        base["unavailable"] = (f"the reference needs ~{need / 2**30:.0f} GiB of host memory at "
+                               f"{n_side}^3 and {mem_available_bytes() / 2**30:.0f} GiB are "
+                               "available")
+        print(json.dumps(base), flush=True)
+        return 0
+    r = reference_solve(n_side, grains, SEED, args.warmup, args.steps, cores)
+    line = dict(base)
+    line.update({
+        "value": r["rate"], "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * r["iter_s"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload(n_side), "grid": [n_side] * 3, "grains": grains,
+                   "seed": SEED, "precision": "fp64 (the reference's Float is double)",
+                   "step": "one fixed-point iteration of the whole grid",
+                   "mpi_ranks": r["ranks"]},
+        "cpu_baseline": {"value": r["rate"], "unit": UNIT, "cores": r["ranks"], "kind": r["kind"],
+                         "seconds_per_iteration": r["iter_s"], "fft_share": r["fft_share"],
+                         "sample": reference_sample_text(r, n_side, grains, args.warmup,
+                                                         args.steps)},
+        "e2e": {"value": r["rate"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "wall_s": r["wall_s"],
+    })
     print(json.dumps(line), flush=True)
     return 0
 

@@ -45,9 +45,21 @@ typedef enum {
   VPFFT_ERR_NOT_INITIALIZED = 8,  /* fields not set before a solve */
   VPFFT_ERR_IO = 9,               /* file could not be read or parsed */
   VPFFT_ERR_CANCELLED = 10,
-  VPFFT_ERR_TIMEOUT = 11,
+  /* 11 is not used */
   VPFFT_ERR_BUSY = 12             /* the grid has a request in flight in a batch */
 } vpfft_status;
+
+/* Bits of vpfft_stats.status_bits and vpfft_batch_result.status_bits: what a
+ * solve that returned VPFFT_OK still reports.  The reference's paths for the
+ * last two are silent (the fixed-point loop ends at NumMaxIterations with no
+ * flag, MaterialGrid.cpp:1046-1068; a voxel's NR returns its last iterate at
+ * its cap, Solvers.cpp:167-170, 213-221). */
+#define VPFFT_STATUS_MAX_RSS_TINY 0x1       /* a voxel's max resolved shear < 1e-10 (the call fails) */
+#define VPFFT_STATUS_NONFINITE 0x2          /* NaN/Inf appeared (the call fails) */
+#define VPFFT_STATUS_LOOP_NOT_CONVERGED 0x100 /* the loop stopped at max_iter with delta_sigma
+                                               or delta_eps above eps */
+#define VPFFT_STATUS_NR_CAPPED 0x200        /* some voxel's Newton-Raphson solve stopped at its
+                                               iteration cap (count: nr_not_converged) */
 
 typedef enum {
   VPFFT_PREC_FP64 = 0,  /* everything in FP64: the GPU oracle path */
@@ -87,7 +99,7 @@ typedef struct {
   double strain_rate_error;   /* final delta_eps   (MaterialGrid.cpp:1053) */
   double avg_strain_rate[5];  /* <edot> of the last iteration */
   int64_t nr_not_converged;   /* voxel-iterations whose NR hit its cap */
-  int32_t status_bits;        /* OR of device-side warnings */
+  int32_t status_bits;        /* OR of VPFFT_STATUS_* bits */
   int32_t pad_;
   double seconds_init;        /* InitializeComputation + reference medium */
   double seconds_loop;        /* the fixed-point loop */
@@ -158,7 +170,10 @@ vpfft_status vpfft_grid_set_field(vpfft_grid *g, vpfft_field which, const double
  * fields widen exactly), so a grid restored from it continues bit for bit as
  * the original would.  vpfft_grid_snapshot_size gives the bytes (a header plus
  * 25 or 37 doubles per voxel); vpfft_grid_restore accepts a snapshot of a
- * grid of the same dimensions and precision only. */
+ * grid of the same dimensions and precision only.  A restore that fails after
+ * its header checks (a CUDA error while the fields are copied) leaves the grid
+ * without fields or reference medium: restore it again, or set its fields,
+ * before the next solve (which otherwise returns VPFFT_ERR_NOT_INITIALIZED). */
 vpfft_status vpfft_grid_snapshot_size(const vpfft_grid *g, size_t *bytes);
 vpfft_status vpfft_grid_snapshot(vpfft_grid *g, void *buf, size_t cap);
 vpfft_status vpfft_grid_restore(vpfft_grid *g, const void *buf, size_t size);
@@ -235,13 +250,20 @@ vpfft_status vpfft_solve_constrained_constitutive(int n, const double *stress0,
  * macro-scale driver calling the point solve from inside its own Newton loop
  * typically gives the device to its own memory pool, where a cudaMalloc can
  * fail and every cudaFree synchronises the device.  The arrays are staged in
- * a fixed device array of VPFFT_NOALLOC_MAX_POINTS points (2.9 MiB) that lives
- * as long as the library; larger n returns VPFFT_ERR_UNSUPPORTED_SIZE.  The
- * first call on each device looks up that array's address: make it before any
- * stream capture begins.  Calls share the array, so they are serialised by a
- * process-wide lock (overlapping calls would otherwise race on it).  A call
- * waits for its own work on the legacy default stream, not for the whole
- * device.
+ * a fixed device array of VPFFT_NOALLOC_MAX_POINTS points (2.9 MiB per
+ * device); larger n returns VPFFT_ERR_UNSUPPORTED_SIZE.
+ * The first call on each device (n = 0 is enough) sets up: it looks up the
+ * array's address and has the CUDA runtime load the array and this call's
+ * kernels, which under the runtime's default lazy module loading allocates
+ * about 3 MiB of device memory.  Make that first call before the caller's
+ * memory pool reserves the device; later calls allocate nothing.
+ * Every call runs its copies and kernels on the legacy default stream: no call
+ * may overlap a stream capture anywhere in the process (on any device), and a
+ * call is ordered after the work of the caller's blocking streams (streams
+ * made with plain cudaStreamCreate); only streams created with
+ * cudaStreamNonBlocking are not stalled.  Calls share the array, so they are
+ * serialised by a process-wide lock (overlapping calls would otherwise race on
+ * it).  A call returns when its results are on the host.
  * not_converged (may be NULL) gets the number of points whose NR error is not
  * below eps. */
 #define VPFFT_NOALLOC_MAX_POINTS 4096
@@ -329,7 +351,7 @@ typedef struct {
   int32_t status;               /* vpfft_status of the request */
   int32_t iterations;           /* fixed-point iterations executed */
   int32_t converged;
-  int32_t pad_;
+  int32_t status_bits;          /* OR of VPFFT_STATUS_* bits */
   double avg_stress[5];         /* <sigma> of the last iteration (the step's return value) */
   double stress_error;          /* final delta_sigma */
   double strain_rate_error;     /* final delta_eps */

@@ -57,6 +57,9 @@ def load():
         lib.oracle_inverse5.argtypes = [_D, _D]
         lib.oracle_dft3d_inplace.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_size_t,
                                              C.c_int]
+        lib.oracle_polycrystal.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_int,
+                                           _D, C.POINTER(C.c_int32)]
+        lib.oracle_polycrystal.restype = C.c_int
         _lib = lib
     return _lib
 
@@ -189,3 +192,17 @@ def green_bar_dhat(L0, idx, dims, h, phat) -> np.ndarray:
 
     G = 0.5 * (op((ix, iy, iz)) + op(((nx - ix) % nx, (ny - iy) % ny, (nz - iz) % nz)))
     return -G @ np.asarray(phat)
+
+
+def polycrystal(nx: int, ny: int, nz: int, grains: int, seed: int, threads: int = 1,
+                with_grains: bool = False):
+    """The oracle-side synthetic polycrystal (oracle/common/polycrystal.c):
+    (N, 9) row-major orientations, and the grain of every voxel on request."""
+    n = nx * ny * nz
+    R = np.zeros((n, 9))
+    g = np.zeros(n, np.int32)
+    rc = load().oracle_polycrystal(nx, ny, nz, grains, seed, threads,
+                                   R.ctypes.data_as(_D), g.ctypes.data_as(C.POINTER(C.c_int32)))
+    if rc != 0:
+        raise ValueError(f"oracle_polycrystal failed ({rc})")
+    return (R, g) if with_grains else R

@@ -24,6 +24,13 @@
 //     at that moment they hold P and d~ produced by the previous iteration.
 //
 // Usage: vpfft_ref <input.bin> <outdir> [--dump-iter K]... [--dump-increments] [--quiet]
+//                  [--run-vpfft] [--timing-only] [--ranks P] [--generate GRAINS SEED]
+//   --run-vpfft    drive the increments through RunVPFFT (writes Stress_Strain.txt)
+//   --timing-only  no copies of P and d~ at each iteration (benchmark runs)
+//   --ranks P      run the reference as P MPI ranks (processes sharing memory
+//                  through the stand-ins); only timing and reductions are written
+//   --generate G S the input file carries no orientations: make the synthetic
+//                  polycrystal with G grains and seed S (oracle/common/polycrystal.c)
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -39,10 +46,13 @@
 #include <string>
 #include <vector>
 
+#include <unistd.h>
+
 #include "Eigen/Dense"
 #include "fftw3-mpi.h"
 #include "mpi.h"
 #include "shim_hooks.h"
+#include "../common/polycrystal.h"
 
 // The harness needs read/write access to MaterialGrid's private fields
 // (material parameters are hard-coded in InitializeMemory and there is no
@@ -63,8 +73,10 @@ static_assert(sizeof(EigenRep) == 5 * sizeof(double), "EigenRep layout");
 namespace {
 
 struct Input {
-  int nx, ny, nz, nsteps, max_iter, crss_per_voxel;
+  int nx, ny, nz, nsteps, max_iter, crss_per_voxel, edot_per_increment;
+  int generated;  // no per-voxel arrays in the file: orientations from --generate
   double dt, eps, edot[5], h[3];
+  std::vector<double> edot_steps;  // nsteps x 5 when edot_per_increment
   double gdot[12];
   int nexp[12];
   double tau0[12], tau1[12], theta0[12], theta1[12], H[144];
@@ -100,6 +112,8 @@ Input read_input(const char *path) {
   in.nsteps = hdr[3];
   in.max_iter = hdr[4];
   in.crss_per_voxel = hdr[5];
+  in.edot_per_increment = hdr[6];
+  in.generated = hdr[7];
   rd(f, &in.dt, 1);
   rd(f, &in.eps, 1);
   rd(f, in.edot, 5);
@@ -114,12 +128,21 @@ Input read_input(const char *path) {
   rd(f, in.theta1, 12);
   rd(f, in.H, 144);
   size_t N = (size_t)in.nx * in.ny * in.nz;
-  in.R.resize(N * 9);
-  in.sigma.resize(N * 5);
-  rd(f, in.R.data(), N * 9);
-  rd(f, in.sigma.data(), N * 5);
+  if (!in.generated) {
+    in.R.resize(N * 9);
+    in.sigma.resize(N * 5);
+    rd(f, in.R.data(), N * 9);
+    rd(f, in.sigma.data(), N * 5);
+  } else if (in.crss_per_voxel) {
+    std::fprintf(stderr, "vpfft_ref: generated inputs take a uniform CRSS\n");
+    std::exit(2);
+  }
   in.crss.resize(in.crss_per_voxel ? N * 12 : 12);
   rd(f, in.crss.data(), in.crss.size());
+  if (in.edot_per_increment) {
+    in.edot_steps.resize((size_t)in.nsteps * 5);
+    rd(f, in.edot_steps.data(), in.edot_steps.size());
+  }
   return in;
 }
 
@@ -139,9 +162,14 @@ struct Observer {
   std::string outdir;
   int increment = 0;
   int fwd_p0_in_increment = 0;  // forward FFTs of P component 0 seen this increment
+  bool snapshots = true;        // copy P and d~ at each forward FFT of P0
   std::vector<int> dump_iters;  // iteration indices of increment 0 to dump
   std::vector<double> allreduce;
+  // allreduce values recorded when each increment began (RunVPFFT mode: the
+  // reference's MPI_Barrier after each increment marks the boundary)
+  std::vector<size_t> increment_ar_starts{0};
   std::vector<double> fwd_times;  // steady-clock seconds at each forward P0 FFT
+  std::vector<double> fwd_fft_seconds;  // seconds inside fftw_execute by then
   std::vector<int> fwd_increment;
   // last snapshot of P and d~ (real parts), [N][5]
   std::vector<double> lastP, lastD;
@@ -161,10 +189,12 @@ void on_exec(int sign, double (*data)[2], long, void *) {
   if (data != o.grid->_PolarizationField[0]) return;
   o.fwd_times.push_back(
       std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count());
+  o.fwd_fft_seconds.push_back(vpfft_shim_fft_seconds());
   o.fwd_increment.push_back(o.increment);
   // Before this forward FFT the buffers hold the previous iteration's P and d~.
   int iter = o.fwd_p0_in_increment;  // 0 = after initialisation, k = after iteration k
   ++o.fwd_p0_in_increment;
+  if (!o.snapshots) return;
   o.snapshot(o.lastP, o.grid->_PolarizationField);
   o.snapshot(o.lastD, o.grid->_DisplacementVariation);
   if (o.increment == 0 &&
@@ -178,6 +208,12 @@ void on_exec(int sign, double (*data)[2], long, void *) {
   }
 }
 
+void on_barrier(void *) {
+  g_obs.increment_ar_starts.push_back(g_obs.allreduce.size());
+  ++g_obs.increment;
+  g_obs.fwd_p0_in_increment = 0;
+}
+
 void on_allreduce(const double *v, int count, void *) {
   for (int i = 0; i < count; ++i) g_obs.allreduce.push_back(v[i]);
 }
@@ -189,7 +225,9 @@ int main(int argc, char **argv) {
     std::fprintf(stderr, "usage: vpfft_ref <input.bin> <outdir> [--dump-iter K]... [--quiet]\n");
     return 2;
   }
-  bool quiet = false, dump_increments = false;
+  bool quiet = false, dump_increments = false, run_vpfft = false;
+  int ranks = 1, gen_grains = 0;
+  unsigned long long gen_seed = 0;
   for (int a = 3; a < argc; ++a) {
     if (!std::strcmp(argv[a], "--dump-iter") && a + 1 < argc)
       g_obs.dump_iters.push_back(std::atoi(argv[++a]));
@@ -197,11 +235,40 @@ int main(int argc, char **argv) {
       quiet = true;
     else if (!std::strcmp(argv[a], "--dump-increments"))
       dump_increments = true;
+    else if (!std::strcmp(argv[a], "--run-vpfft"))
+      run_vpfft = true;
+    else if (!std::strcmp(argv[a], "--timing-only"))
+      g_obs.snapshots = false;
+    else if (!std::strcmp(argv[a], "--ranks") && a + 1 < argc)
+      ranks = std::atoi(argv[++a]);
+    else if (!std::strcmp(argv[a], "--generate") && a + 2 < argc) {
+      gen_grains = std::atoi(argv[++a]);
+      gen_seed = std::strtoull(argv[++a], nullptr, 10);
+    }
   }
   Input in = read_input(argv[1]);
   const size_t N = (size_t)in.nx * in.ny * in.nz;
   g_obs.N = N;
   g_obs.outdir = argv[2];
+  if (in.generated && gen_grains < 1) {
+    std::fprintf(stderr, "vpfft_ref: the input has no orientations; give --generate G SEED\n");
+    return 2;
+  }
+  // With several ranks each process holds a slab of the grid; only timing,
+  // the reduced values and <sigma> are written (no per-voxel fields).
+  if (ranks > 1) {
+    g_obs.snapshots = false;
+    if (!g_obs.dump_iters.empty() || dump_increments || run_vpfft || in.crss_per_voxel) {
+      std::fprintf(stderr, "vpfft_ref: --ranks > 1 writes no per-voxel output\n");
+      return 2;
+    }
+    const size_t slab = (size_t)((in.nx + ranks - 1) / ranks) * in.ny * in.nz;
+    if (vpfft_shim_configure(ranks, slab * 10 * sizeof(fftw_complex) + (1u << 20),
+                             N * (sizeof(SMatrix3x3) + sizeof(EigenRep)) + (1u << 20)) != 0) {
+      std::fprintf(stderr, "vpfft_ref: bad rank count %d\n", ranks);
+      return 2;
+    }
+  }
 
   // The reference prints progress to std::cout; keep stdout for our summary.
   std::ofstream devnull("/dev/null");
@@ -210,6 +277,8 @@ int main(int argc, char **argv) {
 
   int argc0 = 0;
   MPI_Init(&argc0, nullptr);
+  int rank = 0;
+  MPI_Comm_rank(MPI_COMM_WORLD, &rank);
   MaterialGrid grid(in.nx, in.ny, in.nz);
   for (int s = 0; s < 12; ++s) {
     grid.GammaDotBase[s] = in.gdot[s];
@@ -220,9 +289,27 @@ int main(int argc, char **argv) {
     grid.Theta1[s] = in.theta1[s];
     for (int t = 0; t < 12; ++t) grid.HardeningMatrix[s][t] = in.H[s * 12 + t];
   }
-  grid.SendDataAndInitialize(reinterpret_cast<SMatrix3x3 *>(in.R.data()),
-                             reinterpret_cast<EigenRep *>(in.sigma.data()));
-  for (size_t v = 0; v < N; ++v)
+  if (rank == 0) {
+    if (in.generated) {
+      in.R.resize(N * 9);
+      in.sigma.assign(N * 5, 0.0);
+      if (oracle_polycrystal(in.nx, in.ny, in.nz, gen_grains, gen_seed, ranks, in.R.data(),
+                             nullptr) != 0) {
+        std::fprintf(stderr, "vpfft_ref: polycrystal generation failed\n");
+        return 2;
+      }
+    }
+    grid.SendDataAndInitialize(reinterpret_cast<SMatrix3x3 *>(in.R.data()),
+                               reinterpret_cast<EigenRep *>(in.sigma.data()));
+    if (ranks > 1) {  // the caller's arrays are no longer needed
+      std::vector<double>().swap(in.R);
+      std::vector<double>().swap(in.sigma);
+    }
+  } else {
+    grid.RecvDataAndInitialize();
+  }
+  const size_t n_local = (size_t)grid.DimXLocal * grid.DimYZ;
+  for (size_t v = 0; v < n_local; ++v)
     for (int s = 0; s < 12; ++s)
       grid.LocalCRSS[v][s] = in.crss_per_voxel ? in.crss[v * 12 + s] : in.crss[s];
   grid.SetVoxelLength(in.h[0], in.h[1], in.h[2]);
@@ -230,14 +317,44 @@ int main(int argc, char **argv) {
   g_obs.grid = &grid;
   vpfft_shim_set_exec_hook(on_exec, nullptr);
   vpfft_shim_set_allreduce_hook(on_allreduce, nullptr);
+  if (run_vpfft) vpfft_shim_set_barrier_hook(on_barrier, nullptr);
 
   EigenRep edot(in.edot[0], in.edot[1], in.edot[2], in.edot[3], in.edot[4]);
   std::vector<double> steps;        // per increment: iters, <sigma>(5)
   std::vector<double> ar_counts;    // per increment: allreduce values recorded
   std::vector<double> step_seconds; // per increment wall time
-  for (int step = 0; step < in.nsteps; ++step) {
+  if (run_vpfft) {
+    // the reference's own multi-increment driver (MaterialGrid.cpp:1202-1228),
+    // which writes Stress_Strain.txt into the working directory
+    if (chdir(g_obs.outdir.c_str()) != 0) {
+      std::fprintf(stderr, "vpfft_ref: cannot enter %s\n", g_obs.outdir.c_str());
+      return 2;
+    }
+    g_obs.increment = 0;
+    auto t0 = std::chrono::steady_clock::now();
+    grid.RunVPFFT(edot, in.max_iter, in.nsteps, in.dt, in.eps);
+    auto t1 = std::chrono::steady_clock::now();
+    // one increment opens with 25 L0 values and adds 12 per iteration; split
+    // the recorded values at each L0 block (the fwd hook counts increments)
+    size_t off = 0;
+    for (int step = 0; step < in.nsteps; ++step) {
+      size_t nvals = (step + 1 < (int)g_obs.increment_ar_starts.size())
+                         ? g_obs.increment_ar_starts[step + 1] - off
+                         : g_obs.allreduce.size() - off;
+      steps.push_back((double)((nvals - 25) / 12));
+      for (int c = 0; c < 5; ++c) steps.push_back(0.0);
+      ar_counts.push_back((double)nvals);
+      step_seconds.push_back(std::chrono::duration<double>(t1 - t0).count() / in.nsteps);
+      off += nvals;
+    }
+  }
+  for (int step = 0; step < (run_vpfft ? 0 : in.nsteps); ++step) {
     g_obs.increment = step;
     g_obs.fwd_p0_in_increment = 0;
+    if (in.edot_per_increment) {
+      const double *e = &in.edot_steps[(size_t)step * 5];
+      edot = EigenRep(e[0], e[1], e[2], e[3], e[4]);
+    }
     size_t ar0 = g_obs.allreduce.size();
     auto t0 = std::chrono::steady_clock::now();
     EigenRep avg = grid.RunSingleStrainStep(edot, in.max_iter, in.dt, in.eps);
@@ -263,6 +380,10 @@ int main(int argc, char **argv) {
     }
   }
   std::cout.rdbuf(saved);
+  if (rank != 0) {
+    MPI_Finalize();
+    return 0;
+  }
 
   const std::string od = g_obs.outdir;
   write_bin(od + "/steps.bin", steps.data(), steps.size());
@@ -272,6 +393,16 @@ int main(int argc, char **argv) {
   write_bin(od + "/fwd_times.bin", g_obs.fwd_times.data(), g_obs.fwd_times.size());
   std::vector<double> fwd_inc(g_obs.fwd_increment.begin(), g_obs.fwd_increment.end());
   write_bin(od + "/fwd_increment.bin", fwd_inc.data(), fwd_inc.size());
+  write_bin(od + "/fwd_fft_seconds.bin", g_obs.fwd_fft_seconds.data(),
+            g_obs.fwd_fft_seconds.size());
+  if (ranks > 1) {
+    std::printf("{\"increments\": %d, \"ranks\": %d, \"iters\": [", in.nsteps, ranks);
+    for (int s = 0; s < in.nsteps; ++s) std::printf("%s%d", s ? ", " : "", (int)steps[s * 6]);
+    std::printf("]}\n");
+    std::fflush(stdout);
+    MPI_Finalize();
+    return 0;
+  }
   write_bin(od + "/sigma.bin", reinterpret_cast<const double *>(grid.StressField), N * 5);
   write_bin(od + "/lambda.bin",
             reinterpret_cast<const double *>(grid.LagrangeMultiplierField.data()), N * 5);

@@ -5,14 +5,19 @@ Test-oracle infrastructure: imported only by tests/, tests/golden/ scripts,
 
 Input file ("VPFFTIN1") layout, little-endian:
     char[8]  magic
-    int32[8] nx, ny, nz, nsteps, max_iter, crss_per_voxel, 0, 0
+    int32[8] nx, ny, nz, nsteps, max_iter, crss_per_voxel, edot_per_increment, generated
     f64      dt, eps, edot[5], h[3]
     f64[12]  gamma_dot_base          int32[12] rate_sensitivity
     f64[12]  tau0, tau1, theta0, theta1
     f64[144] hardening matrix (row-major h[s][t])
     f64[N*9] R   (row-major 3x3 per voxel, voxel index x*Ny*Nz + y*Nz + z)
     f64[N*5] sigma (deviatoric 5-vector per voxel)
+                 (R and sigma are absent when `generated`: the reference
+                 harness then makes the synthetic polycrystal itself from
+                 --generate GRAINS SEED, with sigma = 0)
     f64[N*12 or 12] CRSS
+    f64[nsteps*5] strain rate of each increment (only when edot_per_increment;
+                  otherwise every increment uses `edot`)
 
 The per-voxel order and the 3x3 / 5-vector layouts are the reference's
 (MaterialGrid.h:121-124 ToIndex; SMatrix3x3 m[3][3], LinearAlgebra.h:114;
@@ -60,7 +65,7 @@ class Material:
 @dataclass
 class Case:
     dims: tuple
-    R: np.ndarray  # (N, 9)
+    R: np.ndarray  # (N, 9), or None: the harness generates the orientations
     sigma: np.ndarray  # (N, 5)
     crss: np.ndarray  # (12,) or (N, 12)
     material: Material
@@ -70,16 +75,42 @@ class Case:
     dt: float = 0.005
     eps: float = 1e-5
     h: tuple = (1.0, 1.0, 1.0)
+    edot_steps: np.ndarray = None  # (nsteps, 5): a strain rate per increment
+
+
+def edot_from_matrix(L) -> np.ndarray:
+    """EigenRep(SMatrix3x3) (LinearAlgebra.h:307-312): the projection of a 3x3
+    velocity gradient on the deviatoric basis (LinearAlgebra.h:207-247), summed
+    over the nine entries in row-major order."""
+    a, b = 1.0 / np.sqrt(2.0), 1.0 / np.sqrt(6.0)
+    B = np.zeros((5, 3, 3))
+    B[0, 0, 0], B[0, 1, 1] = -1 * a, 1 * a
+    B[1, 0, 0], B[1, 1, 1], B[1, 2, 2] = -1 * b, -1 * b, 2 * b
+    B[2, 1, 2] = B[2, 2, 1] = 1 * a
+    B[3, 0, 2] = B[3, 2, 0] = 1 * a
+    B[4, 0, 1] = B[4, 1, 0] = 1 * a
+    L = np.asarray(L, np.float64).reshape(3, 3)
+    out = np.zeros(5)
+    for k in range(5):
+        r = 0.0
+        for i in range(3):
+            for j in range(3):
+                r += float(L[i, j]) * float(B[k, i, j])
+        out[k] = r
+    return out
 
 
 def write_input(path: str, c: Case) -> None:
     nx, ny, nz = c.dims
     n = nx * ny * nz
     per_voxel = 1 if np.asarray(c.crss).ndim == 2 else 0
+    per_inc = 0 if c.edot_steps is None else 1
+    generated = 1 if c.R is None else 0
     m = c.material
     with open(path, "wb") as f:
         f.write(b"VPFFTIN1")
-        f.write(np.array([nx, ny, nz, c.nsteps, c.max_iter, per_voxel, 0, 0], "<i4").tobytes())
+        f.write(np.array([nx, ny, nz, c.nsteps, c.max_iter, per_voxel, per_inc, generated],
+                         "<i4").tobytes())
         f.write(np.array([c.dt, c.eps], "<f8").tobytes())
         f.write(np.asarray(c.edot, "<f8").reshape(5).tobytes())
         f.write(np.asarray(c.h, "<f8").reshape(3).tobytes())
@@ -88,9 +119,12 @@ def write_input(path: str, c: Case) -> None:
         for a in (m.tau0, m.tau1, m.theta0, m.theta1):
             f.write(np.asarray(a, "<f8").reshape(12).tobytes())
         f.write(np.asarray(m.hardening, "<f8").reshape(144).tobytes())
-        f.write(np.ascontiguousarray(c.R, "<f8").reshape(n * 9).tobytes())
-        f.write(np.ascontiguousarray(c.sigma, "<f8").reshape(n * 5).tobytes())
+        if not generated:
+            f.write(np.ascontiguousarray(c.R, "<f8").reshape(n * 9).tobytes())
+            f.write(np.ascontiguousarray(c.sigma, "<f8").reshape(n * 5).tobytes())
         f.write(np.ascontiguousarray(c.crss, "<f8").reshape(-1).tobytes())
+        if per_inc:
+            f.write(np.ascontiguousarray(c.edot_steps, "<f8").reshape(c.nsteps * 5).tobytes())
 
 
 def _rd(outdir, name, shape=None):
@@ -98,6 +132,8 @@ def _rd(outdir, name, shape=None):
     if not os.path.exists(p):
         return None
     a = np.fromfile(p, "<f8")
+    if shape is not None and a.size == 0:
+        return None  # not recorded (--timing-only)
     return a.reshape(shape) if shape is not None else a
 
 
@@ -112,6 +148,7 @@ def read_output(outdir: str, n: int) -> dict:
     out["step_seconds"] = _rd(outdir, "step_seconds.bin")
     out["fwd_times"] = _rd(outdir, "fwd_times.bin")
     out["fwd_increment"] = _rd(outdir, "fwd_increment.bin")
+    out["fwd_fft_seconds"] = _rd(outdir, "fwd_fft_seconds.bin")
     for name, w in (("sigma", 5), ("lambda", 5), ("R", 9), ("crss", 12), ("P_last", 5),
                     ("dtilde_last", 5), ("schmid", 60)):
         out[name] = _rd(outdir, name + ".bin", (n, w))
@@ -157,13 +194,16 @@ def iteration_history(out: dict, dims, edot) -> list:
     """Per increment, per fixed-point iteration: (<sigma>, <edot>, delta_sigma,
     delta_eps) formed from the reduced sums exactly as the reference does
     (MaterialGrid.cpp:1009-1053): sums / N, then the error norms divided by
-    |<sigma>| and |Edot|."""
+    |<sigma>| and |Edot|.  `edot` is one strain rate (5,) or one per
+    increment (nsteps, 5)."""
     nx, ny, nz = dims
     n = float(nx * ny * nz)
-    en = np.sqrt(_inner(edot, edot))
+    edots = np.asarray(edot, np.float64).reshape(-1, 5)
     ar = out["allreduce"]
     hist, off = [], 0
-    for cnt in out["allreduce_counts"]:
+    for k, cnt in enumerate(out["allreduce_counts"]):
+        e_k = edots[k if len(edots) > 1 else 0]
+        en = np.sqrt(_inner(e_k, e_k))
         its = []
         vals = ar[off + 25: off + cnt].reshape(-1, 12)
         for row in vals:
@@ -178,7 +218,10 @@ def iteration_history(out: dict, dims, edot) -> list:
 
 
 def run(binary: str, case: Case, workdir: str, dump_iters=(), dump_increments=False,
-        timeout=None) -> dict:
+        timeout=None, run_vpfft=False, extra_args=()) -> dict:
+    """Run an oracle CLI on `case` in `workdir` and read its outputs.
+    run_vpfft: drive the increments through the reference's own RunVPFFT
+    (reference build only), which also writes workdir/Stress_Strain.txt."""
     os.makedirs(workdir, exist_ok=True)
     inp = os.path.join(workdir, "input.bin")
     write_input(inp, case)
@@ -187,6 +230,9 @@ def run(binary: str, case: Case, workdir: str, dump_iters=(), dump_increments=Fa
         cmd += ["--dump-iter", str(int(k))]
     if dump_increments:
         cmd += ["--dump-increments"]
+    if run_vpfft:
+        cmd += ["--run-vpfft"]
+    cmd += [str(a) for a in extra_args]
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
     if r.returncode != 0:
         raise RuntimeError(f"{binary} failed ({r.returncode}): {r.stderr[-2000:]}")

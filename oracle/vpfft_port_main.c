@@ -119,7 +119,7 @@ int main(int argc, char **argv) {
   int32_t hdr[8];
   rd(f, hdr, 4, 8);
   int nx = hdr[0], ny = hdr[1], nz = hdr[2], nsteps = hdr[3], max_iter = hdr[4],
-      per_voxel = hdr[5];
+      per_voxel = hdr[5], edot_per_increment = hdr[6];
   double dt, eps, edot[5], h[3];
   rd(f, &dt, 8, 1);
   rd(f, &eps, 8, 1);
@@ -143,6 +143,11 @@ int main(int argc, char **argv) {
   rd(f, R, 8, 9 * n);
   rd(f, sig, 8, 5 * n);
   rd(f, crss, 8, ncrss);
+  double *edot_steps = NULL;
+  if (edot_per_increment) {
+    edot_steps = (double *)malloc(sizeof(double) * 5 * (size_t)nsteps);
+    rd(f, edot_steps, 8, 5 * (size_t)nsteps);
+  }
   fclose(f);
 
   oracle_grid *g = oracle_grid_create(nx, ny, nz, &mat);
@@ -163,6 +168,7 @@ int main(int argc, char **argv) {
     for (int i = 0; i < 25; ++i) push(&c, 0.0);
     double avg[5];
     push_fwd(&c);
+    if (edot_steps) memcpy(edot, edot_steps + 5 * (size_t)s, sizeof(edot));
     int it = oracle_grid_run_increment(g, edot, max_iter, dt, eps, avg);
     double t1 = now_s();
     if (it < 0) die("MaxRSS < 1e-10 during initialisation");

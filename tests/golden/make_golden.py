@@ -67,31 +67,99 @@ CASES = {
                   max_iter=100, dt=0.005, eps=1e-5, h=(1.0, 1.0, 1.0), dump_iters=(),
                   sample=4096, sample_stride=4, store_increments=(0, 4, 9, 14, 19)),
 }
-SMALL = ["c1_16", "hard_16", "odd_15x12x10", "n20_16"]
+# Input classes of the batched and serving workloads and of the solver's less
+# common paths, each against the reference build:
+CASES.update({
+    # random traceless velocity gradients (Gaussian entries, symmetric part
+    # scaled to equivalent strain rate 1), a different one per increment, as
+    # the serving workload applies to a persistent RVE; Voce + texture between
+    "shear_16": dict(dims=(16, 16, 16), grains=20, seed=21, n=10, L_seed=101, nsteps=2,
+                     max_iter=100, dt=0.005, eps=1e-5, h=(1.0, 1.0, 1.0), dump_iters=(0, 1)),
+    # the same recipe on an edge that takes the runtime-plan FFT engine (24)
+    "shear_24": dict(dims=(24, 24, 24), grains=40, seed=23, n=10, L_seed=103, nsteps=1,
+                     max_iter=100, dt=0.005, eps=1e-5, h=(1.0, 1.0, 1.0), dump_iters=()),
+    # a rate exponent with no compile-time kernel (n = 7), per-voxel random
+    # orientations and CRSS, gdot0 = 1.3, a full 5-component strain rate,
+    # anisotropic voxels, two increments
+    "rich_n7": dict(dims=(12, 10, 9), orient="random", orient_seed=5, crss="random", gdot=1.3,
+                    n=7, edot=(0.3, -0.7, 0.2, 0.1, -0.4), nsteps=2, max_iter=30, dt=0.01,
+                    eps=1e-6, h=(1.0, 0.7, 1.2), dump_iters=()),
+    # the linear (n = 1) branch of the constitutive law (Solvers.cpp:177-180)
+    "n1_16": dict(dims=(16, 16, 16), grains=8, seed=31, n=1, L=UNIAXIAL, nsteps=1, max_iter=50,
+                  dt=0.005, eps=1e-5, h=(1.0, 1.0, 1.0), dump_iters=()),
+})
+SMALL = ["c1_16", "hard_16", "odd_15x12x10", "n20_16", "shear_16", "shear_24", "rich_n7",
+         "n1_16"]
+
+# RunVPFFT (MaterialGrid.cpp:1202-1228) itself, for its Stress_Strain.txt
+STRESS_STRAIN = dict(dims=(16, 16, 16), grains=8, seed=1, n=10, L=UNIAXIAL, nsteps=3,
+                     max_iter=30, dt=0.005, eps=1e-5, h=(1.0, 1.0, 1.0))
+
+
+def random_orientations(n: int, seed: int) -> np.ndarray:
+    """Per-voxel uniform random rotations (normalised Gaussian quaternions),
+    row-major 3x3: (n, 9)."""
+    rng = np.random.default_rng(seed)
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    return np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y),
+                     2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x),
+                     2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)], axis=1)
+
+
+def case_inputs(c: dict):
+    """(R, crss, material, edot, edot_steps, velocity gradients) of a case."""
+    nx, ny, nz = c["dims"]
+    n = nx * ny * nz
+    if c.get("orient") == "random":
+        R = random_orientations(n, c["orient_seed"])
+    else:
+        R = fixtures.polycrystal(nx, ny, nz, c["grains"], c["seed"])
+    if c.get("crss") == "random":
+        crss = np.random.default_rng(c["orient_seed"] + 1).uniform(0.8, 1.3, size=(n, 12))
+    else:
+        crss = np.ones(12)
+    mat = refio.Material.uniform(c.get("gdot", 1.0), c["n"], VOCE["tau0"], VOCE["tau1"],
+                                 VOCE["theta0"], VOCE["theta1"], VOCE["h"])
+    edot_steps, Ls = None, None
+    if "L_seed" in c:
+        rng = np.random.default_rng(c["L_seed"])
+        Ls = np.array([fixtures.random_traceless_velocity_gradient(rng)
+                       for _ in range(c["nsteps"])])
+        edot_steps = np.array([edot_of(L) for L in Ls])
+        edot = edot_steps[0]
+    elif "edot" in c:
+        edot = np.array(c["edot"], np.float64)
+    else:
+        Ls = np.asarray(c["L"])[None]
+        edot = edot_of(c["L"])
+    return R, crss, mat, edot, edot_steps, Ls
 
 
 def make_case(name: str, binary: str = refio.REF_BIN) -> str:
     c = CASES[name]
     nx, ny, nz = c["dims"]
     n = nx * ny * nz
-    R = fixtures.polycrystal(nx, ny, nz, c["grains"], c["seed"])
-    mat = refio.Material.uniform(1.0, c["n"], VOCE["tau0"], VOCE["tau1"], VOCE["theta0"],
-                                 VOCE["theta1"], VOCE["h"])
-    edot = edot_of(c["L"])
-    case = refio.Case(c["dims"], R, np.zeros((n, 5)), np.ones(12), mat, edot, nsteps=c["nsteps"],
-                      max_iter=c["max_iter"], dt=c["dt"], eps=c["eps"], h=c["h"])
+    R, crss, mat, edot, edot_steps, Ls = case_inputs(c)
+    case = refio.Case(c["dims"], R, np.zeros((n, 5)), crss, mat, edot, nsteps=c["nsteps"],
+                      max_iter=c["max_iter"], dt=c["dt"], eps=c["eps"], h=c["h"],
+                      edot_steps=edot_steps)
     sample = c.get("sample")
     with tempfile.TemporaryDirectory() as td:
         out = refio.run(binary, case, td, dump_iters=c["dump_iters"],
                         dump_increments=sample is not None)
-    hist = refio.iteration_history(out, c["dims"], edot)
+    hist = refio.iteration_history(out, c["dims"], edot if edot_steps is None else edot_steps)
     L0s = refio.l0_per_increment(out, nx)
     rec = dict(
-        dims=np.array(c["dims"]), grains=np.array(c["grains"]), seed=np.array(c["seed"]),
-        rate_sensitivity=np.array(c["n"]), gamma_dot_base=np.array(1.0), crss0=np.array(1.0),
+        dims=np.array(c["dims"]), grains=np.array(c.get("grains", 0)),
+        seed=np.array(c.get("seed", c.get("orient_seed", 0))),
+        rate_sensitivity=np.array(c["n"]), gamma_dot_base=np.array(c.get("gdot", 1.0)),
+        crss0=np.array(1.0),
         tau0=np.array(VOCE["tau0"]), tau1=np.array(VOCE["tau1"]), theta0=np.array(VOCE["theta0"]),
         theta1=np.array(VOCE["theta1"]), hardening=np.array(VOCE["h"]),
-        velocity_gradient=np.asarray(c["L"]), edot=edot, nsteps=np.array(c["nsteps"]),
+        velocity_gradient=np.zeros((0, 3, 3)) if Ls is None else Ls, edot=edot,
+        nsteps=np.array(c["nsteps"]),
         max_iter=np.array(c["max_iter"]), dt=np.array(c["dt"]), eps=np.array(c["eps"]),
         h=np.array(c["h"]), iters=out["iters"], avg_stress=out["avg_stress"],
         hist_counts=np.array([len(h) for h in hist]),
@@ -100,6 +168,10 @@ def make_case(name: str, binary: str = refio.REF_BIN) -> str:
         R_in_sha256=np.array(hashlib.sha256(np.ascontiguousarray(R).tobytes()).hexdigest()),
         oracle=np.array(os.path.basename(binary)),
     )
+    if edot_steps is not None:
+        rec["edot_steps"] = edot_steps
+    if np.asarray(crss).ndim == 2:
+        rec["crss_in"] = crss
     if sample is None:
         rec.update(R_in=R, sigma=out["sigma"], **{"lambda": out["lambda"]}, R=out["R"],
                    crss=out["crss"], accshear=out["accshear"], P_last=out["P_last"],
@@ -124,9 +196,31 @@ def make_case(name: str, binary: str = refio.REF_BIN) -> str:
     return path
 
 
+def make_stress_strain(binary: str = refio.REF_BIN) -> str:
+    """Stress_Strain.txt written by the reference's RunVPFFT, and its inputs."""
+    c = STRESS_STRAIN
+    nx, ny, nz = c["dims"]
+    n = nx * ny * nz
+    R, crss, mat, edot, _, _ = case_inputs(c)
+    case = refio.Case(c["dims"], R, np.zeros((n, 5)), crss, mat, edot, nsteps=c["nsteps"],
+                      max_iter=c["max_iter"], dt=c["dt"], eps=c["eps"], h=c["h"])
+    with tempfile.TemporaryDirectory() as td:
+        refio.run(binary, case, td, run_vpfft=True)
+        with open(os.path.join(td, "Stress_Strain.txt"), "rb") as fh:
+            text = fh.read()
+    path = os.path.join(HERE, "io", "stress_strain_16.txt")
+    with open(path, "wb") as fh:
+        fh.write(text)
+    return path
+
+
 def main(argv):
-    names = argv or SMALL
+    names = argv or SMALL + ["stress_strain"]
     for nm in names:
+        if nm == "stress_strain":
+            p = make_stress_strain()
+            print(nm, "->", os.path.relpath(p, ROOT))
+            continue
         p = make_case(nm)
         print(nm, "->", os.path.relpath(p, ROOT), f"{os.path.getsize(p) / 1e6:.2f} MB")
 

@@ -9,7 +9,8 @@ import pytest
 
 from oracle import portlib, refio
 
-SMALL = ["c1_16", "hard_16", "odd_15x12x10", "n20_16"]
+SMALL = ["c1_16", "hard_16", "odd_15x12x10", "n20_16", "shear_16", "shear_24", "rich_n7",
+         "n1_16"]
 
 
 def case_from_golden(g):
@@ -18,21 +19,24 @@ def case_from_golden(g):
     mat = refio.Material.uniform(float(g["gamma_dot_base"]), int(g["rate_sensitivity"]),
                                  float(g["tau0"]), float(g["tau1"]), float(g["theta0"]),
                                  float(g["theta1"]), float(g["hardening"]))
-    return refio.Case(dims, g["R_in"], np.zeros((n, 5)), np.full(12, float(g["crss0"])), mat,
+    crss = g["crss_in"] if "crss_in" in g else np.full(12, float(g["crss0"]))
+    return refio.Case(dims, g["R_in"], np.zeros((n, 5)), crss, mat,
                       g["edot"], nsteps=int(g["nsteps"]), max_iter=int(g["max_iter"]),
-                      dt=float(g["dt"]), eps=float(g["eps"]), h=tuple(g["h"]))
+                      dt=float(g["dt"]), eps=float(g["eps"]), h=tuple(g["h"]),
+                      edot_steps=g.get("edot_steps"))
 
 
 @pytest.mark.parametrize("name", SMALL)
 def test_port_reproduces_reference_golden_bitwise(name, golden, port):
     g = golden(name)
     case = case_from_golden(g)
-    dump = (0, 1, 2) if name == "c1_16" else ()
+    dump = {"c1_16": (0, 1, 2), "shear_16": (0, 1)}.get(name, ())
     with tempfile.TemporaryDirectory() as td:
         out = refio.run(refio.PORT_BIN, case, td, dump_iters=dump)
     assert np.array_equal(out["iters"], g["iters"])
     assert np.array_equal(out["avg_stress"], g["avg_stress"])
-    hist = refio.iteration_history(out, case.dims, case.edot)
+    hist = refio.iteration_history(out, case.dims,
+                                   case.edot if case.edot_steps is None else case.edot_steps)
     rows = np.array([np.concatenate([s, e, [a, b]]) for h in hist for (s, e, a, b) in h])
     assert np.array_equal(rows, g["history"])
     assert np.array_equal(np.array(refio.l0_per_increment(out, case.dims[0])), g["L0"])
@@ -159,7 +163,64 @@ def test_golden_inputs_reproducible(golden, lib):
 
     for name in SMALL:
         g = golden(name)
+        if int(g["grains"]) == 0:  # per-voxel random orientations, not a polycrystal
+            continue
         dims = tuple(int(x) for x in g["dims"])
         R = fixtures.polycrystal(*dims, int(g["grains"]), int(g["seed"]))
         assert np.array_equal(R, g["R_in"]), name
         assert hashlib.sha256(R.tobytes()).hexdigest() == str(g["R_in_sha256"])
+
+
+def test_oracle_polycrystal_equals_product_generator(port, lib):
+    """The oracle-side generator (which lets the reference make its own
+    benchmark inputs) gives the product's fixture bit for bit."""
+    from vpfft_b200 import fixtures
+
+    for dims, grains, seed in [((16, 16, 16), 8, 1), ((15, 12, 10), 6, 3), ((7, 5, 3), 40, 9),
+                               ((33, 20, 17), 200, 5), ((1, 1, 1), 1, 0),
+                               ((96, 64, 48), 1000, 2024)]:
+        a, ga = portlib.polycrystal(*dims, grains, seed, threads=4, with_grains=True)
+        b, gb = fixtures.polycrystal(*dims, grains, seed, with_grains=True)
+        assert np.array_equal(a, b), dims
+        assert np.array_equal(ga, gb), dims
+
+
+@pytest.mark.skipif(not os.path.exists(refio.REF_BIN), reason="reference build not present")
+def test_reference_as_several_ranks(port):
+    """The reference run as P MPI ranks through the multi-process stand-ins
+    (slab decomposition along x, uneven slabs and an empty rank included)
+    agrees with the one-rank run: equal iteration counts, every reduced value
+    within 1e-13 relative (only the order of the cross-rank sums differs), and
+    the generated inputs equal explicit ones."""
+    from vpfft_b200 import fixtures
+
+    dims = (16, 12, 10)
+    n = int(np.prod(dims))
+    mat = refio.Material.uniform(1.0, 10, 1.0, 0.5, 20.0, 1.0)
+    edot = fixtures.edot_from_matrix(np.diag([1.0, 0.0, -1.0]))
+    gen = refio.Case(dims, None, None, np.ones(12), mat, edot, nsteps=2, max_iter=12, dt=0.005,
+                     eps=1e-5)
+    runs = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for ranks in (1, 2, 3, 5):
+            runs[ranks] = refio.run(refio.REF_BIN, gen, os.path.join(tmp, str(ranks)),
+                                    extra_args=["--generate", 7, 11, "--ranks", ranks,
+                                                "--timing-only"])
+        explicit = refio.Case(dims, portlib.polycrystal(*dims, 7, 11), np.zeros((n, 5)),
+                              np.ones(12), mat, edot, nsteps=2, max_iter=12, dt=0.005, eps=1e-5)
+        one = refio.run(refio.REF_BIN, explicit, os.path.join(tmp, "explicit"))
+    assert np.array_equal(one["allreduce"], runs[1]["allreduce"])
+    for ranks, out in runs.items():
+        assert np.array_equal(out["iters"], one["iters"]), ranks
+        scale = np.abs(one["allreduce"]).max()
+        assert np.abs(out["allreduce"] - one["allreduce"]).max() <= 1e-13 * scale, ranks
+        assert len(out["fwd_times"]) == len(one["fwd_times"])
+
+
+def test_oracle_edot_projection_equals_product(lib):
+    from vpfft_b200 import fixtures
+
+    rng = np.random.default_rng(4)
+    for L in [np.diag([1.0, 0.0, -1.0]), np.diag([1.0, -0.5, -0.5])] + \
+            [fixtures.random_traceless_velocity_gradient(rng) for _ in range(5)]:
+        assert np.array_equal(refio.edot_from_matrix(L), fixtures.edot_from_matrix(L))

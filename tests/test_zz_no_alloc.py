@@ -63,6 +63,23 @@ def test_noalloc_matches_allocating_entry_point_twice(lib, golden):
     assert cnt > 0
 
 
+def test_noalloc_second_call_allocates_nothing(lib, golden):
+    """After the set-up call, a call leaves the device's free memory exactly as
+    it was (cudaMemGetInfo through torch, which shares the primary context)."""
+    import torch
+
+    torch.cuda.init()
+    torch.cuda.mem_get_info(0)
+    n = 1024
+    args = _inputs(golden, n, 21)
+    _call(lib, lib.vpfft_solve_constrained_constitutive_noalloc, args, n, 100, True)  # set-up
+    free0, _ = torch.cuda.mem_get_info(0)
+    out, _, _ = _call(lib, lib.vpfft_solve_constrained_constitutive_noalloc, args, n, 100, True)
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0, (free0, free1)
+    assert np.all(np.isfinite(out))
+
+
 def test_noalloc_refuses_oversize_batch(lib, golden):
     n = capi.NOALLOC_MAX_POINTS + 1
     z5, z60, z12 = np.zeros((n, 5)), np.zeros((n, 60)), np.zeros((n, 12))

@@ -27,6 +27,7 @@ class BatchResult:
     stress_error: float
     strain_rate_error: float
     nr_not_converged: int
+    status_bits: int
     seconds_queued: float
     seconds_total: float
 
@@ -113,7 +114,8 @@ class Batch:
             out.append(BatchResult(int(r.request_id), int(r.status), int(r.iterations),
                                    bool(r.converged), np.array(r.avg_stress[:]),
                                    float(r.stress_error), float(r.strain_rate_error),
-                                   int(r.nr_not_converged), float(r.seconds_queued),
+                                   int(r.nr_not_converged), int(r.status_bits),
+                                   float(r.seconds_queued),
                                    float(r.seconds_total)))
         return out
 

@@ -30,8 +30,12 @@ ERR_NONFINITE = 7
 ERR_NOT_INITIALIZED = 8
 ERR_IO = 9
 ERR_CANCELLED = 10
-ERR_TIMEOUT = 11
 ERR_BUSY = 12
+# bits of Stats.status_bits / BatchResult.status_bits (include/vpfft_capi.h)
+STATUS_MAX_RSS_TINY = 0x1
+STATUS_NONFINITE = 0x2
+STATUS_LOOP_NOT_CONVERGED = 0x100
+STATUS_NR_CAPPED = 0x200
 
 PREC_FP64 = 0
 PREC_MIXED = 1
@@ -143,7 +147,7 @@ class BatchResult(C.Structure):
         ("status", C.c_int32),
         ("iterations", C.c_int32),
         ("converged", C.c_int32),
-        ("pad_", C.c_int32),
+        ("status_bits", C.c_int32),
         ("avg_stress", C.c_double * 5),
         ("stress_error", C.c_double),
         ("strain_rate_error", C.c_double),

@@ -19,6 +19,7 @@
 // launches', so every slot's sums are formed in the same order as when it is
 // solved alone.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <chrono>
@@ -262,6 +263,8 @@ void record(vpfft_batch* b, const Active& a, vpfft_status st, double t_end) {
     r.stress_error = c.last[10];
     r.strain_rate_error = c.last[11];
     r.nr_not_converged = (int64_t)c.nr_capped;
+    r.status_bits = c.status | (r.converged ? 0 : VPFFT_STATUS_LOOP_NOT_CONVERGED) |
+                    (c.nr_capped ? VPFFT_STATUS_NR_CAPPED : 0);
   }
   r.seconds_queued = a.r.t_admit - a.r.t_submit;
   r.seconds_total = t_end - a.r.t_submit;
@@ -862,7 +865,9 @@ vpfft_status vpfft_batch_submit(vpfft_batch* b, vpfft_grid* g, const double edot
 
 vpfft_status vpfft_batch_step(vpfft_batch* b, int* pending) {
   if (!b) return bfail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "NULL batch");
+  nvtxRangePushA("vpfft batch tick");  // NVTX range per tick (Nsight timelines)
   vpfft_status s = b->prec == VPFFT_PREC_FP64 ? tick<double>(b) : tick<float>(b);
+  nvtxRangePop();
   if (pending) *pending = (int)(b->queue.size() + b->active.size());
   return s;
 }

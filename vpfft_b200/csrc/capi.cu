@@ -8,6 +8,7 @@
 // device.  There is no CPU fallback: without a CUDA device every entry point
 // that needs one returns VPFFT_ERR_NO_DEVICE.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <chrono>
 #include <cmath>
@@ -20,6 +21,19 @@
 
 using namespace vpfft;
 using namespace vpfft::grid_ops;
+
+// NVTX range over one phase of a solve (initialisation, reference medium,
+// fixed-point loop, post-increment update), visible in Nsight timelines.
+struct PhaseRange {
+  explicit PhaseRange(const char* name) { nvtxRangePushA(name); }
+  ~PhaseRange() { nvtxRangePop(); }
+  PhaseRange(const PhaseRange&) = delete;
+  PhaseRange& operator=(const PhaseRange&) = delete;
+};
+
+static_assert(VPFFT_STATUS_MAX_RSS_TINY == vpfft::kStatusMaxRssTiny &&
+                  VPFFT_STATUS_NONFINITE == vpfft::kStatusNonFinite,
+              "device status bits and the C ABI's bits agree");
 
 namespace {
 
@@ -355,6 +369,7 @@ vpfft_status from_device_field(vpfft_grid* g, const S* src, int width, double* h
 // ---------------------------------------------------------------- phases
 template <typename S>
 vpfft_status do_init(vpfft_grid* g, const double edot[5]) {
+  PhaseRange range("vpfft InitializeComputation");
   if (!g->fields_set) return fail(g, VPFFT_ERR_NOT_INITIALIZED, "fields not set");
   NRParams p = nr_params(g, edot, true);
   IterCtrl h{};
@@ -375,6 +390,7 @@ vpfft_status do_init(vpfft_grid* g, const double edot[5]) {
 
 template <typename S>
 vpfft_status do_ref_medium(vpfft_grid* g, double* L0_out) {
+  PhaseRange range("vpfft BuildLinearRefMediumStiffness");
   VoxelParams p = voxel_params(g, g->last_edot);
   g->launches += launch_ref_medium<S>(p, fields<S>(g), g->partials, g->sum25, g->stream);
   CKL(g);
@@ -389,6 +405,7 @@ vpfft_status do_ref_medium(vpfft_grid* g, double* L0_out) {
 template <typename S>
 vpfft_status do_fixed_point(vpfft_grid* g, const double edot[5], int max_iter, double eps,
                             double* history, vpfft_stats* st) {
+  PhaseRange range("vpfft fixed-point loop");
   if (!g->have_L0) return fail(g, VPFFT_ERR_NOT_INITIALIZED, "reference medium not built");
   if (vpfft_status r = ensure_hist(g, max_iter)) return r;
   if (vpfft_status r = ensure_spectrum(g)) return r;
@@ -481,7 +498,8 @@ vpfft_status do_fixed_point(vpfft_grid* g, const double edot[5], int max_iter, d
     st->converged = (c.last[10] <= eps && c.last[11] <= eps) ? 1 : 0;
     for (int k = 0; k < 5; ++k) st->avg_strain_rate[k] = c.last[5 + k];
     st->nr_not_converged = (int64_t)c.nr_capped;
-    st->status_bits = c.status;
+    st->status_bits = c.status | (st->converged ? 0 : VPFFT_STATUS_LOOP_NOT_CONVERGED) |
+                      (c.nr_capped ? VPFFT_STATUS_NR_CAPPED : 0);
     std::memcpy(st->L0, g->L0, sizeof(g->L0));
   }
   if (c.status & kStatusNonFinite) return fail(g, VPFFT_ERR_NONFINITE, "non-finite stress or strain rate");
@@ -492,6 +510,7 @@ vpfft_status do_fixed_point(vpfft_grid* g, const double edot[5], int max_iter, d
 
 template <typename S>
 vpfft_status do_post(vpfft_grid* g, const double edot[5], double dt) {
+  PhaseRange range("vpfft post-increment (texture, voxel length, hardening)");
   vpfft_status s = ensure_crss_array(g);
   if (s != VPFFT_OK) return s;
   PostParams p = post_params(g, dt);
@@ -555,7 +574,6 @@ const char* vpfft_status_string(vpfft_status s) {
     case VPFFT_ERR_NOT_INITIALIZED: return "not initialized";
     case VPFFT_ERR_IO: return "I/O or parse error";
     case VPFFT_ERR_CANCELLED: return "cancelled";
-    case VPFFT_ERR_TIMEOUT: return "timeout";
     case VPFFT_ERR_BUSY: return "grid busy in a batch";
   }
   return "unknown status";
@@ -948,10 +966,16 @@ vpfft_status vpfft_grid_restore(vpfft_grid* g, const void* buf, size_t size) {
     return fail(g, VPFFT_ERR_INVALID_ARGUMENT, "snapshot voxel lengths must be > 0");
   const double* d =
       reinterpret_cast<const double*>(static_cast<const unsigned char*>(buf) + sizeof(hd));
+  // From here the grid's fields are overwritten one at a time: if a copy
+  // fails part-way the grid holds a mix of old and new state, so it is marked
+  // unusable (no fields, no reference medium) until it is restored or its
+  // fields are set again.
   for (const SnapField& sf : kSnapFields) {
-    if (sf.f == VPFFT_FIELD_CRSS) {
-      if (vpfft_status s = vpfft_grid_set_crss(g, crss_pv ? d : nullptr)) return s;
-    } else if (vpfft_status s = vpfft_grid_set_field(g, sf.f, d)) {
+    vpfft_status s = sf.f == VPFFT_FIELD_CRSS ? vpfft_grid_set_crss(g, crss_pv ? d : nullptr)
+                                              : vpfft_grid_set_field(g, sf.f, d);
+    if (s != VPFFT_OK) {
+      g->fields_set = false;
+      g->have_L0 = false;
       return s;
     }
     if (sf.f != VPFFT_FIELD_CRSS || crss_pv) d += (size_t)sf.width * (size_t)g->n;

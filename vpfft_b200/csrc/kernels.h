@@ -51,6 +51,8 @@ struct IterCtrl {
   unsigned long long nr_capped;
   double last[12];    // <sigma>(5), <edot>(5), delta_sigma, delta_eps of the last iteration
 };
+// device-side bits of IterCtrl::status; the same values as VPFFT_STATUS_MAX_RSS_TINY
+// and VPFFT_STATUS_NONFINITE of the C ABI (static_assert in capi.cu)
 enum : int32_t { kStatusMaxRssTiny = 1, kStatusNonFinite = 2 };
 
 // Division of 32-bit unsigned t < 2^31 by a fixed d >= 1 without a divide:
@@ -245,6 +247,9 @@ template <typename S>
 int launch_spectral_chain(const SlotDesc<S>* d, const PassChain& c, cudaStream_t st);
 
 // --- batched solver entry points for testing (double, voxel-major) ---------
+// Loads the code of the batched Solvers kernels on the current device now
+// (under lazy module loading it would load, and allocate, at first launch).
+cudaError_t load_solvers_kernels();
 int launch_solvers_constrained(int n, const double* s0, const double* schmid, const double* crss,
                                const MaterialParams& mp, const double edot[5],
                                const double* lambda, const double* dtilde, const double L0[25],

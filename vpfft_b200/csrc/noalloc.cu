@@ -13,16 +13,24 @@
 // Limits and rules:
 //  * at most VPFFT_NOALLOC_MAX_POINTS points per call (larger n is refused
 //    with VPFFT_ERR_UNSUPPORTED_SIZE; split the batch);
-//  * the first call on each device looks up the array's device address
-//    (cudaGetSymbolAddress, with that device current); make that first call
-//    before any stream capture begins;
+//  * the first call on each device sets up: it looks up the array's device
+//    address (cudaGetSymbolAddress, with that device current) and makes the
+//    CUDA runtime load the array and the kernels this call launches.  Under
+//    the runtime's default lazy module loading that load is what allocates
+//    (about 3 MiB per device), so make the first call -- one with n = 0 is
+//    enough -- before the caller's memory pool takes the device; later calls
+//    allocate nothing;
+//  * every copy and launch of a call runs on the legacy default stream, so no
+//    call may overlap a stream capture anywhere in the process, on any
+//    device, and a call is ordered after the work of the caller's blocking
+//    streams (only streams made with cudaStreamNonBlocking are not stalled);
 //  * there is one array per device per process, so two calls that overlapped
 //    in time would race on it: the entry point holds a process-wide lock for
 //    the whole call, and concurrent callers run one after another;
 //  * the array keeps the previous call's contents; the only value that must
 //    start at zero (the count of non-converged points) is cleared each call;
-//  * the call waits for its own work on the legacy default stream, not for
-//    the whole device; it does not return until the results are on the host.
+//  * the call synchronises the legacy default stream, not the whole device,
+//    and does not return until the results are on the host.
 //  * the looked-up address belongs to the device's primary context: after a
 //    cudaDeviceReset the library (its grids, batches and this entry point)
 //    must not be used again in the process.
@@ -91,6 +99,11 @@ vpfft_status scratch_for_current_device(double** out) {
   if (!g_scratch_ptr[dev]) {
     void* p = nullptr;
     NA_CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    // load this unit's count kernel and the solve kernels now, not at the
+    // first launch of a later call
+    cudaFuncAttributes attr;
+    NA_CK(cudaFuncGetAttributes(&attr, k_count_not_converged));
+    NA_CK(vpfft::load_solvers_kernels());
     g_scratch_ptr[dev] = static_cast<double*>(p);
   }
   *out = g_scratch_ptr[dev];
@@ -119,11 +132,11 @@ extern "C" vpfft_status vpfft_solve_constrained_constitutive_noalloc(
                            "no CUDA device available (vpfft_b200 has no CPU fallback)");
   }
   if (not_converged) *not_converged = 0;
-  if (n == 0) return VPFFT_OK;
 
   std::lock_guard<std::mutex> lock(g_noalloc_lock);
   double* base = nullptr;
   if (vpfft_status s = scratch_for_current_device(&base)) return s;
+  if (n == 0) return VPFFT_OK;
   double* d_s0 = base + kOffS0;
   double* d_schmid = base + kOffSchmid;
   double* d_crss = base + kOffCrss;

@@ -157,7 +157,7 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const C& cs, l
 #pragma unroll
     for (int c = 0; c < 5; ++c) ed[c] = cs.edot(c) + d[c];
     double e[5];
-    bool capped;
+    bool capped, cert = false;
     if constexpr (sizeof(S) == 4) {
       // mixed precision: an FP32 Newton predictor from the previous stress,
       // then the FP64 solve from its iterate (normally one Newton step with
@@ -168,23 +168,35 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const C& cs, l
       double s0[5];
 #pragma unroll
       for (int c = 0; c < 5; ++c) s0[c] = s[c];
+#ifdef VPFFT_EXP_CERT
+      float fac[15];
+      const bool ok = nr_predict_fp32<NEXP, kTauSmem, kFull>(msm, tsm, bs, p, cs, lam, ed, s, 8,
+                                                             &mx0, fac, VPFFT_EXP_PRED_TOL);
+      cert = ok && fp64_residual_certifies<NEXP, kTauSmem>(
+                                  msm, tsm, bs, p, cs, lam, ed, s, fac,
+                                  VPFFT_EXP_CERT * VPFFT_EXP_CERT, e);
+#else
       const bool ok =
           nr_predict_fp32<NEXP, kTauSmem, kFull>(msm, tsm, bs, p, cs, lam, ed, s, 8, &mx0);
+#endif
       if (mx0 < 1e-10f) status |= kStatusMaxRssTiny;
-      if (!ok) {
-        const double mx = max_resolved<kTauSmem>(msm, tsm, bs, p, s0);
+      capped = false;
+      if (!cert) {
+        if (!ok) {
+          const double mx = max_resolved<kTauSmem>(msm, tsm, bs, p, s0);
 #pragma unroll
-        for (int c = 0; c < 5; ++c) s[c] = s0[c] / mx;
-      }
-      double el[5];
-      bool tight;
-      nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, cs, lam, ed, s, nullptr, &capped, el,
-                                          &tight);
-      if (!capped && tight) {
+          for (int c = 0; c < 5; ++c) s[c] = s0[c] / mx;
+        }
+        double el[5];
+        bool tight;
+        nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, cs, lam, ed, s, nullptr, &capped, el,
+                                            &tight);
+        if (!capped && tight) {
 #pragma unroll
-        for (int c = 0; c < 5; ++c) e[c] = el[c];
-      } else {
-        apply_smem<NEXP, kTauSmem>(msm, tsm, bs, p, s, e);
+          for (int c = 0; c < 5; ++c) e[c] = el[c];
+        } else {
+          apply_smem<NEXP, kTauSmem>(msm, tsm, bs, p, s, e);
+        }
       }
     } else {
       const double mx = max_resolved<kTauSmem>(msm, tsm, bs, p, s);
@@ -194,7 +206,11 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const C& cs, l
       nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, cs, lam, ed, s, nullptr, &capped);
       apply_smem<NEXP, kTauSmem>(msm, tsm, bs, p, s, e);
     }
+#ifdef VPFFT_EXP_COUNT
+    capped_count += cert ? 1 : 0;  // experiment: count the certified voxels instead
+#else
     capped_count += capped ? 1 : 0;
+#endif
     double P[5];
 #pragma unroll
     for (int i = 0; i < 5; ++i) {
@@ -494,6 +510,13 @@ static NRParams batch_params(const MaterialParams& mp, const double edot[5], con
   p.max_iter = max_iter;
   set_fp32_copies(p);
   return p;
+}
+
+cudaError_t load_solvers_kernels() {
+  cudaFuncAttributes a;
+  cudaError_t e = cudaFuncGetAttributes(&a, k_solvers_nr<true>);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, k_solvers_nr<false>);
+  return e;
 }
 
 int launch_solvers_constrained(int n, const double* s0, const double* schmid, const double* crss,
