@@ -6,7 +6,7 @@ Each case builds a seeded synthetic microstructure with the product's host-side
 fixture generator (vpfft_b200.fixtures.polycrystal: periodic Voronoi, uniform
 SO(3) orientations), runs the reference's own MaterialGrid code compiled
 against the single-process MPI/FFTW/Eigen stand-ins (oracle/_ref/vpfft_ref,
-built by `make -C oracle ref`), and stores inputs and outputs in
+built by `make -C oracle ref REF_SRC=<reference Src>`), and stores inputs and outputs in
 tests/golden/<case>.npz.  The reference sources are only needed here, when the
 fixtures are (re)generated; the tests read the committed .npz files.
 

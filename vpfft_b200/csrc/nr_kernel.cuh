@@ -380,7 +380,9 @@ __device__ __forceinline__ float2 cpow2(float2 x) {
 // kFull: the pass over the 6 pairs fully unrolled (the single-grid kernel,
 // which has the registers for it: measured 3 % faster) or by 2 (the batched
 // kernel at 4 blocks per SM, where the full unroll spills).
-template <int NEXP, bool kTauSmem, bool kFull = true>
+// kJac = false: S only (K is not touched), for chord steps that reuse an
+// earlier factorisation.
+template <int NEXP, bool kTauSmem, bool kFull = true, bool kJac = true>
 __device__ __forceinline__ bool accumulate_pairs(const float* msm, const float* tsm, int bs,
                                                  const NRParams& p, const float s[5], float S[5],
                                                  float K[15], float* rmax) {
@@ -418,13 +420,18 @@ __device__ __forceinline__ bool accumulate_pairs(const float* msm, const float* 
     const float2 pw = cpow2<NEXP - 1>(make_float2(ax, ay));
     const float2 g = __fmul2_rn(make_float2(p.gdot_f[2 * pq], p.gdot_f[2 * pq + 1]), pw);
     const float2 gr = __fmul2_rn(g, r);
-    const float2 w = __fmul2_rn(__fmul2_rn(nn, g), it);
+    if constexpr (kJac) {
+      const float2 w = __fmul2_rn(__fmul2_rn(nn, g), it);
 #pragma unroll
-    for (int i = 0; i < 5; ++i) {
-      S2[i] = __ffma2_rn(m[i], gr, S2[i]);
-      const float2 mw = __fmul2_rn(m[i], w);
+      for (int i = 0; i < 5; ++i) {
+        S2[i] = __ffma2_rn(m[i], gr, S2[i]);
+        const float2 mw = __fmul2_rn(m[i], w);
 #pragma unroll
-      for (int j = i; j < 5; ++j) K2[sym5(i, j)] = __ffma2_rn(mw, m[j], K2[sym5(i, j)]);
+        for (int j = i; j < 5; ++j) K2[sym5(i, j)] = __ffma2_rn(mw, m[j], K2[sym5(i, j)]);
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 5; ++i) S2[i] = __ffma2_rn(m[i], gr, S2[i]);
     }
   };
   if constexpr (kFull) {
@@ -436,8 +443,10 @@ __device__ __forceinline__ bool accumulate_pairs(const float* msm, const float* 
   }
 #pragma unroll
   for (int c = 0; c < 5; ++c) S[c] = S2[c].x + S2[c].y;
+  if constexpr (kJac) {
 #pragma unroll
-  for (int k = 0; k < 15; ++k) K[k] = K2[k].x + K2[k].y;
+    for (int k = 0; k < 15; ++k) K[k] = K2[k].x + K2[k].y;
+  }
   *rmax = rm;
   return adm;
 }
@@ -451,6 +460,12 @@ __device__ __forceinline__ bool accumulate_pairs(const float* msm, const float* 
 // the inverse pivots 10..14), for the FP64 residual check that follows.
 // kTol: the stopping tolerance on |delta| / |avg| (0: the reference's eps).
 template <int NEXP, bool kTauSmem, bool kFull = true, typename MS, class C>
+__device__ __forceinline__ bool nr_predict_fp32_f(const MS* msm, const MS* tsm, int bs,
+                                                  const NRParams& p, const C& cs,
+                                                  const float l32[5], const float e32[5],
+                                                  float cur[5], int max_steps, float* rmax0,
+                                                  float* fac = nullptr, float tol = 0.f);
+template <int NEXP, bool kTauSmem, bool kFull = true, typename MS, class C>
 __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, int bs,
                                                 const NRParams& p, const C& cs,
                                                 const double lam[5], const double ed[5],
@@ -463,6 +478,22 @@ __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, in
     l32[c] = (float)lam[c];
     e32[c] = (float)ed[c];
   }
+  const bool ok = nr_predict_fp32_f<NEXP, kTauSmem, kFull>(msm, tsm, bs, p, cs, l32, e32, cur,
+                                                           max_steps, rmax0, fac, tol);
+  if (ok) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) s_io[c] = (double)cur[c];
+  }
+  return ok;
+}
+// The predictor on FP32 inputs; cur: the start on entry, the converged
+// iterate on a true return.
+template <int NEXP, bool kTauSmem, bool kFull, typename MS, class C>
+__device__ __forceinline__ bool nr_predict_fp32_f(const MS* msm, const MS* tsm, int bs,
+                                                  const NRParams& p, const C& cs,
+                                                  const float l32[5], const float e32[5],
+                                                  float cur[5], int max_steps, float* rmax0,
+                                                  float* fac, float tol) {
   const float eps = tol > 0.f ? tol : p.eps_f;
   *rmax0 = 0.f;
   for (int it = 0; it < max_steps; ++it) {
@@ -503,11 +534,66 @@ __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, in
     bool bad;
     const bool small = small_step_f32(dn, an, eps, &bad);
     if (bad) return false;
-    if (small) {
+    if (small) return true;
+  }
+  return false;
+}
+
+// Chord variant of the predictor (paired FP32, compile-time exponent): the
+// first step is a full Newton step whose LDL^T factors (fac) are kept; the
+// following steps reuse them and evaluate only the strain-rate sum S.  Same
+// stopping rule; returns true with the iterate in cur when it converged.
+template <int NEXP, bool kTauSmem, bool kFull, class C>
+__device__ __forceinline__ bool nr_predict_chord_f(const float* msm, const float* tsm, int bs,
+                                                   const NRParams& p, const C& cs,
+                                                   const float l32[5], const float e32[5],
+                                                   float cur[5], int max_steps, float* rmax0,
+                                                   float fac[15]) {
+  const float eps = p.eps_f;
+  auto residual = [&](const float S[5], float y[5]) {
 #pragma unroll
-      for (int c = 0; c < 5; ++c) s_io[c] = (double)cur[c];
-      return true;
+    for (int i = 0; i < 5; ++i) {
+      float a = S[i] - e32[i];
+#pragma unroll
+      for (int j = 0; j < 5; ++j) a += cs.L0inv_f(sym5(i, j)) * (cur[j] - l32[j]);
+      y[i] = -a;
     }
+  };
+  auto advance = [&](const float delta[5], bool* bad) {
+    float dn = 0.f, an = 0.f;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      const float nw = cur[c] + delta[c];
+      const float av = (nw + cur[c]) * 0.5f;
+      dn += delta[c] * delta[c];
+      an += av * av;
+      cur[c] = nw;
+    }
+    return small_step_f32(dn, an, eps, bad);
+  };
+  {
+    float S[5], K[15], y[5], delta[5];
+    if (!accumulate_pairs<NEXP, kTauSmem, kFull>(msm, tsm, bs, p, cur, S, K, rmax0)) return false;
+    residual(S, y);
+#pragma unroll
+    for (int k = 0; k < 15; ++k) K[k] += cs.L0inv_f(k);
+    if (!ldlt5_factor(K, fac, fac + 10)) return false;
+    ldlt5_apply(fac, fac + 10, y, delta);
+    bool bad;
+    const bool small = advance(delta, &bad);
+    if (bad) return false;
+    if (small) return true;
+  }
+  for (int it = 1; it < max_steps; ++it) {
+    float S[5], y[5], delta[5], rm;
+    if (!accumulate_pairs<NEXP, kTauSmem, kFull, false>(msm, tsm, bs, p, cur, S, nullptr, &rm))
+      return false;
+    residual(S, y);
+    ldlt5_apply(fac, fac + 10, y, delta);
+    bool bad;
+    const bool small = advance(delta, &bad);
+    if (bad) return false;
+    if (small) return true;
   }
   return false;
 }
