@@ -190,19 +190,18 @@ def test_submit_rejects_mismatched_grid(lib):
 # edges with several batched tile families (compile-time engines up to 96
 # points), one axis with the runtime-plan engine, and a 96-point axis
 TILE_DIMS = [(16, 16, 16), (32, 48, 16), (64, 32, 48), (24, 16, 32), (96, 16, 16)]
-# Mixed precision: the FP32 passes of different tile families are separately
-# compiled kernels whose last bits can differ, and the reference's fixed point
-# (which runs to its iteration cap here) carries such differences along; one
-# case measured 1.2e-9 on <sigma> and 2.2e-5 on the stress field.
-TILE_TOL_MIXED = {"avg": 1e-7, "field": 1e-4}
+# Every tile family (and the single-grid tiles) runs the same arithmetic: the
+# line transforms and the Green operator spell out their fused multiply-adds
+# and their units are built without contraction, so results agree bit for bit
+# in both precisions.
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_fft_tile_families_and_autotuner(lib, precision):
-    """Forced tile families and the autotuned choice: FP64 results are the same
-    bit for bit in every family, mixed results within TILE_TOL_MIXED; the
-    tuning record lists each admitted size once, in admission order, with the
-    timed chain of every family and the fastest one chosen."""
+    """Forced tile families and the autotuned choice: results are the same bit
+    for bit in every family, in FP64 and in mixed precision; the tuning record
+    lists each admitted size once, in admission order, with the timed chain of
+    every family and the fastest one chosen."""
     runs = {}
     for tiles in (2, -1, 0, 1):
         with vp.Batch(precision, material=material(), iterations_per_tick=4,
@@ -239,8 +238,4 @@ def test_fft_tile_families_and_autotuner(lib, precision):
             worst[(tiles, d, "avg")] = rel(rb.avg_stress, ra.avg_stress)
             for k in fa:
                 worst[(tiles, d, k)] = rel(fb[k], fa[k])
-    if precision == "fp64":
-        assert max(worst.values()) == 0.0, max(worst.items(), key=lambda kv: kv[1])
-    else:
-        for key, v in worst.items():
-            assert v <= TILE_TOL_MIXED["avg" if key[2] == "avg" else "field"], (key, v)
+    assert max(worst.values()) == 0.0, max(worst.items(), key=lambda kv: kv[1])

@@ -44,12 +44,20 @@ def _deps() -> float:
     return max((os.path.getmtime(h) for h in hdrs), default=0.0)
 
 
+# The line-transform units are built without floating-point contraction: their
+# product-sums are written out with fused multiply-adds (fmad), so every
+# compiled copy of a pass -- single-grid tiles and each batched tile family --
+# performs the same operations and gives the same bits.
+NO_CONTRACT = {"fft.cu", "fft_fixed_small.cu", "fft_fixed_large.cu"}
+
+
 def _compile(src: str, force: bool, verbose_ptxas: bool) -> tuple[str, str]:
     obj = os.path.join(OBJ, os.path.basename(src) + ".o")
     if (not force and os.path.exists(obj)
             and os.path.getmtime(obj) >= max(os.path.getmtime(src), _deps())):
         return obj, ""
-    cmd = [nvcc()] + NVCC_FLAGS + ["-c", src, "-o", obj]
+    extra = ["--fmad=false"] if os.path.basename(src) in NO_CONTRACT else []
+    cmd = [nvcc()] + NVCC_FLAGS + extra + ["-c", src, "-o", obj]
     if verbose_ptxas and src.endswith(".cu"):
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)

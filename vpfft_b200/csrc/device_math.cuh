@@ -26,6 +26,26 @@
 
 namespace vpfft {
 
+// a * b + c with one rounding, spelled out: the line transforms and the Green
+// operator use it for every product-sum so that their arithmetic does not
+// depend on the compiler's choice of contractions (their translation units are
+// built with contraction off), which makes every compiled copy of a pass --
+// the single-grid tiles and each batched tile family -- give the same bits.
+__host__ __device__ __forceinline__ float fmad(float a, float b, float c) {
+#ifdef __CUDA_ARCH__
+  return __fmaf_rn(a, b, c);
+#else
+  return fmaf(a, b, c);
+#endif
+}
+__host__ __device__ __forceinline__ double fmad(double a, double b, double c) {
+#ifdef __CUDA_ARCH__
+  return __fma_rn(a, b, c);
+#else
+  return fma(a, b, c);
+#endif
+}
+
 constexpr int kNS = 12;
 
 // FCC {111}<110> slip systems in the reference's order: Burgers direction b_s
@@ -621,10 +641,11 @@ __device__ __forceinline__ void green_apply(const GreenParams<R>& gp, int ix, in
     R k1 = R(iy > gp.ny / 2 ? iy - gp.ny : iy) * gp.inv_len[1];
     R k2 = R(iz > gp.nz / 2 ? iz - gp.nz : iz) * gp.inv_len[2];
     R il;
+    const R kk = fmad(k2, k2, fmad(k1, k1, k0 * k0));
     if constexpr (sizeof(R) == 4)
-      il = rsqrtf(k0 * k0 + k1 * k1 + k2 * k2);
+      il = rsqrtf(kk);
     else
-      il = R(1) / sqrt(k0 * k0 + k1 * k1 + k2 * k2);
+      il = R(1) / sqrt(kk);
     k0 *= il;
     k1 *= il;
     k2 *= il;
@@ -650,7 +671,7 @@ __device__ __forceinline__ void green_apply(const GreenParams<R>& gp, int ix, in
         R acc = R(0);
 #pragma unroll
         for (int a = 0; a < 5; ++a)
-          if (!vz(i, a)) acc += V[i][a] * gp.L0[b * 5 + a];
+          if (!vz(i, a)) acc = fmad(V[i][a], gp.L0[b * 5 + a], acc);
         VL[i][b] = acc;
       }
     R A[3][3];
@@ -661,21 +682,23 @@ __device__ __forceinline__ void green_apply(const GreenParams<R>& gp, int ix, in
         R acc = R(0);
 #pragma unroll
         for (int b = 0; b < 5; ++b)
-          if (!vz(k, b)) acc += VL[i][b] * V[k][b];
+          if (!vz(k, b)) acc = fmad(VL[i][b], V[k][b], acc);
         A[i][k] = acc;
       }
-    // A^-1 by the adjugate
+    // A^-1 by the adjugate; x*y - z*w as fmad(x, y, -(z*w))
+    auto det2 = [](R x, R y, R z, R w) { return fmad(x, y, -(z * w)); };
     R C[3][3];
-    C[0][0] = A[1][1] * A[2][2] - A[1][2] * A[2][1];
-    C[0][1] = A[0][2] * A[2][1] - A[0][1] * A[2][2];
-    C[0][2] = A[0][1] * A[1][2] - A[0][2] * A[1][1];
-    C[1][0] = A[1][2] * A[2][0] - A[1][0] * A[2][2];
-    C[1][1] = A[0][0] * A[2][2] - A[0][2] * A[2][0];
-    C[1][2] = A[0][2] * A[1][0] - A[0][0] * A[1][2];
-    C[2][0] = A[1][0] * A[2][1] - A[1][1] * A[2][0];
-    C[2][1] = A[0][1] * A[2][0] - A[0][0] * A[2][1];
-    C[2][2] = A[0][0] * A[1][1] - A[0][1] * A[1][0];
-    const R idet = R(1) / (A[0][0] * C[0][0] + A[0][1] * C[1][0] + A[0][2] * C[2][0]);
+    C[0][0] = det2(A[1][1], A[2][2], A[1][2], A[2][1]);
+    C[0][1] = det2(A[0][2], A[2][1], A[0][1], A[2][2]);
+    C[0][2] = det2(A[0][1], A[1][2], A[0][2], A[1][1]);
+    C[1][0] = det2(A[1][2], A[2][0], A[1][0], A[2][2]);
+    C[1][1] = det2(A[0][0], A[2][2], A[0][2], A[2][0]);
+    C[1][2] = det2(A[0][2], A[1][0], A[0][0], A[1][2]);
+    C[2][0] = det2(A[1][0], A[2][1], A[1][1], A[2][0]);
+    C[2][1] = det2(A[0][1], A[2][0], A[0][0], A[2][1]);
+    C[2][2] = det2(A[0][0], A[1][1], A[0][1], A[1][0]);
+    const R idet =
+        R(1) / fmad(A[0][2], C[2][0], fmad(A[0][1], C[1][0], A[0][0] * C[0][0]));
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -684,10 +707,10 @@ __device__ __forceinline__ void green_apply(const GreenParams<R>& gp, int ix, in
     R u[3], w[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      u[i] = C[i][0] * kv[0] + C[i][1] * kv[1] + C[i][2] * kv[2];
-      w[i] = kv[0] * C[0][i] + kv[1] * C[1][i] + kv[2] * C[2][i];
+      u[i] = fmad(C[i][2], kv[2], fmad(C[i][1], kv[1], C[i][0] * kv[0]));
+      w[i] = fmad(kv[2], C[2][i], fmad(kv[1], C[1][i], kv[0] * C[0][i]));
     }
-    const R ikak = R(1) / (kv[0] * u[0] + kv[1] * u[1] + kv[2] * u[2]);
+    const R ikak = R(1) / fmad(kv[2], u[2], fmad(kv[1], u[1], kv[0] * u[0]));
     // q = V phat (3 complex), t = Bk q = A^-1 q - u (w.q)/(k.A^-1 k)
     R qr[3], qi[3];
 #pragma unroll
@@ -696,24 +719,24 @@ __device__ __forceinline__ void green_apply(const GreenParams<R>& gp, int ix, in
 #pragma unroll
       for (int b = 0; b < 5; ++b) {
         if (vz(i, b)) continue;
-        ar += V[i][b] * pre[b];
-        ai += V[i][b] * pim[b];
+        ar = fmad(V[i][b], pre[b], ar);
+        ai = fmad(V[i][b], pim[b], ai);
       }
       qr[i] = ar;
       qi[i] = ai;
     }
-    const R wqr = (w[0] * qr[0] + w[1] * qr[1] + w[2] * qr[2]) * ikak;
-    const R wqi = (w[0] * qi[0] + w[1] * qi[1] + w[2] * qi[2]) * ikak;
+    const R wqr = fmad(w[2], qr[2], fmad(w[1], qr[1], w[0] * qr[0])) * ikak;
+    const R wqi = fmad(w[2], qi[2], fmad(w[1], qi[1], w[0] * qi[0])) * ikak;
     R tr[3], ti[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      tr[i] = C[i][0] * qr[0] + C[i][1] * qr[1] + C[i][2] * qr[2] - u[i] * wqr;
-      ti[i] = C[i][0] * qi[0] + C[i][1] * qi[1] + C[i][2] * qi[2] - u[i] * wqi;
+      tr[i] = fmad(-u[i], wqr, fmad(C[i][2], qr[2], fmad(C[i][1], qr[1], C[i][0] * qr[0])));
+      ti[i] = fmad(-u[i], wqi, fmad(C[i][2], qi[2], fmad(C[i][1], qi[1], C[i][0] * qi[0])));
     }
 #pragma unroll
     for (int a = 0; a < 5; ++a) {
-      dre[a] = wg * (V[0][a] * tr[0] + V[1][a] * tr[1] + V[2][a] * tr[2]);
-      dim[a] = wg * (V[0][a] * ti[0] + V[1][a] * ti[1] + V[2][a] * ti[2]);
+      dre[a] = wg * fmad(V[2][a], tr[2], fmad(V[1][a], tr[1], V[0][a] * tr[0]));
+      dim[a] = wg * fmad(V[2][a], ti[2], fmad(V[1][a], ti[1], V[0][a] * ti[0]));
     }
   }
   if (wl != R(0)) {
@@ -722,11 +745,11 @@ __device__ __forceinline__ void green_apply(const GreenParams<R>& gp, int ix, in
       R ar = R(0), ai = R(0);
 #pragma unroll
       for (int b = 0; b < 5; ++b) {
-        ar += gp.Linv[b * 5 + a] * pre[b];
-        ai += gp.Linv[b * 5 + a] * pim[b];
+        ar = fmad(gp.Linv[b * 5 + a], pre[b], ar);
+        ai = fmad(gp.Linv[b * 5 + a], pim[b], ai);
       }
-      dre[a] -= wl * ar;
-      dim[a] -= wl * ai;
+      dre[a] = fmad(-wl, ar, dre[a]);
+      dim[a] = fmad(-wl, ai, dim[a]);
     }
   }
 #pragma unroll

@@ -75,10 +75,11 @@ VPFFT_HD T scl(T a, R s) {
   return T{a.x * s, a.y * s};
 }
 // v * w for SIGN < 0, v * conj(w) for SIGN > 0 (w from the table: exp(-i theta))
+// (products and sums spelled out with fmad, see device_math.cuh)
 template <int SIGN, typename T>
 VPFFT_HD T tw_mul(T v, T w) {
-  if (SIGN < 0) return T{v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x};
-  return T{v.x * w.x + v.y * w.y, v.y * w.x - v.x * w.y};
+  if (SIGN < 0) return T{fmad(v.x, w.x, -(v.y * w.y)), fmad(v.x, w.y, v.y * w.x)};
+  return T{fmad(v.x, w.x, v.y * w.y), fmad(v.y, w.x, -(v.x * w.y))};
 }
 // z * (SIGN i)
 template <int SIGN, typename T>
@@ -147,7 +148,7 @@ VPFFT_HD T twc(T v) {
   } else {
     constexpr F c = F(cos48(m));
     constexpr F s = F(SIGN < 0 ? -sin48(m) : sin48(m));
-    return T{v.x * c - v.y * s, v.x * s + v.y * c};
+    return T{fmad(v.x, c, -(v.y * s)), fmad(v.x, s, v.y * c)};
   }
 }
 
