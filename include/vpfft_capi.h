@@ -56,6 +56,8 @@ typedef enum {
  * its cap, Solvers.cpp:167-170, 213-221). */
 #define VPFFT_STATUS_MAX_RSS_TINY 0x1       /* a voxel's max resolved shear < 1e-10 (the call fails) */
 #define VPFFT_STATUS_NONFINITE 0x2          /* NaN/Inf appeared (the call fails) */
+#define VPFFT_STATUS_DEVICE_TIMEOUT 0x4     /* a bounded device-side wait gave up (the call
+                                               fails with VPFFT_ERR_CUDA) */
 #define VPFFT_STATUS_LOOP_NOT_CONVERGED 0x100 /* the loop stopped at max_iter with delta_sigma
                                                or delta_eps above eps */
 #define VPFFT_STATUS_NR_CAPPED 0x200        /* some voxel's Newton-Raphson solve stopped at its
@@ -296,6 +298,13 @@ vpfft_status vpfft_green_apply(int n, const int32_t *k_index, int nx, int ny, in
  * real: n_comp x N (component-major); spec: n_comp x nx x ny x (nz/2+1) x 2. */
 vpfft_status vpfft_fft3d_r2c(int nx, int ny, int nz, int n_comp, const double *real,
                              double *spec, vpfft_precision precision);
+/* Tile movement of the FP32 forward y pass: 1 moves the tiles
+ * of y lines of 64, 128 or 256 points with the Tensor Memory Accelerator
+ * (bulk tensor copies on mbarriers), 0 uses the warp-copy pass for every
+ * size (the default); -1 only queries.  Both give the same bits.  Returns the previous
+ * setting.  Process-wide; a tuning and diagnostic switch with no counterpart
+ * in the reference. */
+int vpfft_set_tma_passes(int enable);
 vpfft_status vpfft_fft3d_c2r(int nx, int ny, int nz, int n_comp, const double *spec,
                              double *real, vpfft_precision precision);
 

@@ -82,7 +82,9 @@ def test_single_grid_matches_reference(name, golden, lib):
         assert rel.max() <= 1e-9, (s, rel.max())
         np.testing.assert_allclose(hist[:, 5:10], ref[:, 5:10], rtol=1e-9,
                                    atol=1e-9 * np.abs(ref[:, 5:10]).max())
-        np.testing.assert_allclose(hist[:, 10:], ref[:, 10:], rtol=1e-6)
+        # delta_sigma and delta_eps are relative norms: at rounding level (the
+        # linear n = 1 case, where sigma = lambda to the last bits) compare absolutely
+        np.testing.assert_allclose(hist[:, 10:], ref[:, 10:], rtol=1e-6, atol=1e-12)
     check_fields(grid, g)
     grid.close()
 

@@ -48,7 +48,7 @@ def _deps() -> float:
 # product-sums are written out with fused multiply-adds (fmad), so every
 # compiled copy of a pass -- single-grid tiles and each batched tile family --
 # performs the same operations and gives the same bits.
-NO_CONTRACT = {"fft.cu", "fft_fixed_small.cu", "fft_fixed_large.cu"}
+NO_CONTRACT = {"fft.cu", "fft_fixed_small.cu", "fft_fixed_large.cu", "fft_tma.cu"}
 
 
 def _compile(src: str, force: bool, verbose_ptxas: bool) -> tuple[str, str]:

@@ -34,6 +34,7 @@ ERR_BUSY = 12
 # bits of Stats.status_bits / BatchResult.status_bits (include/vpfft_capi.h)
 STATUS_MAX_RSS_TINY = 0x1
 STATUS_NONFINITE = 0x2
+STATUS_DEVICE_TIMEOUT = 0x4
 STATUS_LOOP_NOT_CONVERGED = 0x100
 STATUS_NR_CAPPED = 0x200
 
@@ -219,6 +220,7 @@ _PROTOS = {
     "vpfft_green_apply": (C.c_int, [C.c_int, _I32, C.c_int, C.c_int, C.c_int, _D, _D, _D, _D,
                                     C.c_int]),
     "vpfft_fft3d_r2c": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _D, _D, C.c_int]),
+    "vpfft_set_tma_passes": (C.c_int, [C.c_int]),
     "vpfft_fft3d_c2r": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _D, _D, C.c_int]),
     "vpfft_fixture_polycrystal": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, _D,
                                             _I32]),

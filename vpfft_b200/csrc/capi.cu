@@ -32,7 +32,8 @@ struct PhaseRange {
 };
 
 static_assert(VPFFT_STATUS_MAX_RSS_TINY == vpfft::kStatusMaxRssTiny &&
-                  VPFFT_STATUS_NONFINITE == vpfft::kStatusNonFinite,
+                  VPFFT_STATUS_NONFINITE == vpfft::kStatusNonFinite &&
+                  VPFFT_STATUS_DEVICE_TIMEOUT == vpfft::kStatusDeviceTimeout,
               "device status bits and the C ABI's bits agree");
 
 namespace {
@@ -502,6 +503,8 @@ vpfft_status do_fixed_point(vpfft_grid* g, const double edot[5], int max_iter, d
                       (c.nr_capped ? VPFFT_STATUS_NR_CAPPED : 0);
     std::memcpy(st->L0, g->L0, sizeof(g->L0));
   }
+  if (c.status & kStatusDeviceTimeout)
+    return fail(g, VPFFT_ERR_CUDA, "a bounded device-side wait timed out in a transform pass");
   if (c.status & kStatusNonFinite) return fail(g, VPFFT_ERR_NONFINITE, "non-finite stress or strain rate");
   if (c.status & kStatusMaxRssTiny)
     return fail(g, VPFFT_ERR_MAX_RSS_TINY, "max resolved shear stress < 1e-10 during the iteration");
@@ -1308,6 +1311,8 @@ vpfft_status vpfft_fft3d_r2c(int nx, int ny, int nz, int ncomp, const double* re
   return prec == VPFFT_PREC_FP64 ? fft_impl<double>(nx, ny, nz, ncomp, real, spec, 0)
                                  : fft_impl<float>(nx, ny, nz, ncomp, real, spec, 0);
 }
+int vpfft_set_tma_passes(int enable) { return vpfft::set_tma_passes(enable); }
+
 vpfft_status vpfft_fft3d_c2r(int nx, int ny, int nz, int ncomp, const double* spec, double* real,
                              vpfft_precision prec) {
   if (!valid_dim(nx) || !valid_dim(ny) || !valid_dim(nz) || ncomp < 1 || ncomp > 5 || !real || !spec)

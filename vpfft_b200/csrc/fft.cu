@@ -41,6 +41,12 @@ const PassSet<S>& pass_set(const LinePlan& p) {
 
 int cdiv(int a, int b) { return (a + b - 1) / b; }
 
+// The TMA forward y pass where it applies (FP32; see fft_tma.cu).
+bool y_fwd_tma(const Spectral<float>& sp, const IterCtrl* ctrl, cudaStream_t st, int ncomp) {
+  return launch_y_fwd_tma(sp, ctrl, st, ncomp);
+}
+bool y_fwd_tma(const Spectral<double>&, const IterCtrl*, cudaStream_t, int) { return false; }
+
 template <typename S>
 struct PassSmem {
   size_t z_r2c, z_c2r, y, x;
@@ -84,7 +90,8 @@ int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S
   Z.z_r2c<<<gz, Z.threads, sm.z_r2c, st>>>(work, A, sp.pz, sp.py.by_n, twz, sp.nx, sp.ny, sp.nh,
                                            ctrl);
   if (ev) cudaEventRecord(ev[1], st);
-  Y.y_fwd<<<gy, Y.threads, sm.y, st>>>(A, B, sp.py, sp.px.by_n, twy, sp.nx, sp.nh, ctrl);
+  if (!y_fwd_tma(sp, ctrl, st, ncomp))
+    Y.y_fwd<<<gy, Y.threads, sm.y, st>>>(A, B, sp.py, sp.px.by_n, twy, sp.nx, sp.nh, ctrl);
   if (ev) cudaEventRecord(ev[2], st);
   X.x_green<<<gx, X.threads_x, sm.x, st>>>(B, sp.px, sp.py.by_n, twx, gp, sp.ny, sp.nh, ncomp,
                                          ctrl);
@@ -116,7 +123,8 @@ int launch_fft3d(const Spectral<S>& sp, S* real, int ncomp, int mode, cudaStream
   if (mode == 0) {
     Z.z_r2c<<<gz, Z.threads, sm.z_r2c, st>>>(real, A, sp.pz, sp.py.by_n, twz, sp.nx, sp.ny, sp.nh,
                                              nullptr);
-    Y.y_fwd<<<gy, Y.threads, sm.y, st>>>(A, B, sp.py, sp.px.by_n, twy, sp.nx, sp.nh, nullptr);
+    if (!y_fwd_tma(sp, nullptr, st, ncomp))
+      Y.y_fwd<<<gy, Y.threads, sm.y, st>>>(A, B, sp.py, sp.px.by_n, twy, sp.nx, sp.nh, nullptr);
     X.x_fwd<<<gx, X.threads_x, sm.x, st>>>(B, sp.px, sp.py.by_n, twx, gp, sp.ny, sp.nh, ncomp,
                                          nullptr);
   } else {

@@ -51,9 +51,10 @@ struct IterCtrl {
   unsigned long long nr_capped;
   double last[12];    // <sigma>(5), <edot>(5), delta_sigma, delta_eps of the last iteration
 };
-// device-side bits of IterCtrl::status; the same values as VPFFT_STATUS_MAX_RSS_TINY
-// and VPFFT_STATUS_NONFINITE of the C ABI (static_assert in capi.cu)
-enum : int32_t { kStatusMaxRssTiny = 1, kStatusNonFinite = 2 };
+// device-side bits of IterCtrl::status; the same values as VPFFT_STATUS_MAX_RSS_TINY,
+// VPFFT_STATUS_NONFINITE and VPFFT_STATUS_DEVICE_TIMEOUT of the C ABI
+// (static_assert in capi.cu)
+enum : int32_t { kStatusMaxRssTiny = 1, kStatusNonFinite = 2, kStatusDeviceTimeout = 4 };
 
 // Division of 32-bit unsigned t < 2^31 by a fixed d >= 1 without a divide:
 // q = (umulhi(t, mul) + t) >> shift, with shift = ceil(log2 d) and
@@ -148,6 +149,13 @@ template <typename S>
 int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S* work,
                               const IterCtrl* ctrl, cudaStream_t st, int ncomp,
                               cudaEvent_t* ev = nullptr);
+// The forward y pass with TMA-moved tiles (fft_tma.cu) for FP32 spectra whose
+// y lines have 64, 128 or 256 points; false (nothing launched) when it does
+// not apply.  set_tma_passes(1/0) enables / disables it process-wide (-1
+// queries) and returns the previous setting.
+bool launch_y_fwd_tma(const Spectral<float>& sp, const IterCtrl* ctrl, cudaStream_t st,
+                      int ncomp);
+int set_tma_passes(int enable);
 // forward-only / inverse-only transforms for testing (mode 0 = forward, 1 = inverse)
 template <typename S>
 int launch_fft3d(const Spectral<S>& sp, S* real, int ncomp, int mode, cudaStream_t st);
