@@ -405,9 +405,15 @@ def serving_arm(n_requests: int) -> dict:
 
 
 # ------------------------------------------------------------------ CPU side
-def ref_binary():
+def ref_binary(timing: bool = False):
+    """The reference build (oracle/_ref): for timed runs its speed build
+    (vpfft_ref_native, release flags + -march=x86-64-v4) when present, else the
+    parity build; the C restatement when neither exists."""
     from oracle import refio
 
+    native = os.path.join(os.path.dirname(refio.REF_BIN), "vpfft_ref_native")
+    if timing and os.path.exists(native):
+        return native, "reference"
     if os.path.exists(refio.REF_BIN):
         return refio.REF_BIN, "reference"
     from oracle import portlib
@@ -446,7 +452,7 @@ def reference_solve(n_side, grains, seed, warm, timed, ranks):
     FFT) and the share of that time inside the FFT stand-in."""
     from oracle import portlib, refio
 
-    binary, kind = ref_binary()
+    binary, kind = ref_binary(timing=True)
     edot = refio.edot_from_matrix(VEL_GRAD)
     m = refio.Material.uniform(1.0, RATE_SENS, 1.0, 0.5, 20.0, 1.0)
     tmp = tempfile.mkdtemp(prefix="vpfft_ref_")
@@ -464,7 +470,15 @@ def reference_solve(n_side, grains, seed, warm, timed, ranks):
                               max_iter=warm + timed, dt=0.005, eps=0.0)
             extra = []
         t0 = time.time()
-        out = refio.run(binary, case, tmp, extra_args=extra)
+        try:
+            out = refio.run(binary, case, tmp, extra_args=extra)
+        except RuntimeError:
+            if not binary.endswith("_native"):
+                raise
+            # the speed build does not run on this host's CPU: the parity build
+            binary = refio.REF_BIN
+            t0 = time.time()
+            out = refio.run(binary, case, tmp, extra_args=extra)
         wall = time.time() - t0
     finally:
         import shutil
@@ -481,8 +495,11 @@ def reference_solve(n_side, grains, seed, warm, timed, ranks):
 
 
 def reference_sample_text(r, n_side, grains, warm, timed) -> str:
+    flags = ("release flags -O3 -DNDEBUG plus -march=x86-64-v4" if r["binary"].endswith("_native")
+             else "release flags -O3 -DNDEBUG")
     return (f"the reference's own code ({os.path.relpath(r['binary'], ROOT)}: Src/*.cpp "
-            f"compiled unmodified against the project's MPI/FFTW/Eigen stand-ins) on the full "
+            f"compiled unmodified, {flags}, against the project's MPI/FFTW/Eigen stand-ins) "
+            f"on the full "
             f"{n_side}^3 workload ({grains} grains, same seed, material and strain rate), run as "
             f"{r['ranks']} MPI ranks (FFTW-MPI slab decomposition, one single-threaded process "
             f"per core); {warm} warm-up + {timed} timed fixed-point iterations of one increment; "

@@ -41,11 +41,29 @@ const PassSet<S>& pass_set(const LinePlan& p) {
 
 int cdiv(int a, int b) { return (a + b - 1) / b; }
 
-// The TMA forward y pass where it applies (FP32; see fft_tma.cu).
+// The TMA y passes where they apply (FP32; see fft_tma.cu).
 bool y_fwd_tma(const Spectral<float>& sp, const IterCtrl* ctrl, cudaStream_t st, int ncomp) {
   return launch_y_fwd_tma(sp, ctrl, st, ncomp);
 }
 bool y_fwd_tma(const Spectral<double>&, const IterCtrl*, cudaStream_t, int) { return false; }
+bool y_inv_tma(const Spectral<float>& sp, const IterCtrl* ctrl, cudaStream_t st, int ncomp) {
+  return launch_y_inv_tma(sp, ctrl, st, ncomp);
+}
+bool y_inv_tma(const Spectral<double>&, const IterCtrl*, cudaStream_t, int) { return false; }
+bool z_r2c_tma(const Spectral<float>& sp, const float* w, const IterCtrl* ctrl, cudaStream_t st,
+               int ncomp) {
+  return launch_z_r2c_tma(sp, w, ctrl, st, ncomp);
+}
+bool z_r2c_tma(const Spectral<double>&, const double*, const IterCtrl*, cudaStream_t, int) {
+  return false;
+}
+bool z_c2r_tma(const Spectral<float>& sp, float* w, const IterCtrl* ctrl, cudaStream_t st,
+               int ncomp) {
+  return launch_z_c2r_tma(sp, w, ctrl, st, ncomp);
+}
+bool z_c2r_tma(const Spectral<double>&, double*, const IterCtrl*, cudaStream_t, int) {
+  return false;
+}
 
 template <typename S>
 struct PassSmem {
@@ -87,8 +105,9 @@ int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S
   const dim3 gx(cdiv(sp.nh * sp.ny, X.tk));
   const S scale = S(1.0 / ((double)sp.nx * sp.ny * sp.nz));
   if (ev) cudaEventRecord(ev[0], st);
-  Z.z_r2c<<<gz, Z.threads, sm.z_r2c, st>>>(work, A, sp.pz, sp.py.by_n, twz, sp.nx, sp.ny, sp.nh,
-                                           ctrl);
+  if (!z_r2c_tma(sp, work, ctrl, st, ncomp))
+    Z.z_r2c<<<gz, Z.threads, sm.z_r2c, st>>>(work, A, sp.pz, sp.py.by_n, twz, sp.nx, sp.ny, sp.nh,
+                                             ctrl);
   if (ev) cudaEventRecord(ev[1], st);
   if (!y_fwd_tma(sp, ctrl, st, ncomp))
     Y.y_fwd<<<gy, Y.threads, sm.y, st>>>(A, B, sp.py, sp.px.by_n, twy, sp.nx, sp.nh, ctrl);
@@ -96,10 +115,12 @@ int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S
   X.x_green<<<gx, X.threads_x, sm.x, st>>>(B, sp.px, sp.py.by_n, twx, gp, sp.ny, sp.nh, ncomp,
                                          ctrl);
   if (ev) cudaEventRecord(ev[3], st);
-  Y.y_inv<<<gy, Y.threads, sm.y, st>>>(B, A, sp.py, sp.px.by_n, twy, sp.nx, sp.nh, ctrl);
+  if (!y_inv_tma(sp, ctrl, st, ncomp))
+    Y.y_inv<<<gy, Y.threads, sm.y, st>>>(B, A, sp.py, sp.px.by_n, twy, sp.nx, sp.nh, ctrl);
   if (ev) cudaEventRecord(ev[4], st);
-  Z.z_c2r<<<gz, Z.threads, sm.z_c2r, st>>>(A, work, sp.pz, sp.py.by_n, twz, sp.nx, sp.ny, sp.nh,
-                                           scale, ctrl);
+  if (!z_c2r_tma(sp, work, ctrl, st, ncomp))
+    Z.z_c2r<<<gz, Z.threads, sm.z_c2r, st>>>(A, work, sp.pz, sp.py.by_n, twz, sp.nx, sp.ny, sp.nh,
+                                             scale, ctrl);
   if (ev) cudaEventRecord(ev[5], st);
   return 5;
 }
@@ -121,8 +142,9 @@ int launch_fft3d(const Spectral<S>& sp, S* real, int ncomp, int mode, cudaStream
   const dim3 gx(cdiv(sp.nh * sp.ny, X.tk));
   GreenParams<S> gp{};
   if (mode == 0) {
-    Z.z_r2c<<<gz, Z.threads, sm.z_r2c, st>>>(real, A, sp.pz, sp.py.by_n, twz, sp.nx, sp.ny, sp.nh,
-                                             nullptr);
+    if (!z_r2c_tma(sp, real, nullptr, st, ncomp))
+      Z.z_r2c<<<gz, Z.threads, sm.z_r2c, st>>>(real, A, sp.pz, sp.py.by_n, twz, sp.nx, sp.ny,
+                                               sp.nh, nullptr);
     if (!y_fwd_tma(sp, nullptr, st, ncomp))
       Y.y_fwd<<<gy, Y.threads, sm.y, st>>>(A, B, sp.py, sp.px.by_n, twy, sp.nx, sp.nh, nullptr);
     X.x_fwd<<<gx, X.threads_x, sm.x, st>>>(B, sp.px, sp.py.by_n, twx, gp, sp.ny, sp.nh, ncomp,
@@ -130,10 +152,12 @@ int launch_fft3d(const Spectral<S>& sp, S* real, int ncomp, int mode, cudaStream
   } else {
     X.x_inv<<<gx, X.threads_x, sm.x, st>>>(B, sp.px, sp.py.by_n, twx, gp, sp.ny, sp.nh, ncomp,
                                          nullptr);
-    Y.y_inv<<<gy, Y.threads, sm.y, st>>>(B, A, sp.py, sp.px.by_n, twy, sp.nx, sp.nh, nullptr);
+    if (!y_inv_tma(sp, nullptr, st, ncomp))
+      Y.y_inv<<<gy, Y.threads, sm.y, st>>>(B, A, sp.py, sp.px.by_n, twy, sp.nx, sp.nh, nullptr);
     const S scale = S(1.0 / ((double)sp.nx * sp.ny * sp.nz));
-    Z.z_c2r<<<gz, Z.threads, sm.z_c2r, st>>>(A, real, sp.pz, sp.py.by_n, twz, sp.nx, sp.ny, sp.nh,
-                                             scale, nullptr);
+    if (!z_c2r_tma(sp, real, nullptr, st, ncomp))
+      Z.z_c2r<<<gz, Z.threads, sm.z_c2r, st>>>(A, real, sp.pz, sp.py.by_n, twz, sp.nx, sp.ny,
+                                               sp.nh, scale, nullptr);
   }
   return 3;
 }

@@ -333,9 +333,7 @@ template <> struct FixedPlan<512> { using type = Radices<16, 16, 2>; };
 // The same stage with every size a compile-time constant.  tws: the stage's
 // own twiddles, tws[(r - 1) NS + j mod NS] = W_N^(r (j mod NS) N / (NS RADIX)),
 // so that the threads of a warp (consecutive j) read consecutive entries.
-// kDenseIn: the input lines are dense (element i of a line at i, lines N
-// apart, as a TMA tile lands in shared memory) instead of padded.
-template <int N, int RADIX, int NS, int SIGN, bool kDenseIn = false, typename T>
+template <int N, int RADIX, int NS, int SIGN, typename T>
 VPFFT_HD void fixed_stage(const T* a, T* b, const T* tws, int nlines, int ls, int tid, int nthr) {
   constexpr int NB = N / RADIX;
   static_assert(N % (NS * RADIX) == 0, "plan does not divide N");
@@ -345,12 +343,12 @@ VPFFT_HD void fixed_stage(const T* a, T* b, const T* tws, int nlines, int ls, in
     const int j = t - line * NB;
     const int jm = j % NS;
     const int od = (j - jm) * RADIX + jm;
-    const T* in = a + line * (kDenseIn ? N : ls);
+    const T* in = a + line * ls;
     T* out = b + line * ls;
     T v[RADIX];
     static_for<0, RADIX>([&](auto rc) {
       constexpr int r = decltype(rc)::value;
-      v[r] = in[kDenseIn ? j + r * NB : sw(j + r * NB)];
+      v[r] = in[sw(j + r * NB)];
     });
     if constexpr (NS > 1) {
       static_for<1, RADIX>([&](auto rc) {
@@ -418,19 +416,42 @@ struct FixedEngine {
     return fixed_stages<N, SIGN, 1, 0>(a, b, tw, nlines, ls, tid, nthr,
                                        typename FixedPlan<N>::type{});
   }
-  // The same transform of dense input lines `in` (left unchanged): the first
-  // stage reads them and writes padded lines to a, the rest ping-pong a / b.
-  template <int SIGN, typename T>
-  VPFFT_HD static T* fft_dense_in(const T* in, T* a, T* b, const T* tw, int nlines, int ls,
-                                  int tid, int nthr) {
-    return first_dense<SIGN>(in, a, b, tw, nlines, ls, tid, nthr, typename FixedPlan<N>::type{});
+  // The same transform of lines staged in any layout: the first stage reads
+  // element i of line l as load(l, i) and writes padded lines to a, the rest
+  // ping-pong a / b.  kLineFastest: consecutive threads take consecutive
+  // lines of one butterfly index (for layouts where the lines are adjacent in
+  // memory, e.g. the columns of a tile), else consecutive butterflies of one
+  // line.  The arithmetic is the first stage's, so the result is the same bit
+  // for bit as fft() on the same values.
+  template <int SIGN, bool kLineFastest, typename T, class Load>
+  VPFFT_HD static T* fft_loaded(Load load, T* a, T* b, const T* tw, int nlines, int ls, int tid,
+                                int nthr) {
+    return first_loaded<SIGN, kLineFastest>(load, a, b, tw, nlines, ls, tid, nthr,
+                                            typename FixedPlan<N>::type{});
   }
 
  private:
-  template <int SIGN, typename T, int R, int... Rest>
-  VPFFT_HD static T* first_dense(const T* in, T* a, T* b, const T* tw, int nlines, int ls,
-                                 int tid, int nthr, Radices<R, Rest...>) {
-    fixed_stage<N, R, 1, SIGN, true>(in, a, tw, nlines, ls, tid, nthr);
+  template <int SIGN, bool kLineFastest, typename T, class Load, int R, int... Rest>
+  VPFFT_HD static T* first_loaded(Load load, T* a, T* b, const T* tw, int nlines, int ls,
+                                  int tid, int nthr, Radices<R, Rest...>) {
+    // first stage: span 1, no twiddles; butterfly j of line l reads elements
+    // j + r N/R and writes j R + r
+    constexpr int NB = N / R;
+    for (int t = tid; t < NB * nlines; t += nthr) {
+      const int line = kLineFastest ? t % nlines : t / NB;
+      const int j = kLineFastest ? t / nlines : t - line * NB;
+      T v[R];
+      static_for<0, R>([&](auto rc) {
+        constexpr int r = decltype(rc)::value;
+        v[r] = load(line, j + r * NB);
+      });
+      dft<R, SIGN>(v);
+      T* out = a + line * ls;
+      static_for<0, R>([&](auto rc) {
+        constexpr int r = decltype(rc)::value;
+        out[sw(j * R + r)] = v[r];
+      });
+    }
     block_sync();
     return fixed_stages<N, SIGN, R, stage_tw_size<1, R>()>(a, b, tw, nlines, ls, tid, nthr,
                                                            Radices<Rest...>{});

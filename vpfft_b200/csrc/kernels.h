@@ -149,12 +149,18 @@ template <typename S>
 int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S* work,
                               const IterCtrl* ctrl, cudaStream_t st, int ncomp,
                               cudaEvent_t* ev = nullptr);
-// The forward y pass with TMA-moved tiles (fft_tma.cu) for FP32 spectra whose
-// y lines have 64, 128 or 256 points; false (nothing launched) when it does
-// not apply.  set_tma_passes(1/0) enables / disables it process-wide (-1
+// The y and z passes with TMA-moved tiles (fft_tma.cu) for FP32 spectra whose
+// lines on the pass's axis have 64, 128 or 256 points; false (nothing
+// launched) when they do not apply.  set_tma_passes(1/0) enables / disables it process-wide (-1
 // queries) and returns the previous setting.
 bool launch_y_fwd_tma(const Spectral<float>& sp, const IterCtrl* ctrl, cudaStream_t st,
                       int ncomp);
+bool launch_y_inv_tma(const Spectral<float>& sp, const IterCtrl* ctrl, cudaStream_t st,
+                      int ncomp);
+bool launch_z_r2c_tma(const Spectral<float>& sp, const float* work, const IterCtrl* ctrl,
+                      cudaStream_t st, int ncomp);
+bool launch_z_c2r_tma(const Spectral<float>& sp, float* work, const IterCtrl* ctrl,
+                      cudaStream_t st, int ncomp);
 int set_tma_passes(int enable);
 // forward-only / inverse-only transforms for testing (mode 0 = forward, 1 = inverse)
 template <typename S>

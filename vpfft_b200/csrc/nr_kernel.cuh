@@ -243,54 +243,6 @@ __device__ __forceinline__ bool ldlt5_solve(const T A[15], const T b[5], T x[5])
   return ok;
 }
 
-// The same LDL^T split in two: the factors of A (L strictly lower, packed
-// row by row: L10, L20, L21, L30, ...; id = 1 / pivots), then solves with
-// them.  Returns false when a pivot is not positive.
-template <typename T>
-__device__ __forceinline__ bool ldlt5_factor(const T A[15], T L[10], T id[5]) {
-  T Lf[5][5], d[5];
-  bool ok = true;
-#pragma unroll
-  for (int j = 0; j < 5; ++j) {
-    T dj = A[sym5(j, j)];
-#pragma unroll
-    for (int k = 0; k < j; ++k) dj -= Lf[j][k] * Lf[j][k] * d[k];
-    ok = ok && (dj > T(0));
-    d[j] = dj;
-    id[j] = recip(dj);
-#pragma unroll
-    for (int i = j + 1; i < 5; ++i) {
-      T a = A[sym5(j, i)];
-#pragma unroll
-      for (int k = 0; k < j; ++k) a -= Lf[i][k] * Lf[j][k] * d[k];
-      Lf[i][j] = a * id[j];
-    }
-  }
-#pragma unroll
-  for (int i = 1; i < 5; ++i)
-#pragma unroll
-    for (int k = 0; k < i; ++k) L[(i * (i - 1)) / 2 + k] = Lf[i][k];
-  return ok;
-}
-template <typename T>
-__device__ __forceinline__ void ldlt5_apply(const T L[10], const T id[5], const T b[5], T x[5]) {
-  T z[5];
-#pragma unroll
-  for (int i = 0; i < 5; ++i) {
-    T a = b[i];
-#pragma unroll
-    for (int k = 0; k < i; ++k) a -= L[(i * (i - 1)) / 2 + k] * z[k];
-    z[i] = a;
-  }
-#pragma unroll
-  for (int i = 4; i >= 0; --i) {
-    T a = z[i] * id[i];
-#pragma unroll
-    for (int k = i + 1; k < 5; ++k) a -= L[(k * (k - 1)) / 2 + i] * x[k];
-    x[i] = a;
-  }
-}
-
 // 1/CRSS of system q: per voxel from shared memory (stride bs) or uniform
 // from the launch parameters.
 template <bool kTauSmem, typename MS>
@@ -305,9 +257,7 @@ __device__ __forceinline__ double itau_of(const MS* tsm, int bs, const NRParams&
 // in arithmetic type T (double, or float for the predictor of the mixed path).
 // snap: set |r| < 1e-10 to 0 (the unconstrained solver does, Solvers.cpp:50-51).
 // rmax (kRmax): max_s |r_s| at s.
-// kJac = false: S only (K is not touched).
-template <int NEXP, bool kSnap, bool kTauSmem, typename T, typename MS, bool kRmax = false,
-          bool kJac = true>
+template <int NEXP, bool kSnap, bool kTauSmem, typename T, typename MS, bool kRmax = false>
 __device__ __forceinline__ bool accumulate(const MS* msm, const MS* tsm, int bs,
                                            const NRParams& p, const T s[5], T S[5], T K[15],
                                            T* rmax = nullptr) {
@@ -316,10 +266,8 @@ __device__ __forceinline__ bool accumulate(const MS* msm, const MS* tsm, int bs,
   T rm = T(0);
 #pragma unroll
   for (int c = 0; c < 5; ++c) S[c] = T(0);
-  if constexpr (kJac) {
 #pragma unroll
-    for (int k = 0; k < 15; ++k) K[k] = T(0);
-  }
+  for (int k = 0; k < 15; ++k) K[k] = T(0);
 #pragma unroll 2
   for (int q = 0; q < kNS; ++q) {
     T m[5];
@@ -339,18 +287,13 @@ __device__ __forceinline__ bool accumulate(const MS* msm, const MS* tsm, int bs,
     const bool power = kSnap ? (n - 1 > 0) : (n != 1);
     const T g = power ? C::gdot(p, q) * pow_nm1<NEXP>(fabs(r), n) : C::gdot(p, q);
     const T gr = g * r;
-    if constexpr (kJac) {
-      const T w = C::n(p, q) * g * it;
+    const T w = C::n(p, q) * g * it;
 #pragma unroll
-      for (int i = 0; i < 5; ++i) {
-        S[i] += m[i] * gr;
-        const T mw = m[i] * w;
+    for (int i = 0; i < 5; ++i) {
+      S[i] += m[i] * gr;
+      const T mw = m[i] * w;
 #pragma unroll
-        for (int j = i; j < 5; ++j) K[sym5(i, j)] += mw * m[j];
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < 5; ++i) S[i] += m[i] * gr;
+      for (int j = i; j < 5; ++j) K[sym5(i, j)] += mw * m[j];
     }
   }
   if constexpr (kRmax) *rmax = rm;
@@ -380,9 +323,7 @@ __device__ __forceinline__ float2 cpow2(float2 x) {
 // kFull: the pass over the 6 pairs fully unrolled (the single-grid kernel,
 // which has the registers for it: measured 3 % faster) or by 2 (the batched
 // kernel at 4 blocks per SM, where the full unroll spills).
-// kJac = false: S only (K is not touched), for chord steps that reuse an
-// earlier factorisation.
-template <int NEXP, bool kTauSmem, bool kFull = true, bool kJac = true>
+template <int NEXP, bool kTauSmem, bool kFull = true>
 __device__ __forceinline__ bool accumulate_pairs(const float* msm, const float* tsm, int bs,
                                                  const NRParams& p, const float s[5], float S[5],
                                                  float K[15], float* rmax) {
@@ -420,18 +361,13 @@ __device__ __forceinline__ bool accumulate_pairs(const float* msm, const float* 
     const float2 pw = cpow2<NEXP - 1>(make_float2(ax, ay));
     const float2 g = __fmul2_rn(make_float2(p.gdot_f[2 * pq], p.gdot_f[2 * pq + 1]), pw);
     const float2 gr = __fmul2_rn(g, r);
-    if constexpr (kJac) {
-      const float2 w = __fmul2_rn(__fmul2_rn(nn, g), it);
+    const float2 w = __fmul2_rn(__fmul2_rn(nn, g), it);
 #pragma unroll
-      for (int i = 0; i < 5; ++i) {
-        S2[i] = __ffma2_rn(m[i], gr, S2[i]);
-        const float2 mw = __fmul2_rn(m[i], w);
+    for (int i = 0; i < 5; ++i) {
+      S2[i] = __ffma2_rn(m[i], gr, S2[i]);
+      const float2 mw = __fmul2_rn(m[i], w);
 #pragma unroll
-        for (int j = i; j < 5; ++j) K2[sym5(i, j)] = __ffma2_rn(mw, m[j], K2[sym5(i, j)]);
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < 5; ++i) S2[i] = __ffma2_rn(m[i], gr, S2[i]);
+      for (int j = i; j < 5; ++j) K2[sym5(i, j)] = __ffma2_rn(mw, m[j], K2[sym5(i, j)]);
     }
   };
   if constexpr (kFull) {
@@ -443,10 +379,8 @@ __device__ __forceinline__ bool accumulate_pairs(const float* msm, const float* 
   }
 #pragma unroll
   for (int c = 0; c < 5; ++c) S[c] = S2[c].x + S2[c].y;
-  if constexpr (kJac) {
 #pragma unroll
-    for (int k = 0; k < 15; ++k) K[k] = K2[k].x + K2[k].y;
-  }
+  for (int k = 0; k < 15; ++k) K[k] = K2[k].x + K2[k].y;
   *rmax = rm;
   return adm;
 }
@@ -456,21 +390,11 @@ __device__ __forceinline__ bool accumulate_pairs(const float* msm, const float* 
 // true and the iterate in s_io when it converged with finite values; the
 // caller then takes the accepted step with FP64 residual and Jacobian.
 // *rmax0 gets max_s |r_s| at the starting point.
-// fac (optional): the LDL^T factors of the last step's matrix (L 0..9, then
-// the inverse pivots 10..14), for the FP64 residual check that follows.
-// kTol: the stopping tolerance on |delta| / |avg| (0: the reference's eps).
-template <int NEXP, bool kTauSmem, bool kFull = true, typename MS, class C>
-__device__ __forceinline__ bool nr_predict_fp32_f(const MS* msm, const MS* tsm, int bs,
-                                                  const NRParams& p, const C& cs,
-                                                  const float l32[5], const float e32[5],
-                                                  float cur[5], int max_steps, float* rmax0,
-                                                  float* fac = nullptr, float tol = 0.f);
 template <int NEXP, bool kTauSmem, bool kFull = true, typename MS, class C>
 __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, int bs,
                                                 const NRParams& p, const C& cs,
                                                 const double lam[5], const double ed[5],
-                                                double s_io[5], int max_steps, float* rmax0,
-                                                float* fac = nullptr, float tol = 0.f) {
+                                                double s_io[5], int max_steps, float* rmax0) {
   float cur[5], l32[5], e32[5];
 #pragma unroll
   for (int c = 0; c < 5; ++c) {
@@ -478,23 +402,6 @@ __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, in
     l32[c] = (float)lam[c];
     e32[c] = (float)ed[c];
   }
-  const bool ok = nr_predict_fp32_f<NEXP, kTauSmem, kFull>(msm, tsm, bs, p, cs, l32, e32, cur,
-                                                           max_steps, rmax0, fac, tol);
-  if (ok) {
-#pragma unroll
-    for (int c = 0; c < 5; ++c) s_io[c] = (double)cur[c];
-  }
-  return ok;
-}
-// The predictor on FP32 inputs; cur: the start on entry, the converged
-// iterate on a true return.
-template <int NEXP, bool kTauSmem, bool kFull, typename MS, class C>
-__device__ __forceinline__ bool nr_predict_fp32_f(const MS* msm, const MS* tsm, int bs,
-                                                  const NRParams& p, const C& cs,
-                                                  const float l32[5], const float e32[5],
-                                                  float cur[5], int max_steps, float* rmax0,
-                                                  float* fac, float tol) {
-  const float eps = tol > 0.f ? tol : p.eps_f;
   *rmax0 = 0.f;
   for (int it = 0; it < max_steps; ++it) {
     float S[5], K[15], rm;
@@ -516,12 +423,7 @@ __device__ __forceinline__ bool nr_predict_fp32_f(const MS* msm, const MS* tsm, 
 #pragma unroll
     for (int k = 0; k < 15; ++k) K[k] += cs.L0inv_f(k);
     float delta[5];
-    if (fac) {
-      if (!ldlt5_factor(K, fac, fac + 10)) return false;
-      ldlt5_apply(fac, fac + 10, y, delta);
-    } else if (!ldlt5_solve(K, y, delta)) {
-      return false;
-    }
+    if (!ldlt5_solve(K, y, delta)) return false;
     float dn = 0.f, an = 0.f;
 #pragma unroll
     for (int c = 0; c < 5; ++c) {
@@ -532,108 +434,15 @@ __device__ __forceinline__ bool nr_predict_fp32_f(const MS* msm, const MS* tsm, 
       cur[c] = nw;
     }
     bool bad;
-    const bool small = small_step_f32(dn, an, eps, &bad);
+    const bool small = small_step_f32(dn, an, p.eps_f, &bad);
     if (bad) return false;
-    if (small) return true;
+    if (small) {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) s_io[c] = (double)cur[c];
+      return true;
+    }
   }
   return false;
-}
-
-// Chord variant of the predictor (paired FP32, compile-time exponent): the
-// first step is a full Newton step whose LDL^T factors (fac) are kept; the
-// following steps reuse them and evaluate only the strain-rate sum S.  Same
-// stopping rule; returns true with the iterate in cur when it converged.
-template <int NEXP, bool kTauSmem, bool kFull, class C>
-__device__ __forceinline__ bool nr_predict_chord_f(const float* msm, const float* tsm, int bs,
-                                                   const NRParams& p, const C& cs,
-                                                   const float l32[5], const float e32[5],
-                                                   float cur[5], int max_steps, float* rmax0,
-                                                   float fac[15]) {
-  const float eps = p.eps_f;
-  auto residual = [&](const float S[5], float y[5]) {
-#pragma unroll
-    for (int i = 0; i < 5; ++i) {
-      float a = S[i] - e32[i];
-#pragma unroll
-      for (int j = 0; j < 5; ++j) a += cs.L0inv_f(sym5(i, j)) * (cur[j] - l32[j]);
-      y[i] = -a;
-    }
-  };
-  auto advance = [&](const float delta[5], bool* bad) {
-    float dn = 0.f, an = 0.f;
-#pragma unroll
-    for (int c = 0; c < 5; ++c) {
-      const float nw = cur[c] + delta[c];
-      const float av = (nw + cur[c]) * 0.5f;
-      dn += delta[c] * delta[c];
-      an += av * av;
-      cur[c] = nw;
-    }
-    return small_step_f32(dn, an, eps, bad);
-  };
-  {
-    float S[5], K[15], y[5], delta[5];
-    if (!accumulate_pairs<NEXP, kTauSmem, kFull>(msm, tsm, bs, p, cur, S, K, rmax0)) return false;
-    residual(S, y);
-#pragma unroll
-    for (int k = 0; k < 15; ++k) K[k] += cs.L0inv_f(k);
-    if (!ldlt5_factor(K, fac, fac + 10)) return false;
-    ldlt5_apply(fac, fac + 10, y, delta);
-    bool bad;
-    const bool small = advance(delta, &bad);
-    if (bad) return false;
-    if (small) return true;
-  }
-  for (int it = 1; it < max_steps; ++it) {
-    float S[5], y[5], delta[5], rm;
-    if (!accumulate_pairs<NEXP, kTauSmem, kFull, false>(msm, tsm, bs, p, cur, S, nullptr, &rm))
-      return false;
-    residual(S, y);
-    ldlt5_apply(fac, fac + 10, y, delta);
-    bool bad;
-    const bool small = advance(delta, &bad);
-    if (bad) return false;
-    if (small) return true;
-  }
-  return false;
-}
-
-// The FP64 check of a predicted stress s: the constrained residual
-//   y = L0^-1 (s - lambda) + S(s) - (Edot + d~)
-// with FP64 power law and sums (no Jacobian), and the Newton step it calls
-// for, estimated with the predictor's last LDL^T factors.  Returns true when
-// s is admissible and that step is below tol |s| (tol2 = tol^2); then e gets
-// the strain rate S(s) (ApplyConstitutiveEquations at s, in FP64).
-template <int NEXP, bool kTauSmem, typename MS, class C>
-__device__ __forceinline__ bool fp64_residual_certifies(const MS* msm, const MS* tsm, int bs,
-                                                        const NRParams& p, const C& cs,
-                                                        const double lam[5],
-                                                        const double ed[5], const double s[5],
-                                                        const float fac[15], double tol2,
-                                                        double e[5]) {
-  double S[5];
-  if (!accumulate<NEXP, false, kTauSmem, double, MS, false, false>(msm, tsm, bs, p, s, S,
-                                                                   nullptr))
-    return false;
-  float y[5], dl[5];
-#pragma unroll
-  for (int i = 0; i < 5; ++i) {
-    double a = S[i] - ed[i];
-#pragma unroll
-    for (int j = 0; j < 5; ++j) a += cs.L0inv(sym5(i, j)) * (s[j] - lam[j]);
-    y[i] = (float)-a;
-  }
-  ldlt5_apply(fac, fac + 10, y, dl);
-  double dn = 0.0, sn = 0.0;
-#pragma unroll
-  for (int c = 0; c < 5; ++c) {
-    dn += (double)dl[c] * (double)dl[c];
-    sn += s[c] * s[c];
-  }
-  if (!(dn < tol2 * sn)) return false;  // also false for NaN
-#pragma unroll
-  for (int c = 0; c < 5; ++c) e[c] = S[c];
-  return true;
 }
 
 // SolveConstrainedConstitutiveEquations (Solvers.cpp:111-222).  ed = Edot + d~.

@@ -37,11 +37,7 @@ constexpr int nr_batch_min_blocks() {
 // three there).
 template <typename MS>
 constexpr int nr_loop_min_blocks() {
-#ifdef VPFFT_EXP_MINB
-  return sizeof(MS) == 4 ? VPFFT_EXP_MINB : 3;
-#else
   return 3;
-#endif
 }
 template <typename MS>
 constexpr int nr_loop_batch_min_blocks() {
@@ -161,7 +157,7 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const C& cs, l
 #pragma unroll
     for (int c = 0; c < 5; ++c) ed[c] = cs.edot(c) + d[c];
     double e[5];
-    bool capped, cert = false;
+    bool capped;
     if constexpr (sizeof(S) == 4) {
       // mixed precision: an FP32 Newton predictor from the previous stress,
       // then the FP64 solve from its iterate (normally one Newton step with
@@ -172,59 +168,23 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const C& cs, l
       double s0[5];
 #pragma unroll
       for (int c = 0; c < 5; ++c) s0[c] = s[c];
-#if defined(VPFFT_EXP_CERT) && defined(VPFFT_EXP_CHORD)
-      float fac[15];
-      bool ok;
-      if constexpr (NEXP > 1 && sizeof(MS) == 4) {
-        float l32[5], e32[5], cur[5];
-#pragma unroll
-        for (int c = 0; c < 5; ++c) {
-          l32[c] = (float)lam[c];
-          e32[c] = (float)ed[c];
-          cur[c] = (float)s[c];
-        }
-        ok = nr_predict_chord_f<NEXP, kTauSmem, kFull>(msm, tsm, bs, p, cs, l32, e32, cur, 8,
-                                                        &mx0, fac);
-        if (ok) {
-#pragma unroll
-          for (int c = 0; c < 5; ++c) s[c] = (double)cur[c];
-        }
-      } else {
-        ok = nr_predict_fp32<NEXP, kTauSmem, kFull>(msm, tsm, bs, p, cs, lam, ed, s, 8, &mx0,
-                                                    fac);
-      }
-      cert = ok && fp64_residual_certifies<NEXP, kTauSmem>(
-                                  msm, tsm, bs, p, cs, lam, ed, s, fac,
-                                  VPFFT_EXP_CERT * VPFFT_EXP_CERT, e);
-#elif defined(VPFFT_EXP_CERT)
-      float fac[15];
-      const bool ok = nr_predict_fp32<NEXP, kTauSmem, kFull>(msm, tsm, bs, p, cs, lam, ed, s, 8,
-                                                             &mx0, fac, VPFFT_EXP_PRED_TOL);
-      cert = ok && fp64_residual_certifies<NEXP, kTauSmem>(
-                                  msm, tsm, bs, p, cs, lam, ed, s, fac,
-                                  VPFFT_EXP_CERT * VPFFT_EXP_CERT, e);
-#else
       const bool ok =
           nr_predict_fp32<NEXP, kTauSmem, kFull>(msm, tsm, bs, p, cs, lam, ed, s, 8, &mx0);
-#endif
       if (mx0 < 1e-10f) status |= kStatusMaxRssTiny;
-      capped = false;
-      if (!cert) {
-        if (!ok) {
-          const double mx = max_resolved<kTauSmem>(msm, tsm, bs, p, s0);
+      if (!ok) {
+        const double mx = max_resolved<kTauSmem>(msm, tsm, bs, p, s0);
 #pragma unroll
-          for (int c = 0; c < 5; ++c) s[c] = s0[c] / mx;
-        }
-        double el[5];
-        bool tight;
-        nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, cs, lam, ed, s, nullptr, &capped, el,
-                                            &tight);
-        if (!capped && tight) {
+        for (int c = 0; c < 5; ++c) s[c] = s0[c] / mx;
+      }
+      double el[5];
+      bool tight;
+      nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, cs, lam, ed, s, nullptr, &capped, el,
+                                          &tight);
+      if (!capped && tight) {
 #pragma unroll
-          for (int c = 0; c < 5; ++c) e[c] = el[c];
-        } else {
-          apply_smem<NEXP, kTauSmem>(msm, tsm, bs, p, s, e);
-        }
+        for (int c = 0; c < 5; ++c) e[c] = el[c];
+      } else {
+        apply_smem<NEXP, kTauSmem>(msm, tsm, bs, p, s, e);
       }
     } else {
       const double mx = max_resolved<kTauSmem>(msm, tsm, bs, p, s);
@@ -234,11 +194,7 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const C& cs, l
       nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, cs, lam, ed, s, nullptr, &capped);
       apply_smem<NEXP, kTauSmem>(msm, tsm, bs, p, s, e);
     }
-#ifdef VPFFT_EXP_COUNT
-    capped_count += cert ? 1 : 0;  // experiment: count the certified voxels instead
-#else
     capped_count += capped ? 1 : 0;
-#endif
     double P[5];
 #pragma unroll
     for (int i = 0; i < 5; ++i) {
@@ -273,124 +229,6 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const C& cs, l
   block_reduce_store<12, kVoxelBlock>(acc, partials + (long long)blk * 12);
 }
 
-#ifdef VPFFT_EXP_LOWREG
-// Mixed-precision body with fewer live registers: the voxel's fields are held
-// as FP32 (their storage type) until the FP64 stage, and the 12 running sums
-// live in shared memory (one column per thread) instead of registers.
-template <typename MS, int NEXP, bool kTauSmem, bool kFull, class C>
-__device__ __forceinline__ void nr_update_body_mixed(const NRParams& p, const C& cs, long long n,
-                                                     const FieldPtrs<float>& f, double* partials,
-                                                     IterCtrl* ctrl, int blk, int nblk, MS* msm,
-                                                     MS* tsm) {
-  constexpr int bs = kVoxelBlock;
-  __shared__ double sacc[12][kVoxelBlock];
-  const int t = threadIdx.x;
-#pragma unroll
-  for (int k = 0; k < 12; ++k) sacc[k][t] = 0.0;
-  unsigned long long capped_count = 0;
-  int status = 0;
-  for (long long v = (long long)blk * bs + t; v < n; v += (long long)nblk * bs) {
-    voxel_schmid<kTauSmem>(f, n, v, msm, tsm, bs);
-    float s32[5], l32[5], d32[5], e32[5], cur[5];
-#pragma unroll
-    for (int c = 0; c < 5; ++c) {
-      s32[c] = f.sigma[c * n + v];
-      l32[c] = f.lambda[c * n + v];
-      d32[c] = f.work[c * n + v];
-    }
-    if (f.dkeep) {
-#pragma unroll
-      for (int c = 0; c < 5; ++c) f.dkeep[c * n + v] = d32[c];
-    }
-#pragma unroll
-    for (int c = 0; c < 5; ++c) {
-      e32[c] = (float)(cs.edot(c) + (double)d32[c]);
-      cur[c] = s32[c];
-    }
-    float mx0;
-    double s[5], lam[5], ed[5], e[5];
-    bool capped = false, cert = false;
-#ifdef VPFFT_EXP_CERT
-    float fac[15];
-    const bool ok = nr_predict_fp32_f<NEXP, kTauSmem, kFull>(msm, tsm, bs, p, cs, l32, e32, cur,
-                                                             8, &mx0, fac, VPFFT_EXP_PRED_TOL);
-#pragma unroll
-    for (int c = 0; c < 5; ++c) {
-      s[c] = ok ? (double)cur[c] : (double)s32[c];
-      lam[c] = (double)l32[c];
-      ed[c] = cs.edot(c) + (double)d32[c];
-    }
-    cert = ok && fp64_residual_certifies<NEXP, kTauSmem>(msm, tsm, bs, p, cs, lam, ed, s, fac,
-                                                         VPFFT_EXP_CERT * VPFFT_EXP_CERT, e);
-#else
-    const bool ok = nr_predict_fp32_f<NEXP, kTauSmem, kFull>(msm, tsm, bs, p, cs, l32, e32, cur,
-                                                             8, &mx0);
-#pragma unroll
-    for (int c = 0; c < 5; ++c) {
-      s[c] = ok ? (double)cur[c] : (double)s32[c];
-      lam[c] = (double)l32[c];
-      ed[c] = cs.edot(c) + (double)d32[c];
-    }
-#endif
-    if (mx0 < 1e-10f) status |= kStatusMaxRssTiny;
-    if (!cert) {
-      if (!ok) {
-        const double mx = max_resolved<kTauSmem>(msm, tsm, bs, p, s);
-#pragma unroll
-        for (int c = 0; c < 5; ++c) s[c] = s[c] / mx;
-      }
-      double el[5];
-      bool tight;
-      nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, cs, lam, ed, s, nullptr, &capped, el,
-                                          &tight);
-      if (!capped && tight) {
-#pragma unroll
-        for (int c = 0; c < 5; ++c) e[c] = el[c];
-      } else {
-        apply_smem<NEXP, kTauSmem>(msm, tsm, bs, p, s, e);
-      }
-    }
-#ifdef VPFFT_EXP_COUNT
-    capped_count += cert ? 1 : 0;
-#else
-    capped_count += capped ? 1 : 0;
-#endif
-    double es = 0.0, ee = 0.0;
-#pragma unroll
-    for (int i = 0; i < 5; ++i) {
-      double ld = 0.0, lt = 0.0;
-#pragma unroll
-      for (int j = 0; j < 5; ++j) {
-        const double l0 = cs.L0(j * 5 + i);
-        ld += l0 * (double)d32[j];
-        lt += l0 * (ed[j] - e[j]);
-      }
-      f.work[i * n + v] = (float)(s[i] - ld);
-      lam[i] += lt;
-    }
-#pragma unroll
-    for (int c = 0; c < 5; ++c) {
-      f.sigma[c * n + v] = (float)s[c];
-      f.lambda[c * n + v] = (float)lam[c];
-      sacc[c][t] += s[c];
-      sacc[5 + c][t] += e[c];
-      const double ds = s[c] - lam[c];
-      const double de = e[c] - cs.edot(c) - (double)d32[c];
-      es += ds * ds;
-      ee += de * de;
-    }
-    sacc[10][t] += sqrt(es);
-    sacc[11][t] += sqrt(ee);
-  }
-  if (status) atomicOr(&ctrl->status, status);
-  if (capped_count) atomicAdd(&ctrl->nr_capped, capped_count);
-  double acc[12];
-#pragma unroll
-  for (int k = 0; k < 12; ++k) acc[k] = sacc[k][t];
-  block_reduce_store<12, kVoxelBlock>(acc, partials + (long long)blk * 12);
-}
-#endif
-
 template <typename S, typename MS, int NEXP, bool kTauSmem>
 __global__ void __launch_bounds__(kVoxelBlock, nr_loop_min_blocks<MS>())
     k_nr_update(const __grid_constant__ NRParams p, const __grid_constant__ FieldPtrs<S> f,
@@ -399,18 +237,6 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_loop_min_blocks<MS>())
   extern __shared__ __align__(16) unsigned char nr_smem[];
   MS* msm = reinterpret_cast<MS*>(nr_smem) + SL<MS>::kThreadStride * threadIdx.x;
   MS* tsm = msm + 60 * kVoxelBlock;
-#ifdef VPFFT_EXP_LOWREG
-  if constexpr (sizeof(S) == 4) {
-#ifdef VPFFT_EXP_NOFULL
-    constexpr bool kF = false;
-#else
-    constexpr bool kF = true;
-#endif
-    nr_update_body_mixed<MS, NEXP, kTauSmem, kF>(p, ParamConsts{p}, p.n, f, partials, ctrl,
-                                                 blockIdx.x, gridDim.x, msm, tsm);
-    return;
-  }
-#endif
   nr_update_body<S, MS, NEXP, kTauSmem, true>(p, ParamConsts{p}, p.n, f, partials, ctrl,
                                               blockIdx.x, gridDim.x, msm, tsm);
 }
