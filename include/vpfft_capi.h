@@ -346,14 +346,15 @@ typedef struct {
   int32_t iterations_per_tick;  /* fixed-point iterations enqueued per tick (default 8) */
   int64_t hbm_budget_bytes;     /* device memory for in-flight spectra (default 8 GiB) */
   int32_t use_graphs;           /* replay the tick's iterations from a CUDA graph (default 1) */
-  int32_t fft_tiles;            /* tile family of the batched FFT passes: 0, 1, 2 = tiles of
-                                   about 512, 1024, 2048 complex values per buffer (clamped per
-                                   axis to the longest its line engine has; default 2, the
-                                   same results bit for bit as the single-grid path); -1 =
-                                   autotuned per RVE size (vpfft_batch_get_tunings).  FP64
-                                   results are the same bit for bit in every family; FP32
-                                   passes of different families are separately compiled
-                                   kernels whose last bits can differ. */
+  int32_t fft_tiles;            /* tile family of the batched FFT passes: -1 (the default) =
+                                   autotuned per RVE size: the first admission of a size times
+                                   the five-pass chain in every family and keeps the fastest
+                                   (vpfft_batch_get_tunings); 0, 1, 2 = tiles of about 512,
+                                   1024, 2048 complex values per buffer (clamped per axis to
+                                   the longest its line engine has).  A family only regroups
+                                   lines into blocks and every family performs the same
+                                   operations, so results are the same bit for bit in every
+                                   family, in both precisions, and as the single-grid path. */
 } vpfft_batch_options;
 typedef struct {
   int64_t request_id;

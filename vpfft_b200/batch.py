@@ -38,7 +38,7 @@ class Batch:
     def __init__(self, precision: str = "mixed", material: capi.Material | None = None,
                  options: capi.SolverOptions | None = None, max_slots: int = 256,
                  iterations_per_tick: int = 8, hbm_budget_bytes: int = 8 << 30,
-                 use_graphs: bool = True, fft_tiles: int = 2):
+                 use_graphs: bool = True, fft_tiles: int = -1):
         lib = capi.load()
         bo = capi.BatchOptions()
         lib.vpfft_batch_options_default(C.byref(bo))

@@ -337,8 +337,10 @@ vpfft_status admit(vpfft_batch* b, std::vector<int>& admitted) {
 }
 
 // ---- autotuner of the batched FFT passes' tile family (vpfft_batch_options
-// fft_tiles = -1).  A family only regroups lines into blocks: FP64 results
-// are the same bit for bit, FP32 ones can differ in the last bits.
+// fft_tiles = -1, the default).  A family only regroups lines into blocks and
+// performs the same operations (the line transforms spell out their fused
+// multiply-adds and are built without contraction): results are the same bit
+// for bit in every family.
 struct TileChoice {
   int fam;
   double ms[3];
@@ -738,7 +740,7 @@ void vpfft_batch_options_default(vpfft_batch_options* o) {
   o->iterations_per_tick = 8;
   o->hbm_budget_bytes = 8LL << 30;
   o->use_graphs = 1;
-  o->fft_tiles = 2;
+  o->fft_tiles = -1;
 }
 
 vpfft_status vpfft_batch_create(vpfft_precision precision, const vpfft_material* material,

@@ -450,7 +450,12 @@ __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, in
 // The stopping test |delta| / |avg| < eps is taken on the squared norms
 // (|delta|^2 < eps^2 |avg|^2); *rel_out (optional) gets the last step's ratio,
 // *tight (optional) whether it was below 1e-5.
-template <int NEXP, bool kTauSmem, typename MS, class C = ParamConsts>
+// kSolveF32: the Newton system, formed in FP64 (residual and Jacobian), is
+// solved by an FP32 LDL^T (the mixed path's final step, which is small: the
+// step's relative error ~1e-6 is a relative change of sigma far below FP32
+// storage, and the next step, if any, sees the FP64 residual); otherwise by
+// an FP64 LDL^T (the FP64 path, the reference's arithmetic).
+template <int NEXP, bool kTauSmem, typename MS, class C = ParamConsts, bool kSolveF32 = false>
 __device__ __forceinline__ int nr_constrained_smem(const MS* msm, const MS* tsm, int bs,
                                                    const NRParams& p, const C& cs,
                                                    const double lam[5],
@@ -501,7 +506,18 @@ __device__ __forceinline__ int nr_constrained_smem(const MS* msm, const MS* tsm,
 #pragma unroll
     for (int k = 0; k < 15; ++k) K[k] += cs.L0inv(k);
     double delta[5];
-    ldlt5_solve<double>(K, y, delta);
+    if constexpr (kSolveF32) {
+      float Kf[15], yf[5], df[5];
+#pragma unroll
+      for (int k = 0; k < 15; ++k) Kf[k] = (float)K[k];
+#pragma unroll
+      for (int c = 0; c < 5; ++c) yf[c] = (float)y[c];
+      ldlt5_solve<float>(Kf, yf, df);
+#pragma unroll
+      for (int c = 0; c < 5; ++c) delta[c] = (double)df[c];
+    } else {
+      ldlt5_solve<double>(K, y, delta);
+    }
     dn = 0.0;
     an = 0.0;
 #pragma unroll

@@ -161,7 +161,7 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const C& cs, l
     if constexpr (sizeof(S) == 4) {
       // mixed precision: an FP32 Newton predictor from the previous stress,
       // then the FP64 solve from its iterate (normally one Newton step with
-      // FP64 residual and Jacobian).  If the predictor fails, the FP64 solve
+      // FP64 residual and Jacobian, its 5x5 system solved in FP32).  If the predictor fails, the FP64 solve
       // starts where the reference's does, at sigma / MaxRSS.  The strain rate
       // comes from the last Newton linearisation when that step was tiny.
       float mx0;
@@ -178,8 +178,8 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const C& cs, l
       }
       double el[5];
       bool tight;
-      nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, cs, lam, ed, s, nullptr, &capped, el,
-                                          &tight);
+      nr_constrained_smem<NEXP, kTauSmem, MS, C, true>(msm, tsm, bs, p, cs, lam, ed, s, nullptr,
+                                                       &capped, el, &tight);
       if (!capped && tight) {
 #pragma unroll
         for (int c = 0; c < 5; ++c) e[c] = el[c];
