@@ -91,7 +91,15 @@ typedef struct {
   double nr_epsilon;          /* 5e-4  (fixed-point loop) */
   double nr_max_resolved;     /* 1e9 */
   int32_t nr_max_iter;        /* 100 */
-  int32_t pad_;
+  int32_t green_operator;     /* the x pass's Green operator (no counterpart in the reference,
+                                 which recomputes it per wave vector, MaterialGrid.cpp:682-743):
+                                 0 (default) = chosen per grid size: where a stored table of the
+                                 operator (25 values per wave vector of the half spectrum) would
+                                 take at most 256 MiB, the first solve of that size times the x
+                                 pass computing the operator against one reading the table and
+                                 keeps the faster (vpfft_grid_green_operator); 1 = always compute;
+                                 2 = always store (rebuilt at each fixed-point loop, since L0 and
+                                 the voxel lengths change per increment) */
 } vpfft_solver_options;
 
 typedef struct {
@@ -225,6 +233,12 @@ int64_t vpfft_grid_launch_count(const vpfft_grid *g);
 vpfft_status vpfft_grid_set_profiling(vpfft_grid *g, int enabled);
 vpfft_status vpfft_grid_phase_times(const vpfft_grid *g, double *ms_total, int64_t *launches);
 const char *vpfft_phase_name(int phase);
+/* The Green operator in use (vpfft_solver_options.green_operator): *mode = 1
+ * computed per wave vector, 2 read from the stored table, 0 not chosen yet;
+ * ms_compute / ms_table (may be NULL) get the x pass's times measured when the
+ * choice was made (0 where not timed). */
+vpfft_status vpfft_grid_green_operator(const vpfft_grid *g, int *mode, double *ms_compute,
+                                       double *ms_table);
 /* Last error message of the grid (or of the library when g is NULL). */
 const char *vpfft_last_error(const vpfft_grid *g);
 

@@ -1,0 +1,94 @@
+"""The x pass with the Green operator read from a stored table
+(vpfft_solver_options.green_operator = 2) instead of computed per wave vector:
+the FP64 path still matches the reference (golden c1_16: iteration count,
+<sigma> within 1e-9 at every iteration, fields within 1e-7); mixed precision
+agrees with the computed operator to rounding; the automatic choice times both
+on the first solve of a size, keeps the faster, and reuses the choice for the
+next grid of that size; sizes whose table would exceed 256 MiB compute."""
+import numpy as np
+import pytest
+
+import vpfft_b200 as vp
+from vpfft_b200 import capi, fixtures
+
+pytestmark = pytest.mark.gpu
+
+
+def _material(g):
+    return capi.material(gamma_dot_base=float(g["gamma_dot_base"]),
+                         rate_sensitivity=int(g["rate_sensitivity"]), crss=float(g["crss0"]),
+                         tau0=float(g["tau0"]), tau1=float(g["tau1"]), theta0=float(g["theta0"]),
+                         theta1=float(g["theta1"]), hardening=float(g["hardening"]))
+
+
+def _run(g, precision, mode):
+    dims = tuple(int(x) for x in g["dims"])
+    grid = vp.MaterialGrid(*dims, material=_material(g), precision=precision,
+                           options=capi.solver_options(mode))
+    grid.SendDataAndInitialize(g["R_in"], np.zeros((grid.N, 5)))
+    grid.SetVoxelLength(*[float(x) for x in g["h"]])
+    e = g["edot"]
+    grid.InitializeComputation(e)
+    grid.BuildLinearRefMediumStiffness()
+    hist = grid.FixedPoint(e, int(g["max_iter"]), float(g["eps"]))
+    out = (hist, grid.Stress(), grid.green_operator())
+    grid.close()
+    return out
+
+
+def test_stored_operator_fp64_matches_reference(golden, lib):
+    g = golden("c1_16")
+    hist, sigma, info = _run(g, "fp64", 2)
+    assert info["mode"] == 2
+    assert len(hist) == int(g["iters"][0])
+    ref = g["history"][: len(hist)]
+    rel = np.linalg.norm(hist[:, :5] - ref[:, :5], axis=1) / np.linalg.norm(ref[:, :5], axis=1)
+    assert rel.max() <= 1e-9
+    vrel = np.linalg.norm(sigma - g["sigma"], axis=1) / np.linalg.norm(g["sigma"], axis=1)
+    assert vrel.max() <= 1e-7
+
+
+def test_stored_operator_mixed_agrees_with_computed(golden, lib):
+    g = golden("n20_16")
+    h1, s1, i1 = _run(g, "mixed", 1)
+    h2, s2, i2 = _run(g, "mixed", 2)
+    assert (i1["mode"], i2["mode"]) == (1, 2)
+    rel = np.linalg.norm(h2[:, :5] - h1[:, :5], axis=1) / np.linalg.norm(h1[:, :5], axis=1)
+    assert rel.max() <= 1e-5, rel.max()
+
+
+def test_automatic_choice_is_timed_and_cached(lib):
+    n = 64
+    R = fixtures.polycrystal(n, n, n, 20, 3)
+    e = fixtures.edot_from_matrix(np.diag([1.0, 0.0, -1.0]))
+    mat = vp.material(gamma_dot_base=1.0, rate_sensitivity=10, crss=1.0)
+    seen = []
+    for _ in range(2):
+        grid = vp.MaterialGrid(n, n, n, material=mat, precision="mixed")
+        grid.SendDataAndInitialize(R)
+        assert grid.green_operator()["mode"] == 0
+        grid.RunSingleStrainStep(e, 3, 0.005, 0.0)
+        info = grid.green_operator()
+        grid.close()
+        assert info["mode"] in (1, 2)
+        assert info["ms_compute"] > 0 and info["ms_table"] > 0
+        assert info["mode"] == (2 if info["ms_table"] < info["ms_compute"] else 1)
+        seen.append(info)
+    assert seen[0] == seen[1]  # the second grid of the size reuses the timing
+
+
+def test_large_table_is_not_tried(lib):
+    n = 150  # FP64 table: 25 x 150 x 150 x 76 x 8 B = 342 MB > 256 MiB
+    R = fixtures.polycrystal(n, n, n, 20, 4)
+    e = fixtures.edot_from_matrix(np.diag([1.0, 0.0, -1.0]))
+    grid = vp.MaterialGrid(n, n, n, material=vp.material(1.0, 10, 1.0), precision="fp64")
+    grid.SendDataAndInitialize(R)
+    grid.RunSingleStrainStep(e, 2, 0.005, 0.0)
+    info = grid.green_operator()
+    grid.close()
+    assert info == {"mode": 1, "ms_compute": 0.0, "ms_table": 0.0}
+
+
+def test_bad_option_rejected(lib):
+    with pytest.raises(vp.VpfftError):
+        vp.MaterialGrid(8, 8, 8, options=capi.solver_options(3))

@@ -81,7 +81,7 @@ class SolverOptions(C.Structure):
         ("nr_epsilon", C.c_double),
         ("nr_max_resolved", C.c_double),
         ("nr_max_iter", C.c_int32),
-        ("pad_", C.c_int32),
+        ("green_operator", C.c_int32),
     ]
 
 
@@ -221,6 +221,7 @@ _PROTOS = {
                                     C.c_int]),
     "vpfft_fft3d_r2c": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _D, _D, C.c_int]),
     "vpfft_set_tma_passes": (C.c_int, [C.c_int]),
+    "vpfft_grid_green_operator": (C.c_int, [_G, C.POINTER(C.c_int), _D, _D]),
     "vpfft_fft3d_c2r": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _D, _D, C.c_int]),
     "vpfft_fixture_polycrystal": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, _D,
                                             _I32]),
@@ -322,6 +323,15 @@ def material(gamma_dot_base=15.5, rate_sensitivity=10, crss=11.0, tau0=11.0, tau
     m.rate_sensitivity[:] = list(np.broadcast_to(np.asarray(rate_sensitivity, np.int32), (NSYS,)))
     m.hardening[:] = list(np.broadcast_to(np.asarray(hardening, np.float64), (NSYS, NSYS)).ravel())
     return m
+
+
+def solver_options(green_operator: int = 0) -> SolverOptions:
+    """The default solver constants (the reference's, vpfft_solver_options_default)
+    with the x pass's Green operator: 0 chosen per grid size, 1 computed, 2 stored."""
+    o = SolverOptions()
+    load().vpfft_solver_options_default(C.byref(o))
+    o.green_operator = int(green_operator)
+    return o
 
 
 def device_count() -> int:

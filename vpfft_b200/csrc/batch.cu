@@ -844,8 +844,15 @@ vpfft_status vpfft_batch_submit(vpfft_batch* b, vpfft_grid* g, const double edot
   if (!b || !g || !edot) return bfail(b, VPFFT_ERR_INVALID_ARGUMENT, "NULL argument");
   if (g->prec != b->prec) return bfail(b, VPFFT_ERR_INVALID_ARGUMENT, "grid precision differs from the batch's");
   if (g->device != b->device) return bfail(b, VPFFT_ERR_INVALID_ARGUMENT, "grid lives on another device");
-  if (std::memcmp(&g->mat, &b->mat, sizeof(vpfft_material)) != 0 ||
-      std::memcmp(&g->opt, &b->opt, sizeof(vpfft_solver_options)) != 0)
+  // the solver constants must agree (field by field: the struct has padding);
+  // green_operator does not apply to batched solves (they compute the operator)
+  const vpfft_solver_options& go = g->opt;
+  const vpfft_solver_options& bo = b->opt;
+  const bool same_opt = go.init_nr_epsilon == bo.init_nr_epsilon &&
+                        go.init_nr_max_iter == bo.init_nr_max_iter &&
+                        go.nr_epsilon == bo.nr_epsilon && go.nr_max_resolved == bo.nr_max_resolved &&
+                        go.nr_max_iter == bo.nr_max_iter;
+  if (std::memcmp(&g->mat, &b->mat, sizeof(vpfft_material)) != 0 || !same_opt)
     return bfail(b, VPFFT_ERR_INVALID_ARGUMENT, "grid material or solver options differ from the batch's");
   if (!g->fields_set) return bfail(b, VPFFT_ERR_NOT_INITIALIZED, "grid fields not set");
   if (max_iter < 1) return bfail(b, VPFFT_ERR_INVALID_ARGUMENT, "max_iter must be >= 1");

@@ -10,6 +10,10 @@
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -315,7 +319,7 @@ vpfft_status upload_twiddles(vpfft_grid* g) {
 void free_grid_buffers(vpfft_grid* g) {
   void* ptrs[] = {g->R,   g->sigma, g->lambda, g->work,     g->dkeep, g->crss,
                   g->acc, g->X,     g->X2,     g->twx,      g->twy,   g->twz,
-                  g->partials, g->sum25, g->ctrl, g->hist, g->staging};
+                  g->partials, g->sum25, g->ctrl, g->hist, g->staging, g->gtab};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (g->h_ctrl) cudaFreeHost(g->h_ctrl);
@@ -403,6 +407,96 @@ vpfft_status do_ref_medium(vpfft_grid* g, double* L0_out) {
   return VPFFT_OK;
 }
 
+// ---- the x pass's Green operator: computed per wave vector or stored.
+// A stored table costs 25 values per wave vector of the half spectrum in HBM
+// traffic per iteration against ~300 operations per wave vector recomputed;
+// which is faster depends on the size (a table that stays in L2 can win), so
+// it is timed: the first solve of a size (per device and precision) times the
+// x pass both ways on the spare spectrum buffer A (free between the forward y
+// pass and the inverse one; not read before the next z pass rewrites it) and
+// keeps the faster.  Tables above kGreenTableMax bytes are not tried.
+constexpr size_t kGreenTableMax = 256ull << 20;
+std::mutex g_green_mu;
+std::map<std::tuple<int, int, int, int, int>, std::pair<int, std::pair<double, double>>>
+    g_green_choice;  // (device, bytes, nx, ny, nz) -> (mode, (ms computed, ms stored))
+
+template <typename S>
+size_t green_table_bytes(const vpfft_grid* g) {
+  return sizeof(S) * 25 * (size_t)g->nh * g->ny * g->nx;
+}
+
+template <typename S>
+vpfft_status time_x_pass(vpfft_grid* g, const Spectral<S>& sp, const GreenParams<S>& gp,
+                         const S* tab, double* ms) {
+  cudaEvent_t e0, e1;
+  CK(g, cudaEventCreate(&e0));
+  CK(g, cudaEventCreate(&e1));
+  launch_x_pass<S>(sp, gp, tab, g->X, 5, g->stream);  // warm-up
+  CK(g, cudaEventRecord(e0, g->stream));
+  constexpr int kReps = 3;
+  for (int r = 0; r < kReps; ++r) launch_x_pass<S>(sp, gp, tab, g->X, 5, g->stream);
+  CK(g, cudaEventRecord(e1, g->stream));
+  CKL(g);
+  CK(g, cudaEventSynchronize(e1));
+  float t = 0.f;
+  CK(g, cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = (double)t / kReps;
+  return VPFFT_OK;
+}
+
+// Picks the operator (if not done for this grid) and, when it is the stored
+// one, rebuilds the table for the current L0 and voxel lengths.
+template <typename S>
+vpfft_status prepare_green(vpfft_grid* g, const Spectral<S>& sp, const GreenParams<S>& gp) {
+  const size_t bytes = green_table_bytes<S>(g);
+  auto ensure_table = [&]() -> vpfft_status {
+    if (!g->gtab) CK(g, cudaMalloc(&g->gtab, bytes));
+    g->launches += launch_green_table<S>(gp, (S*)g->gtab, g->nh, g->stream);
+    CKL(g);
+    return VPFFT_OK;
+  };
+  if (g->green_mode == 0) {
+    const int opt = g->opt.green_operator;
+    if (opt == 1 || opt == 2) {
+      g->green_mode = opt;
+    } else if (bytes > kGreenTableMax) {
+      g->green_mode = 1;
+    } else {
+      const auto key = std::make_tuple(g->device, (int)sizeof(S), g->nx, g->ny, g->nz);
+      bool cached = false;
+      {
+        std::lock_guard<std::mutex> lk(g_green_mu);
+        auto it = g_green_choice.find(key);
+        if (it != g_green_choice.end()) {
+          g->green_mode = it->second.first;
+          g->green_ms[0] = it->second.second.first;
+          g->green_ms[1] = it->second.second.second;
+          cached = true;
+        }
+      }
+      if (!cached) {
+        if (vpfft_status r = ensure_table()) return r;
+        if (vpfft_status r = time_x_pass<S>(g, sp, gp, nullptr, &g->green_ms[0])) return r;
+        if (vpfft_status r = time_x_pass<S>(g, sp, gp, (const S*)g->gtab, &g->green_ms[1]))
+          return r;
+        g->green_mode = g->green_ms[1] < g->green_ms[0] ? 2 : 1;
+        std::lock_guard<std::mutex> lk(g_green_mu);
+        g_green_choice.emplace(key, std::make_pair(g->green_mode,
+                                                   std::make_pair(g->green_ms[0], g->green_ms[1])));
+      }
+    }
+  }
+  if (g->green_mode == 2) return ensure_table();
+  if (g->gtab) {  // computed operator chosen: the table is not needed
+    CK(g, cudaStreamSynchronize(g->stream));
+    cudaFree(g->gtab);
+    g->gtab = nullptr;
+  }
+  return VPFFT_OK;
+}
+
 template <typename S>
 vpfft_status do_fixed_point(vpfft_grid* g, const double edot[5], int max_iter, double eps,
                             double* history, vpfft_stats* st) {
@@ -415,6 +509,8 @@ vpfft_status do_fixed_point(vpfft_grid* g, const double edot[5], int max_iter, d
   NRParams p = nr_params(g, edot, false);
   GreenParams<S> gp = green_params<S>(g->nx, g->ny, g->nz, g->h, g->L0, g->Linv);
   Spectral<S> sp = spectral<S>(g, g->X, g->X2);
+  if (vpfft_status r = prepare_green<S>(g, sp, gp)) return r;
+  const S* gtab = g->green_mode == 2 ? (const S*)g->gtab : nullptr;
   FieldPtrs<S> f = fields<S>(g);
   const int batch = g->n >= (1LL << 21) ? 4 : 16;
   constexpr int kEv = 8;  // events per iteration when profiling
@@ -434,7 +530,7 @@ vpfft_status do_fixed_point(vpfft_grid* g, const double edot[5], int max_iter, d
     int n = 0;
     for (int b = 0; b < batch; ++b) {
       cudaEvent_t* e = profiled ? &g->ev[(size_t)b * kEv] : nullptr;
-      n += launch_spectral_iteration<S>(sp, gp, (S*)g->work, g->ctrl, g->stream, 5, e);
+      n += launch_spectral_iteration<S>(sp, gp, (S*)g->work, g->ctrl, g->stream, 5, e, gtab);
       n += launch_nr_update<S>(p, f, g->partials, g->ctrl, g->hist, g->stream,
                                e ? e + 6 : nullptr);
     }
@@ -612,7 +708,7 @@ void vpfft_solver_options_default(vpfft_solver_options* o) {
   o->nr_epsilon = 5e-4;       // 909
   o->nr_max_resolved = 1e9;   // 910
   o->nr_max_iter = 100;       // 911
-  o->pad_ = 0;
+  o->green_operator = 0;      // chosen per grid size
 }
 
 vpfft_status vpfft_grid_create(int nx, int ny, int nz, const vpfft_material* material,
@@ -630,6 +726,8 @@ vpfft_status vpfft_grid_create(int nx, int ny, int nz, const vpfft_material* mat
       if (!(material->crss[k] > 0) || !(material->gamma_dot_base[k] > 0))
         return fail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "CRSS and reference rates must be > 0");
   }
+  if (options && (options->green_operator < 0 || options->green_operator > 2))
+    return fail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "green_operator must be 0, 1 or 2");
   vpfft_status s = need_device(nullptr);
   if (s != VPFFT_OK) return s;
   vpfft_grid* g = new vpfft_grid();
@@ -1312,6 +1410,15 @@ vpfft_status vpfft_fft3d_r2c(int nx, int ny, int nz, int ncomp, const double* re
                                  : fft_impl<float>(nx, ny, nz, ncomp, real, spec, 0);
 }
 int vpfft_set_tma_passes(int enable) { return vpfft::set_tma_passes(enable); }
+
+vpfft_status vpfft_grid_green_operator(const vpfft_grid* g, int* mode, double* ms_compute,
+                                       double* ms_table) {
+  if (!g || !mode) return VPFFT_ERR_INVALID_ARGUMENT;
+  *mode = g->green_mode;
+  if (ms_compute) *ms_compute = g->green_ms[0];
+  if (ms_table) *ms_table = g->green_ms[1];
+  return VPFFT_OK;
+}
 
 vpfft_status vpfft_fft3d_c2r(int nx, int ny, int nz, int ncomp, const double* spec, double* real,
                              vpfft_precision prec) {

@@ -89,7 +89,7 @@ PassSmem<S> pass_smem(const Spectral<S>& sp, int tz, int ty, int tk, int ncomp) 
 template <typename S>
 int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S* work,
                               const IterCtrl* ctrl, cudaStream_t st, int ncomp,
-                              cudaEvent_t* ev) {
+                              cudaEvent_t* ev, const S* gtab) {
   using T = typename CX<S>::T;
   const PassSet<S>& Z = pass_set<S>(sp.pz);
   const PassSet<S>& Y = pass_set<S>(sp.py);
@@ -112,8 +112,8 @@ int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S
   if (!y_fwd_tma(sp, ctrl, st, ncomp))
     Y.y_fwd<<<gy, Y.threads, sm.y, st>>>(A, B, sp.py, sp.px.by_n, twy, sp.nx, sp.nh, ctrl);
   if (ev) cudaEventRecord(ev[2], st);
-  X.x_green<<<gx, X.threads_x, sm.x, st>>>(B, sp.px, sp.py.by_n, twx, gp, sp.ny, sp.nh, ncomp,
-                                         ctrl);
+  (gtab ? X.x_table : X.x_green)<<<gx, X.threads_x, sm.x, st>>>(B, sp.px, sp.py.by_n, twx, gp,
+                                                               gtab, sp.ny, sp.nh, ncomp, ctrl);
   if (ev) cudaEventRecord(ev[3], st);
   if (!y_inv_tma(sp, ctrl, st, ncomp))
     Y.y_inv<<<gy, Y.threads, sm.y, st>>>(B, A, sp.py, sp.px.by_n, twy, sp.nx, sp.nh, ctrl);
@@ -123,6 +123,52 @@ int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S
                                              scale, ctrl);
   if (ev) cudaEventRecord(ev[5], st);
   return 5;
+}
+
+// The stored Green operator: for every wave vector of the half spectrum the
+// 5x5 matrix that the x pass applies (columns from green_apply on the unit
+// vectors, so the table holds exactly the on-the-fly operator's values),
+// entry (a, b) of (f = kz ny + ky, x) at tab[(a 5 + b) M + f nx + x].
+template <typename S>
+__global__ void k_green_table(const GreenParams<S> gp, S* __restrict__ tab, int nh) {
+  const long long M = (long long)nh * gp.ny * gp.nx;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % gp.nx);
+    const long long f = i / gp.nx;
+    const int ky = (int)(f % gp.ny), kz = (int)(f / gp.ny);
+#pragma unroll 1
+    for (int b = 0; b < 5; ++b) {
+      S pre[5] = {S(0), S(0), S(0), S(0), S(0)}, pim[5] = {S(0), S(0), S(0), S(0), S(0)};
+      pre[b] = S(1);
+      green_apply<S>(gp, x, ky, kz, pre, pim);
+#pragma unroll
+      for (int a = 0; a < 5; ++a) tab[(a * 5 + b) * M + i] = pre[a];
+    }
+  }
+}
+
+template <typename S>
+int launch_green_table(const GreenParams<S>& gp, S* tab, int nh, cudaStream_t st) {
+  const long long M = (long long)nh * gp.ny * gp.nx;
+  const int blocks = (int)std::min<long long>((M + 255) / 256, 148LL * 16);
+  k_green_table<S><<<blocks, 256, 0, st>>>(gp, tab, nh);
+  return 1;
+}
+
+template <typename S>
+int launch_x_pass(const Spectral<S>& sp, const GreenParams<S>& gp, const S* gtab, void* buf,
+                  int ncomp, cudaStream_t st) {
+  using T = typename CX<S>::T;
+  const PassSet<S>& Z = pass_set<S>(sp.pz);
+  const PassSet<S>& Y = pass_set<S>(sp.py);
+  const PassSet<S>& X = pass_set<S>(sp.px);
+  const PassSmem<S> sm = pass_smem(sp, Z.tz, Y.ty, X.tk, ncomp);
+  const dim3 gx(cdiv(sp.nh * sp.ny, X.tk));
+  (gtab ? X.x_table : X.x_green)<<<gx, X.threads_x, sm.x, st>>>(
+      reinterpret_cast<T*>(buf), sp.px, sp.py.by_n, reinterpret_cast<const T*>(sp.twx), gp, gtab,
+      sp.ny, sp.nh, ncomp, nullptr);
+  return 1;
 }
 
 template <typename S>
@@ -147,10 +193,12 @@ int launch_fft3d(const Spectral<S>& sp, S* real, int ncomp, int mode, cudaStream
                                                sp.nh, nullptr);
     if (!y_fwd_tma(sp, nullptr, st, ncomp))
       Y.y_fwd<<<gy, Y.threads, sm.y, st>>>(A, B, sp.py, sp.px.by_n, twy, sp.nx, sp.nh, nullptr);
-    X.x_fwd<<<gx, X.threads_x, sm.x, st>>>(B, sp.px, sp.py.by_n, twx, gp, sp.ny, sp.nh, ncomp,
+    X.x_fwd<<<gx, X.threads_x, sm.x, st>>>(B, sp.px, sp.py.by_n, twx, gp, nullptr, sp.ny, sp.nh,
+                                         ncomp,
                                          nullptr);
   } else {
-    X.x_inv<<<gx, X.threads_x, sm.x, st>>>(B, sp.px, sp.py.by_n, twx, gp, sp.ny, sp.nh, ncomp,
+    X.x_inv<<<gx, X.threads_x, sm.x, st>>>(B, sp.px, sp.py.by_n, twx, gp, nullptr, sp.ny, sp.nh,
+                                         ncomp,
                                          nullptr);
     if (!y_inv_tma(sp, nullptr, st, ncomp))
       Y.y_inv<<<gy, Y.threads, sm.y, st>>>(B, A, sp.py, sp.px.by_n, twy, sp.nx, sp.nh, nullptr);
@@ -215,10 +263,16 @@ template int launch_spectral_chain<double>(const SlotDesc<double>*, const PassCh
 template int launch_spectral_chain<float>(const SlotDesc<float>*, const PassChain&, cudaStream_t);
 template int launch_spectral_iteration<double>(const Spectral<double>&, const GreenParams<double>&,
                                                double*, const IterCtrl*, cudaStream_t, int,
-                                               cudaEvent_t*);
+                                               cudaEvent_t*, const double*);
 template int launch_spectral_iteration<float>(const Spectral<float>&, const GreenParams<float>&,
                                               float*, const IterCtrl*, cudaStream_t, int,
-                                              cudaEvent_t*);
+                                              cudaEvent_t*, const float*);
+template int launch_green_table<double>(const GreenParams<double>&, double*, int, cudaStream_t);
+template int launch_green_table<float>(const GreenParams<float>&, float*, int, cudaStream_t);
+template int launch_x_pass<double>(const Spectral<double>&, const GreenParams<double>&,
+                                   const double*, void*, int, cudaStream_t);
+template int launch_x_pass<float>(const Spectral<float>&, const GreenParams<float>&, const float*,
+                                  void*, int, cudaStream_t);
 template int launch_fft3d<double>(const Spectral<double>&, double*, int, int, cudaStream_t);
 template int launch_fft3d<float>(const Spectral<float>&, float*, int, int, cudaStream_t);
 

@@ -296,12 +296,17 @@ __device__ __forceinline__ void pass_y_body(const typename CX<S>::T* __restrict_
 
 // ---------------------------------------------------------------- x pass
 // In place on B[c][kz][ky][x], lines f = kz ny + ky of all ncomp components:
-// MODE 0 forward, 1 inverse, 2 forward + Green + inverse.
+// MODE 0 forward, 1 inverse, 2 forward + Green operator computed per wave
+// vector + inverse, 3 forward + Green operator read from a stored table +
+// inverse.  The table (gtab, MODE 3) holds the 5x5 operator of every wave
+// vector of the half spectrum, entry (a, b) of wave vector (f, x) at
+// gtab[(a 5 + b) nh ny nx + f nx + x] (consecutive x contiguous: coalesced).
 template <int MODE, typename S, class E, class TL>
 __device__ __forceinline__ void pass_x_body(typename CX<S>::T* __restrict__ B, const LinePlan& pl,
                                             const FastDiv& dny,
                                             const typename CX<S>::T* __restrict__ twg,
-                                            const GreenParams<S>& gp, int ny, int nh, int ncomp,
+                                            const GreenParams<S>& gp,
+                                            const S* __restrict__ gtab, int ny, int nh, int ncomp,
                                             int bt) {
   using T = typename CX<S>::T;
   constexpr int TK = TL::kX;
@@ -350,6 +355,33 @@ __device__ __forceinline__ void pass_x_body(typename CX<S>::T* __restrict__ B, c
     }
     __syncthreads();
   }
+  if (MODE == 3) {
+    const long long M = (long long)nh * ny * nx;
+    for (int i = threadIdx.x; i < TK * nx; i += blockDim.x) {
+      const int kl = E::div_n(i, pl), xx = i - kl * nx;
+      if (kl >= nfk) continue;
+      const long long at = (long long)(f0 + kl) * nx + xx;
+      S pre[5], pim[5];
+#pragma unroll
+      for (int c = 0; c < 5; ++c) {
+        const T z = r[(c * TK + kl) * ls + sw(xx)];
+        pre[c] = z.x;
+        pim[c] = z.y;
+      }
+#pragma unroll
+      for (int a = 0; a < 5; ++a) {
+        S ar = S(0), ai = S(0);
+#pragma unroll
+        for (int b = 0; b < 5; ++b) {
+          const S gab = gtab[(a * 5 + b) * M + at];
+          ar = fmad(gab, pre[b], ar);
+          ai = fmad(gab, pim[b], ai);
+        }
+        r[(a * TK + kl) * ls + sw(xx)] = T{ar, ai};
+      }
+    }
+    __syncthreads();
+  }
   if (MODE != 0) r = E::template fft<1>(r, o, tw, pl, nl, ls, threadIdx.x, blockDim.x);
   copy_rows<T>(
       nl, nx, [&](int L, int xx) { return r[L * ls + sw(xx)]; },
@@ -388,10 +420,10 @@ __global__ void __launch_bounds__(Tiles<S, E>::kThreads)
 template <int MODE, typename S, class E>
 __global__ void __launch_bounds__(Tiles<S, E>::kThreadsX, Tiles<S, E>::kMinBlocksX)
     k_pass_x(typename CX<S>::T* __restrict__ B, LinePlan pl, FastDiv dny,
-             const typename CX<S>::T* __restrict__ twg, GreenParams<S> gp, int ny, int nh,
-             int ncomp, const IterCtrl* ctrl) {
+             const typename CX<S>::T* __restrict__ twg, GreenParams<S> gp,
+             const S* __restrict__ gtab, int ny, int nh, int ncomp, const IterCtrl* ctrl) {
   if (ctrl && ctrl->done) return;
-  pass_x_body<MODE, S, E, Tiles<S, E>>(B, pl, dny, twg, gp, ny, nh, ncomp, blockIdx.x);
+  pass_x_body<MODE, S, E, Tiles<S, E>>(B, pl, dny, twg, gp, gtab, ny, nh, ncomp, blockIdx.x);
 }
 
 // Batched passes of the fixed-point iteration (5 components): block -> slot,
@@ -476,7 +508,8 @@ __global__ void __launch_bounds__(Tiles<S, E, kEl>::kThreadsX, 512 / Tiles<S, E,
   if (!d) return;
   const FftSlot<S>& fs = sm.fs;
   pass_x_body<2, S, E, TL>(reinterpret_cast<T*>(fs.X2), d->sp.px, fs.dny,
-                           reinterpret_cast<const T*>(fs.twx), sm.gp, fs.ny, fs.nh, 5, lb);
+                           reinterpret_cast<const T*>(fs.twx), sm.gp, nullptr, fs.ny, fs.nh, 5,
+                           lb);
 }
 
 // ---------------------------------------------------------------- entry table
@@ -499,9 +532,13 @@ struct PassSet {
   void (*z_c2r)(const T*, S*, LinePlan, FastDiv, const T*, int, int, int, S, const IterCtrl*);
   void (*y_fwd)(const T*, T*, LinePlan, FastDiv, const T*, int, int, const IterCtrl*);
   void (*y_inv)(const T*, T*, LinePlan, FastDiv, const T*, int, int, const IterCtrl*);
-  void (*x_fwd)(T*, LinePlan, FastDiv, const T*, GreenParams<S>, int, int, int, const IterCtrl*);
-  void (*x_inv)(T*, LinePlan, FastDiv, const T*, GreenParams<S>, int, int, int, const IterCtrl*);
-  void (*x_green)(T*, LinePlan, FastDiv, const T*, GreenParams<S>, int, int, int,
+  void (*x_fwd)(T*, LinePlan, FastDiv, const T*, GreenParams<S>, const S*, int, int, int,
+                const IterCtrl*);
+  void (*x_inv)(T*, LinePlan, FastDiv, const T*, GreenParams<S>, const S*, int, int, int,
+                const IterCtrl*);
+  void (*x_table)(T*, LinePlan, FastDiv, const T*, GreenParams<S>, const S*, int, int, int,
+                  const IterCtrl*);
+  void (*x_green)(T*, LinePlan, FastDiv, const T*, GreenParams<S>, const S*, int, int, int,
                   const IterCtrl*);
   int nfam;                // batched tile families; the last is the long tile
   BatchPasses<S> fam[3];
@@ -556,6 +593,7 @@ PassSet<S> make_pass_set() {
   p.x_fwd = k_pass_x<0, S, E>;
   p.x_inv = k_pass_x<1, S, E>;
   p.x_green = k_pass_x<2, S, E>;
+  p.x_table = k_pass_x<3, S, E>;
   const int s = 227 * 1024;
   optin_rest(p.z_r2c, s);
   optin_rest(p.z_c2r, s);
@@ -564,6 +602,7 @@ PassSet<S> make_pass_set() {
   optin_rest(p.x_fwd, s);
   optin_rest(p.x_inv, s);
   optin_rest(p.x_green, s);
+  optin_rest(p.x_table, s);
   constexpr int nf = batch_families<S, E>();
   p.nfam = nf;
   p.fam[0] = make_batch_passes<S, E, batch_family_elems<S, E>(0)>(s);

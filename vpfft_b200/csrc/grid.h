@@ -63,6 +63,11 @@ struct vpfft_grid {
   // the fixed-point loop's chunk of iterations as a CUDA graph (re-captured for
   // each loop, replayed for its chunks after the first)
   cudaGraphExec_t loop_graph = nullptr;
+  // the x pass's Green operator: 0 not chosen yet, 1 computed per wave
+  // vector, 2 read from the stored table gtab (25 x nh ny nx values)
+  int green_mode = 0;
+  void* gtab = nullptr;
+  double green_ms[2] = {0, 0};  // x pass computed / stored, when timed
   std::string err;
 };
 

@@ -145,10 +145,22 @@ struct Spectral {
 };
 // forward: work (P) -> X ; inverse: X -> work (d~, scaled by 1/N)
 // ev (optional): 6 events recorded before the first and after each of the 5 kernels
+// gtab (optional): the stored Green operator (launch_green_table); the x pass
+// then reads it instead of computing the operator per wave vector.
 template <typename S>
 int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S* work,
                               const IterCtrl* ctrl, cudaStream_t st, int ncomp,
-                              cudaEvent_t* ev = nullptr);
+                              cudaEvent_t* ev = nullptr, const S* gtab = nullptr);
+// The stored Green operator of every wave vector of the half spectrum: 25 x
+// nh ny nx values, entry (a, b) of wave vector (f = kz ny + ky, x) at
+// tab[(a 5 + b) nh ny nx + f nx + x].
+template <typename S>
+int launch_green_table(const GreenParams<S>& gp, S* tab, int nh, cudaStream_t st);
+// The x pass alone (computed or stored Green operator) on a spectrum buffer
+// of B's layout, for timing the two against each other.
+template <typename S>
+int launch_x_pass(const Spectral<S>& sp, const GreenParams<S>& gp, const S* gtab, void* buf,
+                  int ncomp, cudaStream_t st);
 // The y and z passes with TMA-moved tiles (fft_tma.cu) for FP32 spectra whose
 // lines on the pass's axis have 64, 128 or 256 points; false (nothing
 // launched) when they do not apply.  set_tma_passes(1/0) enables / disables it process-wide (-1

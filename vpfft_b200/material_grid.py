@@ -222,6 +222,16 @@ class MaterialGrid:
         """MaterialGrid::PrintPolarization (MaterialGrid.cpp:80-100)."""
         self._print(capi.PRINT_POLARIZATION, filename)
 
+    def green_operator(self) -> dict:
+        """The x pass's Green operator (vpfft_grid_green_operator): mode 1
+        computed per wave vector, 2 stored table, 0 not chosen yet, with the x
+        pass times (ms) measured when it was chosen."""
+        mode = C.c_int()
+        a, b = C.c_double(), C.c_double()
+        check(self._lib.vpfft_grid_green_operator(self._h, C.byref(mode), C.byref(a), C.byref(b)),
+              self._h)
+        return {"mode": int(mode.value), "ms_compute": a.value, "ms_table": b.value}
+
     def launch_count(self) -> int:
         return int(self._lib.vpfft_grid_launch_count(self._h))
 
