@@ -283,6 +283,30 @@ def material_n10():
                        theta0=20.0, theta1=1.0)
 
 
+def green_operator_arm(edges=(64, 128, 256)) -> dict:
+    """The x pass's Green operator per grid size (mixed, the headline material):
+    computed per wave vector or read from a stored table, as the library
+    chooses it on a grid's first solve (the table is timed against the
+    computed operator where it would take at most 512 MiB)."""
+    import vpfft_b200 as vp
+    from vpfft_b200 import fixtures
+
+    out = {}
+    e = fixtures.edot_from_matrix(VEL_GRAD)
+    for n in edges:
+        grains = max(1, round(N_GRAINS * (n / N_GRID) ** 3))
+        g = vp.MaterialGrid(n, n, n, material=material(), precision="mixed")
+        g.SendDataAndInitialize(fixtures.polycrystal(n, n, n, grains, SEED))
+        g.RunSingleStrainStep(e, 2, 0.005, 0.0)
+        info = g.green_operator()
+        g.close()
+        out[str(n)] = {"operator": {1: "computed", 2: "stored table"}.get(info["mode"], "?"),
+                       "x_pass_ms_computed": info["ms_compute"] or None,
+                       "x_pass_ms_table": info["ms_table"] or None,
+                       "table_mib": 10 * 4 * n * n * (n // 2 + 1) / 2 ** 20}
+    return out
+
+
 def batched_arm(n_rves: int) -> dict:
     """Batched RVE solves: n_rves RVEs with edges uniform in {16, 32, 48, 64},
     8-200 Voronoi grains, random traceless velocity gradients (equivalent
@@ -748,6 +772,7 @@ def main(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-green", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--batch-rves", type=int, default=256)
     ap.add_argument("--serve-requests", type=int, default=1000)
@@ -881,6 +906,8 @@ def main(argv=None):
                        "step": ("one increment via vpfft_run_single_strain_step (max_iter 100, "
                                 "eps 1e-5) with pinned host orientation/stress in and the "
                                 "stress field out")}
+    if ws == 1 and not args.no_green:
+        line["green_operator"] = green_operator_arm()
     if ws == 1 and not args.no_batched:
         line["batched"] = batched_arm(args.batch_rves)
     if ws == 1 and not args.no_serving:

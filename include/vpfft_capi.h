@@ -94,12 +94,13 @@ typedef struct {
   int32_t green_operator;     /* the x pass's Green operator (no counterpart in the reference,
                                  which recomputes it per wave vector, MaterialGrid.cpp:682-743):
                                  0 (default) = chosen per grid size: where a stored table of the
-                                 operator (25 values per wave vector of the half spectrum) would
-                                 take at most 256 MiB, the first solve of that size times the x
-                                 pass computing the operator against one reading the table and
-                                 keeps the faster (vpfft_grid_green_operator); 1 = always compute;
-                                 2 = always store (rebuilt at each fixed-point loop, since L0 and
-                                 the voxel lengths change per increment) */
+                                 operator's costly part (10 values per wave vector of the half
+                                 spectrum) would take at most 512 MiB, the first solve of that
+                                 size times the x pass computing the operator against one
+                                 reading the table and keeps the faster
+                                 (vpfft_grid_green_operator); 1 = always compute; 2 = always
+                                 store (rebuilt at each fixed-point loop, since L0 and the voxel
+                                 lengths change per increment).  All three give the same bits. */
 } vpfft_solver_options;
 
 typedef struct {

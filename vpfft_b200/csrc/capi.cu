@@ -408,21 +408,22 @@ vpfft_status do_ref_medium(vpfft_grid* g, double* L0_out) {
 }
 
 // ---- the x pass's Green operator: computed per wave vector or stored.
-// A stored table costs 25 values per wave vector of the half spectrum in HBM
-// traffic per iteration against ~300 operations per wave vector recomputed;
-// which is faster depends on the size (a table that stays in L2 can win), so
-// it is timed: the first solve of a size (per device and precision) times the
+// A stored table costs kGreenStored values per wave vector of the half
+// spectrum in HBM traffic per iteration against the ~200 operations of
+// (V L0 V^T)^-1 and 1/(k.C k) recomputed per wave vector.  Both give the same
+// bits; which is faster depends on the size (a table that stays in L2 can
+// win), so it is timed: the first solve of a size (per device and precision) times the
 // x pass both ways on the spare spectrum buffer A (free between the forward y
 // pass and the inverse one; not read before the next z pass rewrites it) and
 // keeps the faster.  Tables above kGreenTableMax bytes are not tried.
-constexpr size_t kGreenTableMax = 256ull << 20;
+constexpr size_t kGreenTableMax = 512ull << 20;
 std::mutex g_green_mu;
 std::map<std::tuple<int, int, int, int, int>, std::pair<int, std::pair<double, double>>>
     g_green_choice;  // (device, bytes, nx, ny, nz) -> (mode, (ms computed, ms stored))
 
 template <typename S>
 size_t green_table_bytes(const vpfft_grid* g) {
-  return sizeof(S) * 25 * (size_t)g->nh * g->ny * g->nx;
+  return sizeof(S) * kGreenStored * (size_t)g->nh * g->ny * g->nx;
 }
 
 template <typename S>

@@ -126,9 +126,10 @@ int launch_spectral_iteration(const Spectral<S>& sp, const GreenParams<S>& gp, S
 }
 
 // The stored Green operator: for every wave vector of the half spectrum the
-// 5x5 matrix that the x pass applies (columns from green_apply on the unit
-// vectors, so the table holds exactly the on-the-fly operator's values),
-// entry (a, b) of (f = kz ny + ky, x) at tab[(a 5 + b) M + f nx + x].
+// kGreenStored values of green_core (C = (V L0 V^T)^-1 row-major, then
+// 1/(k.C k); zeros where the operator has no Gamma part), value j of
+// (f = kz ny + ky, x) at tab[j M + f nx + x].  The x pass then finishes the
+// operator with the arithmetic of the computed path, so both give the same bits.
 template <typename S>
 __global__ void k_green_table(const GreenParams<S> gp, S* __restrict__ tab, int nh) {
   const long long M = (long long)nh * gp.ny * gp.nx;
@@ -137,14 +138,12 @@ __global__ void k_green_table(const GreenParams<S> gp, S* __restrict__ tab, int 
     const int x = (int)(i % gp.nx);
     const long long f = i / gp.nx;
     const int ky = (int)(f % gp.ny), kz = (int)(f / gp.ny);
-#pragma unroll 1
-    for (int b = 0; b < 5; ++b) {
-      S pre[5] = {S(0), S(0), S(0), S(0), S(0)}, pim[5] = {S(0), S(0), S(0), S(0), S(0)};
-      pre[b] = S(1);
-      green_apply<S>(gp, x, ky, kz, pre, pim);
+    GreenPoint<S> q;
+    S C[3][3] = {}, ikak = S(0);
+    if (green_geometry(gp, x, ky, kz, q) && q.wg != S(0)) green_core(gp, q, C, ikak);
 #pragma unroll
-      for (int a = 0; a < 5; ++a) tab[(a * 5 + b) * M + i] = pre[a];
-    }
+    for (int j = 0; j < 9; ++j) tab[j * M + i] = C[j / 3][j % 3];
+    tab[9 * M + i] = ikak;
   }
 }
 

@@ -40,9 +40,8 @@ namespace fft {
 // kEl != 0 selects a batched tile family: about kEl complex values per buffer
 // (512, 1024 or 2048, at most the long tile), chosen by the batch's options or
 // its autotuner.  A tile only groups lines: every line goes through the same
-// arithmetic whatever the family (FP64 results are the same bit for bit; the
-// FP32 kernels of different families are compiled separately and their last
-// bits can differ).
+// arithmetic whatever the family, and the line transforms spell out their
+// fused multiply-adds, so every family gives the same bits in both precisions.
 template <typename S, class E, int kEl = 0>
 struct Tiles {
   static constexpr bool kF32 = sizeof(S) == 4;
@@ -298,9 +297,10 @@ __device__ __forceinline__ void pass_y_body(const typename CX<S>::T* __restrict_
 // In place on B[c][kz][ky][x], lines f = kz ny + ky of all ncomp components:
 // MODE 0 forward, 1 inverse, 2 forward + Green operator computed per wave
 // vector + inverse, 3 forward + Green operator read from a stored table +
-// inverse.  The table (gtab, MODE 3) holds the 5x5 operator of every wave
-// vector of the half spectrum, entry (a, b) of wave vector (f, x) at
-// gtab[(a 5 + b) nh ny nx + f nx + x] (consecutive x contiguous: coalesced).
+// inverse.  The table (gtab, MODE 3) holds the kGreenStored values of every
+// wave vector of the half spectrum, value j of wave vector (f, x) at
+// gtab[j nh ny nx + f nx + x] (consecutive x contiguous: coalesced); MODE 2
+// and MODE 3 perform the same operations on the same values.
 template <int MODE, typename S, class E, class TL>
 __device__ __forceinline__ void pass_x_body(typename CX<S>::T* __restrict__ B, const LinePlan& pl,
                                             const FastDiv& dny,
@@ -360,7 +360,8 @@ __device__ __forceinline__ void pass_x_body(typename CX<S>::T* __restrict__ B, c
     for (int i = threadIdx.x; i < TK * nx; i += blockDim.x) {
       const int kl = E::div_n(i, pl), xx = i - kl * nx;
       if (kl >= nfk) continue;
-      const long long at = (long long)(f0 + kl) * nx + xx;
+      const int f = f0 + kl;
+      const int kz = (int)fast_div((uint32_t)f, dny);
       S pre[5], pim[5];
 #pragma unroll
       for (int c = 0; c < 5; ++c) {
@@ -368,17 +369,9 @@ __device__ __forceinline__ void pass_x_body(typename CX<S>::T* __restrict__ B, c
         pre[c] = z.x;
         pim[c] = z.y;
       }
+      green_apply_stored<S>(gp, xx, f - kz * ny, kz, gtab, M, (long long)f * nx + xx, pre, pim);
 #pragma unroll
-      for (int a = 0; a < 5; ++a) {
-        S ar = S(0), ai = S(0);
-#pragma unroll
-        for (int b = 0; b < 5; ++b) {
-          const S gab = gtab[(a * 5 + b) * M + at];
-          ar = fmad(gab, pre[b], ar);
-          ai = fmad(gab, pim[b], ai);
-        }
-        r[(a * TK + kl) * ls + sw(xx)] = T{ar, ai};
-      }
+      for (int c = 0; c < 5; ++c) r[(c * TK + kl) * ls + sw(xx)] = T{pre[c], pim[c]};
     }
     __syncthreads();
   }

@@ -6,9 +6,9 @@
 // Each persistent block walks its tiles (the same lines per tile as the
 // warp-copy pass); per tile:
 //   * a 3D tiled TMA load brings the tile's input box into shared memory,
-//     completing on an mbarrier; the load of the block's next tile is issued
-//     before the current one is transformed, into the other of two input
-//     buffers, so HBM reads overlap the FFT;
+//     completing on an mbarrier; the loads of the block's next kTmaStages - 1
+//     tiles are in flight while the current one is transformed (a ring of
+//     kTmaStages input buffers), so HBM reads overlap the FFT;
 //   * the line FFT reads the staged box in its first stage (rows, columns, or
 //     pairs of real rows packed as complex lines; the same fixed engine and
 //     arithmetic as the warp-copy pass, so results are the same bit for bit);
@@ -35,6 +35,10 @@ namespace fft {
 namespace {
 
 constexpr int kTmaThreads = 256;
+#ifndef VPFFT_TMA_STAGES
+#define VPFFT_TMA_STAGES 3
+#endif
+constexpr int kTmaStages = VPFFT_TMA_STAGES;  // input buffers per block (loads in flight: kTmaStages - 1)
 std::atomic<int> g_tma_enabled{1};
 constexpr long long kWaitPolls = 1ll << 26;
 
@@ -246,9 +250,9 @@ struct ZC2R {
 template <class P>
 constexpr size_t pass_smem() {
   constexpr int N = P::N_;
-  return 2 * (size_t)round128(P::kInBytes) + (size_t)round128(P::kOutBytes) +
-         sizeof(float2) * (2 * (size_t)P::kLines * line_stride(N) + N) + 2 * sizeof(uint64_t) +
-         128;
+  return kTmaStages * (size_t)round128(P::kInBytes) + (size_t)round128(P::kOutBytes) +
+         sizeof(float2) * (2 * (size_t)P::kLines * line_stride(N) + N) +
+         kTmaStages * sizeof(uint64_t) + 128;
 }
 
 template <class P>
@@ -257,15 +261,16 @@ __global__ void __launch_bounds__(kTmaThreads)
                const __grid_constant__ CUtensorMap out_map, const float2* __restrict__ twg,
                const PassDims d, IterCtrl* ctrl) {
   constexpr int N = P::N_;
+  constexpr int S = kTmaStages;
+  constexpr int kInStride = round128(P::kInBytes);
   using E = FixedEngine<N>;
   constexpr int LS = line_stride(N);
   if (ctrl && ctrl->done) return;
   extern __shared__ __align__(128) unsigned char tsm_raw[];
   // TMA boxes start on a 128-byte boundary (the size has 128 bytes of slack)
   unsigned char* const tsm = tsm_raw + ((128u - (smem_u32(tsm_raw) & 127u)) & 127u);
-  unsigned char* const in0 = tsm;
-  unsigned char* const in1 = in0 + round128(P::kInBytes);
-  unsigned char* const stg = in1 + round128(P::kInBytes);
+  unsigned char* const in0 = tsm;  // S input buffers of kInStride bytes
+  unsigned char* const stg = in0 + S * kInStride;
   float2* const a = reinterpret_cast<float2*>(stg + round128(P::kOutBytes));
   float2* const b = a + P::kLines * LS;
   float2* const tw = b + P::kLines * LS;
@@ -273,36 +278,36 @@ __global__ void __launch_bounds__(kTmaThreads)
   const int tiles = P::tiles(d);
   E::load_tw(tw, twg, N, threadIdx.x, blockDim.x);
   if (threadIdx.x == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+#pragma unroll
+    for (int j = 0; j < S; ++j) mbar_init(&bar[j], 1);
     mbar_init_fence();
   }
   __syncthreads();
-  // loads issued and waited for per buffer: the m-th use of a buffer's
-  // mbarrier completes phase m, waited for with parity m & 1
-  int issued0 = 0, issued1 = 0, waited0 = 0, waited1 = 0;
-  auto issue = [&](int t, int i) {
+  auto issue = [&](int t, int buf) {
     const TileBoxes bx = P::box(d, t);
-    mbar_expect_tx(&bar[i], (uint32_t)P::kInBytes);
-    tma_load_3d(i ? in1 : in0, &in_map, &bar[i], bx.in[0], bx.in[1], bx.in[2]);
-    if (i) ++issued1; else ++issued0;
+    mbar_expect_tx(&bar[buf], (uint32_t)P::kInBytes);
+    tma_load_3d(in0 + buf * kInStride, &in_map, &bar[buf], bx.in[0], bx.in[1], bx.in[2]);
   };
-  if (threadIdx.x == 0 && (int)blockIdx.x < tiles) issue(blockIdx.x, 0);
+  // The block's k-th tile goes to buffer k mod S as that buffer's (k div S)-th
+  // load, completing phase k div S of its mbarrier (waited for with parity
+  // (k div S) & 1).  Tiles 0 .. S-2 are issued up front; each step issues
+  // tile k+S-1 into the buffer of tile k-1, whose contents the first FFT
+  // stage of tile k-1 read behind that tile's barriers.
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int j = 0; j < S - 1; ++j)
+      if ((int)blockIdx.x + j * (int)gridDim.x < tiles) issue(blockIdx.x + j * gridDim.x, j);
   bool failed = false;
-  int k = 0;
+  int k = 0, buf = 0, use = 0;  // buf = k mod S, use = k div S
   for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++k) {
-    const int i = k & 1;
-    // the next tile into the other buffer: its previous contents (tile k-1)
-    // were read by the first FFT stage, behind the barriers of that tile
-    if (threadIdx.x == 0 && t + (int)gridDim.x < tiles) issue(t + gridDim.x, i ^ 1);
-    const int use = k >> 1;  // this tile is use `use` of buffer i
-    const bool ok = mbar_wait(&bar[i], (uint32_t)(use & 1));
+    if (threadIdx.x == 0 && t + (S - 1) * (int)gridDim.x < tiles)
+      issue(t + (S - 1) * gridDim.x, buf == 0 ? S - 1 : buf - 1);
+    const bool ok = mbar_wait(&bar[buf], (uint32_t)(use & 1));
     if (__syncthreads_or(!ok)) {
       failed = true;
       break;
     }
-    if (i) waited1 = use + 1; else waited0 = use + 1;
-    const void* src = i ? in1 : in0;
+    const void* src = in0 + buf * kInStride;
     const float2* r = E::template fft_loaded<P::kSign, P::kLineFastest>(
         [&](int l, int e) { return P::load(src, l, e); }, a, b, tw, P::kLines, LS, threadIdx.x,
         blockDim.x);
@@ -317,14 +322,25 @@ __global__ void __launch_bounds__(kTmaThreads)
       tma_store_3d(&out_map, stg, bx.out[0], bx.out[1], bx.out[2]);
       bulk_commit();
     }
+    if (++buf == S) {
+      buf = 0;
+      ++use;
+    }
   }
   if (threadIdx.x == 0) {
     bulk_wait_all();
     if (failed) {
-      // loads still in flight land in this block's shared memory: wait for
-      // them (bounded) before the block exits, then report
-      if (issued0 > waited0) mbar_wait(&bar[0], (uint32_t)(waited0 & 1));
-      if (issued1 > waited1) mbar_wait(&bar[1], (uint32_t)(waited1 & 1));
+      // the loads still in flight (tiles k .. k+S-1 of this block, those that
+      // exist) land in this block's shared memory: wait for them (bounded)
+      // before the block exits, then report
+      for (int j = 0; j < S; ++j) {
+        if ((long long)blockIdx.x + (long long)(k + j) * gridDim.x < tiles)
+          mbar_wait(&bar[buf], (uint32_t)(use & 1));
+        if (++buf == S) {
+          buf = 0;
+          ++use;
+        }
+      }
       if (ctrl) atomicOr(&ctrl->status, (int)kStatusDeviceTimeout);
     }
   }
