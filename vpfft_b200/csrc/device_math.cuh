@@ -792,18 +792,146 @@ __device__ __forceinline__ void green_finish(const GreenParams<R>& gp, const Gre
 }
 
 // dh[c] (in: phat, out: dhat) for wave-vector indices (ix, iy, iz) of the full grid.
+// The geometry, green_core and green_finish written out in one body (the
+// compiler schedules this form better: 72 instead of 80 registers in the
+// 256-point x pass, and a faster pass); every value is formed by the same
+// operations as in those parts, so the stored-table path gives the same bits.
 template <typename R>
 __device__ __forceinline__ void green_apply(const GreenParams<R>& gp, int ix, int iy, int iz,
                                             R pre[5], R pim[5]) {
-  GreenPoint<R> q;
-  if (!green_geometry(gp, ix, iy, iz, q)) {
+  if (ix == 0 && iy == 0 && iz == 0) {
 #pragma unroll
     for (int c = 0; c < 5; ++c) pre[c] = pim[c] = R(0);
     return;
   }
-  R C[3][3], ikak = R(0);
-  if (q.wg != R(0)) green_core(gp, q, C, ikak);
-  green_finish(gp, q, C, ikak, pre, pim);
+  // index of -k (indices are in [0, n))
+  const int mx = ix ? gp.nx - ix : 0, my = iy ? gp.ny - iy : 0, mz = iz ? gp.nz - iz : 0;
+  const bool ovk = nyq_override(ix, gp.nx) || nyq_override(iy, gp.ny) || nyq_override(iz, gp.nz);
+  const bool ovm = nyq_override(mx, gp.nx) || nyq_override(my, gp.ny) || nyq_override(mz, gp.nz);
+  const R wg = R(0.5) * R((ovk ? 0 : 1) + (ovm ? 0 : 1));  // weight of Gamma
+  const R wl = R(0.5) * R((ovk ? 1 : 0) + (ovm ? 1 : 0));  // weight of inverse(-L0)
+  R dre[5] = {0, 0, 0, 0, 0}, dim[5] = {0, 0, 0, 0, 0};
+  if (wg != R(0)) {
+    R k0 = R(ix > gp.nx / 2 ? ix - gp.nx : ix) * gp.inv_len[0];
+    R k1 = R(iy > gp.ny / 2 ? iy - gp.ny : iy) * gp.inv_len[1];
+    R k2 = R(iz > gp.nz / 2 ? iz - gp.nz : iz) * gp.inv_len[2];
+    R il;
+    const R kk = fmad(k2, k2, fmad(k1, k1, k0 * k0));
+    if constexpr (sizeof(R) == 4)
+      il = rsqrtf(kk);
+    else
+      il = R(1) / sqrt(kk);
+    k0 *= il;
+    k1 *= il;
+    k2 *= il;
+    const R is2 = R(0.70710678118654752440), is6 = R(0.40824829046386301637);
+    // columns v_a = B_a k
+    R V[3][5];
+    V[0][0] = -k0 * is2; V[1][0] = k1 * is2;  V[2][0] = R(0);
+    V[0][1] = -k0 * is6; V[1][1] = -k1 * is6; V[2][1] = R(2) * k2 * is6;
+    V[0][2] = R(0);      V[1][2] = k2 * is2;  V[2][2] = k1 * is2;
+    V[0][3] = k2 * is2;  V[1][3] = R(0);      V[2][3] = k0 * is2;
+    V[0][4] = k1 * is2;  V[1][4] = k0 * is2;  V[2][4] = R(0);
+    // A = V L0 V^T.  The four structural zeros of V (vz) are skipped: adding
+    // 0 * x to a sum leaves it unchanged for finite x, so the results are the
+    // same as with the full products.
+    auto vz = [](int i, int a) {
+      return (i == 0 && a == 2) || (i == 1 && a == 3) || (i == 2 && (a == 0 || a == 4));
+    };
+    R VL[3][5];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int b = 0; b < 5; ++b) {
+        R acc = R(0);
+#pragma unroll
+        for (int a = 0; a < 5; ++a)
+          if (!vz(i, a)) acc = fmad(V[i][a], gp.L0[b * 5 + a], acc);
+        VL[i][b] = acc;
+      }
+    R A[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        R acc = R(0);
+#pragma unroll
+        for (int b = 0; b < 5; ++b)
+          if (!vz(k, b)) acc = fmad(VL[i][b], V[k][b], acc);
+        A[i][k] = acc;
+      }
+    // A^-1 by the adjugate; x*y - z*w as fmad(x, y, -(z*w))
+    auto det2 = [](R x, R y, R z, R w) { return fmad(x, y, -(z * w)); };
+    R C[3][3];
+    C[0][0] = det2(A[1][1], A[2][2], A[1][2], A[2][1]);
+    C[0][1] = det2(A[0][2], A[2][1], A[0][1], A[2][2]);
+    C[0][2] = det2(A[0][1], A[1][2], A[0][2], A[1][1]);
+    C[1][0] = det2(A[1][2], A[2][0], A[1][0], A[2][2]);
+    C[1][1] = det2(A[0][0], A[2][2], A[0][2], A[2][0]);
+    C[1][2] = det2(A[0][2], A[1][0], A[0][0], A[1][2]);
+    C[2][0] = det2(A[1][0], A[2][1], A[1][1], A[2][0]);
+    C[2][1] = det2(A[0][1], A[2][0], A[0][0], A[2][1]);
+    C[2][2] = det2(A[0][0], A[1][1], A[0][1], A[1][0]);
+    const R idet =
+        R(1) / fmad(A[0][2], C[2][0], fmad(A[0][1], C[1][0], A[0][0] * C[0][0]));
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) C[i][k] *= idet;
+    const R kv[3] = {k0, k1, k2};
+    R u[3], w[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      u[i] = fmad(C[i][2], kv[2], fmad(C[i][1], kv[1], C[i][0] * kv[0]));
+      w[i] = fmad(kv[2], C[2][i], fmad(kv[1], C[1][i], kv[0] * C[0][i]));
+    }
+    const R ikak = R(1) / fmad(kv[2], u[2], fmad(kv[1], u[1], kv[0] * u[0]));
+    // q = V phat (3 complex), t = Bk q = A^-1 q - u (w.q)/(k.A^-1 k)
+    R qr[3], qi[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      R ar = R(0), ai = R(0);
+#pragma unroll
+      for (int b = 0; b < 5; ++b) {
+        if (vz(i, b)) continue;
+        ar = fmad(V[i][b], pre[b], ar);
+        ai = fmad(V[i][b], pim[b], ai);
+      }
+      qr[i] = ar;
+      qi[i] = ai;
+    }
+    const R wqr = fmad(w[2], qr[2], fmad(w[1], qr[1], w[0] * qr[0])) * ikak;
+    const R wqi = fmad(w[2], qi[2], fmad(w[1], qi[1], w[0] * qi[0])) * ikak;
+    R tr[3], ti[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      tr[i] = fmad(-u[i], wqr, fmad(C[i][2], qr[2], fmad(C[i][1], qr[1], C[i][0] * qr[0])));
+      ti[i] = fmad(-u[i], wqi, fmad(C[i][2], qi[2], fmad(C[i][1], qi[1], C[i][0] * qi[0])));
+    }
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+      dre[a] = wg * fmad(V[2][a], tr[2], fmad(V[1][a], tr[1], V[0][a] * tr[0]));
+      dim[a] = wg * fmad(V[2][a], ti[2], fmad(V[1][a], ti[1], V[0][a] * ti[0]));
+    }
+  }
+  if (wl != R(0)) {
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+      R ar = R(0), ai = R(0);
+#pragma unroll
+      for (int b = 0; b < 5; ++b) {
+        ar = fmad(gp.Linv[b * 5 + a], pre[b], ar);
+        ai = fmad(gp.Linv[b * 5 + a], pim[b], ai);
+      }
+      dre[a] = fmad(-wl, ar, dre[a]);
+      dim[a] = fmad(-wl, ai, dim[a]);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 5; ++c) {
+    pre[c] = dre[c];
+    pim[c] = dim[c];
+  }
 }
 
 // The same with C and ikak read from a stored table: value j of the wave
