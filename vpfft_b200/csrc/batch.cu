@@ -114,6 +114,12 @@ struct HostList {
   }
   int m() const { return (int)slot.size(); }
   int blocks() const { return prefix.back(); }
+  // the common block count when every slot has the same, else 0
+  int per() const {
+    for (size_t i = 2; i < prefix.size(); ++i)
+      if (prefix[i] - prefix[i - 1] != prefix[1]) return 0;
+    return prefix.size() > 1 ? prefix[1] : 0;
+  }
 };
 
 // Device copy of a set of lists, packed into one buffer, staged through a
@@ -225,6 +231,7 @@ vpfft_status upload_lists(vpfft_batch* b, DeviceLists& dl, const std::vector<Hos
     pos += l->prefix.size();
     bl.m = l->m();
     bl.blocks = l->blocks();
+    bl.per = l->per();
     out.push_back(bl);
   }
   if (pos)

@@ -791,14 +791,43 @@ __device__ __forceinline__ void green_finish(const GreenParams<R>& gp, const Gre
   }
 }
 
+// The Green constants as green_apply reads them: from a GreenParams (a kernel
+// parameter: constant-bank operands), or through GreenShared, a view of a
+// GreenParams in shared memory read at each use, so that a batched pass keeps
+// no registers for the 50 matrix entries.
+template <typename R>
+__device__ __forceinline__ R green_l0(const GreenParams<R>& g, int i) {
+  return g.L0[i];
+}
+template <typename R>
+__device__ __forceinline__ R green_linv(const GreenParams<R>& g, int i) {
+  return g.Linv[i];
+}
+template <typename R>
+struct GreenShared {
+  const GreenParams<R>* p;
+  int nx, ny, nz;
+  R inv_len[3];
+  __device__ explicit GreenShared(const GreenParams<R>* q)
+      : p(q), nx(q->nx), ny(q->ny), nz(q->nz), inv_len{q->inv_len[0], q->inv_len[1], q->inv_len[2]} {}
+};
+template <typename R>
+__device__ __forceinline__ R green_l0(const GreenShared<R>& g, int i) {
+  return *reinterpret_cast<const volatile R*>(&g.p->L0[i]);
+}
+template <typename R>
+__device__ __forceinline__ R green_linv(const GreenShared<R>& g, int i) {
+  return *reinterpret_cast<const volatile R*>(&g.p->Linv[i]);
+}
+
 // dh[c] (in: phat, out: dhat) for wave-vector indices (ix, iy, iz) of the full grid.
 // The geometry, green_core and green_finish written out in one body (the
 // compiler schedules this form better: 72 instead of 80 registers in the
 // 256-point x pass, and a faster pass); every value is formed by the same
 // operations as in those parts, so the stored-table path gives the same bits.
-template <typename R>
-__device__ __forceinline__ void green_apply(const GreenParams<R>& gp, int ix, int iy, int iz,
-                                            R pre[5], R pim[5]) {
+template <typename R, class G>
+__device__ __forceinline__ void green_apply(const G& gp, int ix, int iy, int iz, R pre[5],
+                                            R pim[5]) {
   if (ix == 0 && iy == 0 && iz == 0) {
 #pragma unroll
     for (int c = 0; c < 5; ++c) pre[c] = pim[c] = R(0);
@@ -846,7 +875,7 @@ __device__ __forceinline__ void green_apply(const GreenParams<R>& gp, int ix, in
         R acc = R(0);
 #pragma unroll
         for (int a = 0; a < 5; ++a)
-          if (!vz(i, a)) acc = fmad(V[i][a], gp.L0[b * 5 + a], acc);
+          if (!vz(i, a)) acc = fmad(V[i][a], green_l0(gp, b * 5 + a), acc);
         VL[i][b] = acc;
       }
     R A[3][3];
@@ -920,8 +949,8 @@ __device__ __forceinline__ void green_apply(const GreenParams<R>& gp, int ix, in
       R ar = R(0), ai = R(0);
 #pragma unroll
       for (int b = 0; b < 5; ++b) {
-        ar = fmad(gp.Linv[b * 5 + a], pre[b], ar);
-        ai = fmad(gp.Linv[b * 5 + a], pim[b], ai);
+        ar = fmad(green_linv(gp, b * 5 + a), pre[b], ar);
+        ai = fmad(green_linv(gp, b * 5 + a), pim[b], ai);
       }
       dre[a] = fmad(-wl, ar, dre[a]);
       dim[a] = fmad(-wl, ai, dim[a]);

@@ -50,7 +50,9 @@ struct Tiles {
   static constexpr int kThreads = E::kN ? (kF32 ? 256 : 128) : 256;  // z and y passes
   static constexpr int kThreadsX = E::kN ? 128 : 256;                // x pass
   // x-pass blocks per SM the registers are capped for: FP32 at 6 (85
-  // registers; measured 15 % faster than 4), FP64 at 4 (more would spill)
+  // registers; measured 15 % faster than 4), FP64 at 4 (more would spill).
+  // The batched x pass reads its Green constants from shared memory at each
+  // use (GreenShared), which keeps it within the same caps without spills.
   static constexpr int kMinBlocksX = (E::kN && kF32) ? 6 : 512 / kThreadsX;
   static constexpr int cmax(int a, int b) { return a > b ? a : b; }
   static constexpr int kZ = E::kN ? cmax(2, 2 * (kElems / E::kN)) : 16;  // real z-lines
@@ -301,11 +303,11 @@ __device__ __forceinline__ void pass_y_body(const typename CX<S>::T* __restrict_
 // wave vector of the half spectrum, value j of wave vector (f, x) at
 // gtab[j nh ny nx + f nx + x] (consecutive x contiguous: coalesced); MODE 2
 // and MODE 3 perform the same operations on the same values.
-template <int MODE, typename S, class E, class TL>
+template <int MODE, typename S, class E, class TL, class G>
 __device__ __forceinline__ void pass_x_body(typename CX<S>::T* __restrict__ B, const LinePlan& pl,
                                             const FastDiv& dny,
                                             const typename CX<S>::T* __restrict__ twg,
-                                            const GreenParams<S>& gp,
+                                            const G& gp,
                                             const S* __restrict__ gtab, int ny, int nh, int ncomp,
                                             int bt) {
   using T = typename CX<S>::T;
@@ -336,7 +338,7 @@ __device__ __forceinline__ void pass_x_body(typename CX<S>::T* __restrict__ B, c
     r = E::template fft<-1>(a, b, tw, pl, nl, ls, threadIdx.x, blockDim.x);
     o = (r == a) ? b : a;
   }
-  if (MODE == 2) {
+  if constexpr (MODE == 2) {
     for (int i = threadIdx.x; i < TK * nx; i += blockDim.x) {
       const int kl = E::div_n(i, pl), xx = i - kl * nx;
       if (kl >= nfk) continue;
@@ -355,7 +357,7 @@ __device__ __forceinline__ void pass_x_body(typename CX<S>::T* __restrict__ B, c
     }
     __syncthreads();
   }
-  if (MODE == 3) {
+  if constexpr (MODE == 3) {
     const long long M = (long long)nh * ny * nx;
     for (int i = threadIdx.x; i < TK * nx; i += blockDim.x) {
       const int kl = E::div_n(i, pl), xx = i - kl * nx;
@@ -491,7 +493,7 @@ __global__ void __launch_bounds__(Tiles<S, E, kEl>::kThreads)
                               fs.nx, fs.nh, lb - c * gt, c);
 }
 template <typename S, class E, int kEl>
-__global__ void __launch_bounds__(Tiles<S, E, kEl>::kThreadsX, 512 / Tiles<S, E, kEl>::kThreadsX)
+__global__ void __launch_bounds__(Tiles<S, E, kEl>::kThreadsX, Tiles<S, E, kEl>::kMinBlocksX)
     k_pass_x_batch(const SlotDesc<S>* __restrict__ desc, const BatchLaunch bl) {
   using T = typename CX<S>::T;
   using TL = Tiles<S, E, kEl>;
@@ -501,8 +503,8 @@ __global__ void __launch_bounds__(Tiles<S, E, kEl>::kThreadsX, 512 / Tiles<S, E,
   if (!d) return;
   const FftSlot<S>& fs = sm.fs;
   pass_x_body<2, S, E, TL>(reinterpret_cast<T*>(fs.X2), d->sp.px, fs.dny,
-                           reinterpret_cast<const T*>(fs.twx), sm.gp, nullptr, fs.ny, fs.nh, 5,
-                           lb);
+                           reinterpret_cast<const T*>(fs.twx), GreenShared<S>(&sm.gp), nullptr,
+                           fs.ny, fs.nh, 5, lb);
 }
 
 // ---------------------------------------------------------------- entry table

@@ -70,6 +70,11 @@ __device__ __forceinline__ void store5(S* __restrict__ f, long long n, long long
 
 // Slot of block b of a batched launch and the block's index within the slot.
 __device__ __forceinline__ int batch_slot(const BatchLaunch& bl, int b, int* local) {
+  if (bl.per > 0) {  // equal counts (the passes of a size class): no search
+    const int k = b / bl.per;
+    *local = b - k * bl.per;
+    return bl.slot[k];
+  }
   int lo = 0, hi = bl.m - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;

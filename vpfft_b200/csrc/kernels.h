@@ -220,6 +220,7 @@ struct BatchLaunch {
   const int* prefix;
   int m;
   int blocks;
+  int per;  // blocks of every slot when all slots have the same count, else 0
 };
 // Dispatch value of the compile-time rate exponent (10, 20, or 0 = generic).
 int uniform_exponent(const NRParams& p);
