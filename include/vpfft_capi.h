@@ -101,6 +101,13 @@ typedef struct {
                                  (vpfft_grid_green_operator); 1 = always compute; 2 = always
                                  store (rebuilt at each fixed-point loop, since L0 and the voxel
                                  lengths change per increment).  All three give the same bits. */
+  double mixed_certify_step;  /* VPFFT_PREC_MIXED only (no counterpart in the reference): after
+                                 the FP32 Newton predictor, the FP64 residual at the predicted
+                                 stress gives an estimate of the Newton step still to take; where
+                                 it is at most this fraction of |sigma| the predicted stress is
+                                 kept with its FP64 strain rate, elsewhere the FP64 Newton step
+                                 (FP64 residual and Jacobian) is taken.  Default 1e-5; 0 always
+                                 takes the step. */
 } vpfft_solver_options;
 
 typedef struct {
@@ -116,6 +123,9 @@ typedef struct {
   double seconds_loop;        /* the fixed-point loop */
   double seconds_post;        /* texture, voxel length, hardening */
   double L0[25];              /* reference medium of the increment, column-major */
+  int64_t nr_fp64_steps;      /* mixed precision: voxel-iterations that took the FP64 Newton
+                                 step (the others kept the FP32 predictor's stress, certified by
+                                 the FP64 residual; vpfft_solver_options.mixed_certify_step) */
 } vpfft_stats;
 
 typedef enum {

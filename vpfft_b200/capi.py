@@ -82,6 +82,7 @@ class SolverOptions(C.Structure):
         ("nr_max_resolved", C.c_double),
         ("nr_max_iter", C.c_int32),
         ("green_operator", C.c_int32),
+        ("mixed_certify_step", C.c_double),
     ]
 
 
@@ -99,6 +100,7 @@ class Stats(C.Structure):
         ("seconds_loop", C.c_double),
         ("seconds_post", C.c_double),
         ("L0", C.c_double * 25),
+        ("nr_fp64_steps", C.c_int64),
     ]
 
 
@@ -325,12 +327,18 @@ def material(gamma_dot_base=15.5, rate_sensitivity=10, crss=11.0, tau0=11.0, tau
     return m
 
 
-def solver_options(green_operator: int = 0) -> SolverOptions:
+def solver_options(green_operator: int = 0, mixed_certify_step: float | None = None
+                   ) -> SolverOptions:
     """The default solver constants (the reference's, vpfft_solver_options_default)
-    with the x pass's Green operator: 0 chosen per grid size, 1 computed, 2 stored."""
+    with the x pass's Green operator (0 chosen per grid size, 1 computed, 2 stored)
+    and, for mixed precision, the bound below which the FP64 residual certifies
+    the FP32 predictor's stress (None: the default, 1e-5; 0: the FP64 Newton step
+    is always taken)."""
     o = SolverOptions()
     load().vpfft_solver_options_default(C.byref(o))
     o.green_operator = int(green_operator)
+    if mixed_certify_step is not None:
+        o.mixed_certify_step = float(mixed_certify_step)
     return o
 
 

@@ -858,7 +858,8 @@ vpfft_status vpfft_batch_submit(vpfft_batch* b, vpfft_grid* g, const double edot
   const bool same_opt = go.init_nr_epsilon == bo.init_nr_epsilon &&
                         go.init_nr_max_iter == bo.init_nr_max_iter &&
                         go.nr_epsilon == bo.nr_epsilon && go.nr_max_resolved == bo.nr_max_resolved &&
-                        go.nr_max_iter == bo.nr_max_iter;
+                        go.nr_max_iter == bo.nr_max_iter &&
+                        go.mixed_certify_step == bo.mixed_certify_step;
   if (std::memcmp(&g->mat, &b->mat, sizeof(vpfft_material)) != 0 || !same_opt)
     return bfail(b, VPFFT_ERR_INVALID_ARGUMENT, "grid material or solver options differ from the batch's");
   if (!g->fields_set) return bfail(b, VPFFT_ERR_NOT_INITIALIZED, "grid fields not set");

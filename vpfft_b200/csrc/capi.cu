@@ -198,6 +198,7 @@ NRParams nr_params(const vpfft_grid* g, const double edot[5], bool init) {
     p.max_iter = g->opt.nr_max_iter;
   }
   set_fp32_copies(p);
+  p.cert2_f = (float)(g->opt.mixed_certify_step * g->opt.mixed_certify_step);
   return p;
 }
 
@@ -596,6 +597,7 @@ vpfft_status do_fixed_point(vpfft_grid* g, const double edot[5], int max_iter, d
     st->converged = (c.last[10] <= eps && c.last[11] <= eps) ? 1 : 0;
     for (int k = 0; k < 5; ++k) st->avg_strain_rate[k] = c.last[5 + k];
     st->nr_not_converged = (int64_t)c.nr_capped;
+    st->nr_fp64_steps = (int64_t)c.nr_fp64;
     st->status_bits = c.status | (st->converged ? 0 : VPFFT_STATUS_LOOP_NOT_CONVERGED) |
                       (c.nr_capped ? VPFFT_STATUS_NR_CAPPED : 0);
     std::memcpy(st->L0, g->L0, sizeof(g->L0));
@@ -710,6 +712,7 @@ void vpfft_solver_options_default(vpfft_solver_options* o) {
   o->nr_max_resolved = 1e9;   // 910
   o->nr_max_iter = 100;       // 911
   o->green_operator = 0;      // chosen per grid size
+  o->mixed_certify_step = 1e-5;
 }
 
 vpfft_status vpfft_grid_create(int nx, int ny, int nz, const vpfft_material* material,
@@ -729,6 +732,8 @@ vpfft_status vpfft_grid_create(int nx, int ny, int nz, const vpfft_material* mat
   }
   if (options && (options->green_operator < 0 || options->green_operator > 2))
     return fail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "green_operator must be 0, 1 or 2");
+  if (options && !(options->mixed_certify_step >= 0.0 && options->mixed_certify_step <= 1e-2))
+    return fail(nullptr, VPFFT_ERR_INVALID_ARGUMENT, "mixed_certify_step must be in [0, 1e-2]");
   vpfft_status s = need_device(nullptr);
   if (s != VPFFT_OK) return s;
   vpfft_grid* g = new vpfft_grid();

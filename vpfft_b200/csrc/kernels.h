@@ -50,6 +50,7 @@ struct IterCtrl {
   double n_voxels;    // N as double
   unsigned long long nr_capped;
   double last[12];    // <sigma>(5), <edot>(5), delta_sigma, delta_eps of the last iteration
+  unsigned long long nr_fp64;  // mixed precision: voxel-iterations that took the FP64 step
 };
 // device-side bits of IterCtrl::status; the same values as VPFFT_STATUS_MAX_RSS_TINY,
 // VPFFT_STATUS_NONFINITE and VPFFT_STATUS_DEVICE_TIMEOUT of the C ABI

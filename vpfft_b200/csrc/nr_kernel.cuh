@@ -88,7 +88,10 @@ struct NRParams {
   float eps_f;
   float max_rss_f;
   float L0inv_f[15];
-  float pad_f_;
+  // mixed precision: the FP64 Newton step is skipped where the step estimated
+  // from the FP64 residual at the predicted stress, squared, is at most
+  // cert2_f |sigma|^2 (0: the step is always taken)
+  float cert2_f;
 };
 
 // Fills the FP32 copies of the per-system constants from the FP64 values.
@@ -203,43 +206,61 @@ __device__ __forceinline__ bool small_step_f32(float dn, float an, float eps, bo
   return dn < eps * eps * an;
 }
 
-// LDL^T solve of a symmetric positive-definite 5x5 A (packed upper) x = b.
-// Returns false when a pivot is not positive (A not numerically SPD).
+// LDL^T factorisation of a symmetric positive-definite 5x5 A (packed upper):
+// the strict lower part of L and the reciprocal pivots.  Returns false when a
+// pivot is not positive (A not numerically SPD).
 template <typename T>
-__device__ __forceinline__ bool ldlt5_solve(const T A[15], const T b[5], T x[5]) {
-  T L[5][5], d[5], id[5];
+struct Ldl5 {
+  T L[5][5];  // L[i][j], i > j
+  T id[5];    // 1 / d[j]
+};
+template <typename T>
+__device__ __forceinline__ bool ldlt5_factor(const T A[15], Ldl5<T>& f) {
+  T d[5];
   bool ok = true;
 #pragma unroll
   for (int j = 0; j < 5; ++j) {
     T dj = A[sym5(j, j)];
 #pragma unroll
-    for (int k = 0; k < j; ++k) dj -= L[j][k] * L[j][k] * d[k];
+    for (int k = 0; k < j; ++k) dj -= f.L[j][k] * f.L[j][k] * d[k];
     ok = ok && (dj > T(0));
     d[j] = dj;
-    id[j] = recip(dj);
+    f.id[j] = recip(dj);
 #pragma unroll
     for (int i = j + 1; i < 5; ++i) {
       T a = A[sym5(j, i)];
 #pragma unroll
-      for (int k = 0; k < j; ++k) a -= L[i][k] * L[j][k] * d[k];
-      L[i][j] = a * id[j];
+      for (int k = 0; k < j; ++k) a -= f.L[i][k] * f.L[j][k] * d[k];
+      f.L[i][j] = a * f.id[j];
     }
   }
+  return ok;
+}
+// x = A^-1 b from the factors of A.
+template <typename T>
+__device__ __forceinline__ void ldlt5_subst(const Ldl5<T>& f, const T b[5], T x[5]) {
   T z[5];
 #pragma unroll
   for (int i = 0; i < 5; ++i) {
     T a = b[i];
 #pragma unroll
-    for (int k = 0; k < i; ++k) a -= L[i][k] * z[k];
+    for (int k = 0; k < i; ++k) a -= f.L[i][k] * z[k];
     z[i] = a;
   }
 #pragma unroll
   for (int i = 4; i >= 0; --i) {
-    T a = z[i] * id[i];
+    T a = z[i] * f.id[i];
 #pragma unroll
-    for (int k = i + 1; k < 5; ++k) a -= L[k][i] * x[k];
+    for (int k = i + 1; k < 5; ++k) a -= f.L[k][i] * x[k];
     x[i] = a;
   }
+}
+// LDL^T solve of A x = b; false when A is not numerically SPD.
+template <typename T>
+__device__ __forceinline__ bool ldlt5_solve(const T A[15], const T b[5], T x[5]) {
+  Ldl5<T> f;
+  const bool ok = ldlt5_factor(A, f);
+  ldlt5_subst(f, b, x);
   return ok;
 }
 
@@ -390,18 +411,15 @@ __device__ __forceinline__ bool accumulate_pairs(const float* msm, const float* 
 // true and the iterate in s_io when it converged with finite values; the
 // caller then takes the accepted step with FP64 residual and Jacobian.
 // *rmax0 gets max_s |r_s| at the starting point.
+// fac (optional): the LDL^T factors of the converged step's Newton matrix.
 template <int NEXP, bool kTauSmem, bool kFull = true, typename MS, class C>
+// l32, e32: lambda and Edot + d~ rounded to FP32; cur: the starting stress in,
+// the converged iterate out (undefined when the predictor fails).
 __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, int bs,
                                                 const NRParams& p, const C& cs,
-                                                const double lam[5], const double ed[5],
-                                                double s_io[5], int max_steps, float* rmax0) {
-  float cur[5], l32[5], e32[5];
-#pragma unroll
-  for (int c = 0; c < 5; ++c) {
-    cur[c] = (float)s_io[c];
-    l32[c] = (float)lam[c];
-    e32[c] = (float)ed[c];
-  }
+                                                const float l32[5], const float e32[5],
+                                                float cur[5], int max_steps, float* rmax0,
+                                                Ldl5<float>* fac = nullptr) {
   *rmax0 = 0.f;
   for (int it = 0; it < max_steps; ++it) {
     float S[5], K[15], rm;
@@ -423,7 +441,9 @@ __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, in
 #pragma unroll
     for (int k = 0; k < 15; ++k) K[k] += cs.L0inv_f(k);
     float delta[5];
-    if (!ldlt5_solve(K, y, delta)) return false;
+    Ldl5<float> f;
+    if (!ldlt5_factor(K, f)) return false;
+    ldlt5_subst(f, y, delta);
     float dn = 0.f, an = 0.f;
 #pragma unroll
     for (int c = 0; c < 5; ++c) {
@@ -437,12 +457,37 @@ __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, in
     const bool small = small_step_f32(dn, an, p.eps_f, &bad);
     if (bad) return false;
     if (small) {
-#pragma unroll
-      for (int c = 0; c < 5; ++c) s_io[c] = (double)cur[c];
+      if (fac) *fac = f;
       return true;
     }
   }
   return false;
+}
+
+// The strain rate S(s) = sum_s m_s gdot_s |r_s|^(n-1) r_s in FP64 and the
+// admissibility of s (every |r_s| within the cap): the FP64 residual pass of
+// the mixed path, the S half of `accumulate` for the constrained solver.
+template <int NEXP, bool kTauSmem, typename MS>
+__device__ __forceinline__ bool strain_rate_fp64(const MS* msm, const MS* tsm, int bs,
+                                                 const NRParams& p, const double s[5],
+                                                 double S[5]) {
+  bool adm = true;
+#pragma unroll
+  for (int c = 0; c < 5; ++c) S[c] = 0.0;
+#pragma unroll 2
+  for (int q = 0; q < kNS; ++q) {
+    double m[5];
+    load_m(msm, bs, q, m);
+    const double it = itau_of<kTauSmem>(tsm, bs, p, q);
+    const double r = (m[0] * s[0] + m[1] * s[1] + m[2] * s[2] + m[3] * s[3] + m[4] * s[4]) * it;
+    adm = adm && !(fabs(r) > p.max_rss);
+    const int n = p.nexp[q];
+    const double g = n != 1 ? p.gdot[q] * pow_nm1<NEXP>(fabs(r), n) : p.gdot[q];
+    const double gr = g * r;
+#pragma unroll
+    for (int i = 0; i < 5; ++i) S[i] += m[i] * gr;
+  }
+  return adm;
 }
 
 // SolveConstrainedConstitutiveEquations (Solvers.cpp:111-222).  ed = Edot + d~.

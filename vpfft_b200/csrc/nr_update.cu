@@ -32,9 +32,9 @@ constexpr int nr_batch_min_blocks() {
   return 3;
 }
 // The fixed-point NR sweep: three blocks per SM for the single grid (168
-// registers, no spills; measured 2.4 % faster at 256^3 mixed than four blocks
-// with spills), four for the batched FP32 sweep (measured 3 % faster than
-// three there).
+// registers, no spills; measured 3 % faster at 256^3 mixed than four blocks
+// of 128 registers, which spill), four for the batched FP32 sweep (measured
+// 3 % faster than three there).
 template <typename MS>
 constexpr int nr_loop_min_blocks() {
   return 3;
@@ -125,7 +125,48 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_batch_min_blocks<MS>())
   init_body<S, MS, NEXP, kTauSmem>(sp, sf, d.ctrl, lb, d.init_blocks, msm, tsm);
 }
 
-// The per-voxel body of the fixed-point loop (MaterialGrid.cpp:946-1003):
+// The end of a voxel's update in the fixed-point loop (MaterialGrid.cpp:982-1003):
+//   P = sigma - L0 d~;  lambda += L0 (Edot + d~ - edot);
+// stores sigma, lambda and P (into `work`) and adds the voxel's terms to the
+// block sums acc: sigma (5), edot (5), |sigma - lambda|, |edot - Edot - d~|
+// (lambda already updated).  ed = Edot + d~.  The sums live at acc[k * kStride]
+// (registers for kStride 1, the thread's column of a shared-memory array else).
+template <int kStride = 1, typename S, class C>
+__device__ __forceinline__ void finish_voxel(const C& cs, long long n, const FieldPtrs<S>& f,
+                                             long long v, const double s[5], const double e[5],
+                                             double lam[5], const double d[5],
+                                             const double ed[5], double* acc) {
+  double P[5];
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    double ld = 0.0, lt = 0.0;
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      const double l0 = cs.L0(j * 5 + i);
+      ld += l0 * d[j];
+      lt += l0 * (ed[j] - e[j]);
+    }
+    P[i] = s[i] - ld;
+    lam[i] += lt;
+  }
+  store5(f.sigma, n, v, s);
+  store5(f.lambda, n, v, lam);
+  store5(f.work, n, v, P);
+  double es = 0.0, ee = 0.0;
+#pragma unroll
+  for (int c = 0; c < 5; ++c) {
+    acc[c * kStride] += s[c];
+    acc[(5 + c) * kStride] += e[c];
+    const double ds = s[c] - lam[c];
+    const double de = e[c] - cs.edot(c) - d[c];
+    es += ds * ds;
+    ee += de * de;
+  }
+  acc[10 * kStride] += sqrt(es);
+  acc[11 * kStride] += sqrt(ee);
+}
+
+// The per-voxel body of the fixed-point loop, FP64 (MaterialGrid.cpp:946-1003):
 //   sigma /= MaxRSS(sigma); sigma = SolveConstrained(...); edot = Apply(sigma);
 //   P = sigma - L0 d~; lambda += L0 (Edot + d~ - edot);
 // and the block partials of sum sigma, sum edot, sum |sigma - lambda|,
@@ -140,6 +181,7 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const C& cs, l
                                                const FieldPtrs<S>& f, double* partials,
                                                IterCtrl* ctrl, int blk, int nblk, MS* msm,
                                                MS* tsm) {
+  static_assert(sizeof(S) == 8, "the mixed path is nr_update_body_mixed");
   constexpr int bs = kVoxelBlock;  // every launch of these kernels uses kVoxelBlock threads
   double acc[12];
 #pragma unroll
@@ -158,75 +200,217 @@ __device__ __forceinline__ void nr_update_body(const NRParams& p, const C& cs, l
     for (int c = 0; c < 5; ++c) ed[c] = cs.edot(c) + d[c];
     double e[5];
     bool capped;
-    if constexpr (sizeof(S) == 4) {
-      // mixed precision: an FP32 Newton predictor from the previous stress,
-      // then the FP64 solve from its iterate (normally one Newton step with
-      // FP64 residual and Jacobian, its 5x5 system solved in FP32).  If the predictor fails, the FP64 solve
-      // starts where the reference's does, at sigma / MaxRSS.  The strain rate
-      // comes from the last Newton linearisation when that step was tiny.
-      float mx0;
-      double s0[5];
+    const double mx = max_resolved<kTauSmem>(msm, tsm, bs, p, s);
+    if (mx < 1e-10) status |= kStatusMaxRssTiny;
 #pragma unroll
-      for (int c = 0; c < 5; ++c) s0[c] = s[c];
-      const bool ok =
-          nr_predict_fp32<NEXP, kTauSmem, kFull>(msm, tsm, bs, p, cs, lam, ed, s, 8, &mx0);
-      if (mx0 < 1e-10f) status |= kStatusMaxRssTiny;
-      if (!ok) {
-        const double mx = max_resolved<kTauSmem>(msm, tsm, bs, p, s0);
-#pragma unroll
-        for (int c = 0; c < 5; ++c) s[c] = s0[c] / mx;
-      }
-      double el[5];
-      bool tight;
-      nr_constrained_smem<NEXP, kTauSmem, MS, C, true>(msm, tsm, bs, p, cs, lam, ed, s, nullptr,
-                                                       &capped, el, &tight);
-      if (!capped && tight) {
-#pragma unroll
-        for (int c = 0; c < 5; ++c) e[c] = el[c];
-      } else {
-        apply_smem<NEXP, kTauSmem>(msm, tsm, bs, p, s, e);
-      }
-    } else {
-      const double mx = max_resolved<kTauSmem>(msm, tsm, bs, p, s);
-      if (mx < 1e-10) status |= kStatusMaxRssTiny;
-#pragma unroll
-      for (int c = 0; c < 5; ++c) s[c] /= mx;
-      nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, cs, lam, ed, s, nullptr, &capped);
-      apply_smem<NEXP, kTauSmem>(msm, tsm, bs, p, s, e);
-    }
+    for (int c = 0; c < 5; ++c) s[c] /= mx;
+    nr_constrained_smem<NEXP, kTauSmem>(msm, tsm, bs, p, cs, lam, ed, s, nullptr, &capped);
+    apply_smem<NEXP, kTauSmem>(msm, tsm, bs, p, s, e);
     capped_count += capped ? 1 : 0;
-    double P[5];
-#pragma unroll
-    for (int i = 0; i < 5; ++i) {
-      double ld = 0.0, lt = 0.0;
-#pragma unroll
-      for (int j = 0; j < 5; ++j) {
-        const double l0 = cs.L0(j * 5 + i);
-        ld += l0 * d[j];
-        lt += l0 * (ed[j] - e[j]);
-      }
-      P[i] = s[i] - ld;
-      lam[i] += lt;
-    }
-    store5(f.sigma, n, v, s);
-    store5(f.lambda, n, v, lam);
-    store5(f.work, n, v, P);
-    double es = 0.0, ee = 0.0;
-#pragma unroll
-    for (int c = 0; c < 5; ++c) {
-      acc[c] += s[c];
-      acc[5 + c] += e[c];
-      const double ds = s[c] - lam[c];
-      const double de = e[c] - cs.edot(c) - d[c];
-      es += ds * ds;
-      ee += de * de;
-    }
-    acc[10] += sqrt(es);
-    acc[11] += sqrt(ee);
+    finish_voxel(cs, n, f, v, s, e, lam, d, ed, acc);
   }
   if (status) atomicOr(&ctrl->status, status);
   if (capped_count) atomicAdd(&ctrl->nr_capped, capped_count);
   block_reduce_store<12, kVoxelBlock>(acc, partials + (long long)blk * 12);
+}
+
+// Shared memory of the mixed sweep beyond the Schmid staging: the threads' 12
+// running sums (double [12][kVoxelBlock]) and, per warp, the queue of its
+// voxels that take the FP64 Newton step: kDeferCap voxel indices, with
+// kDeferRestart set when the FP32 predictor failed (the FP64 solve then starts
+// at sigma / MaxRSS from the previous stress; otherwise from the predicted
+// stress, which the voxel's lane has stored into sigma).
+constexpr int kDeferCap = 64;  // at most 31 waiting + 32 added in one round
+constexpr uint32_t kDeferRestart = 0x80000000u;
+template <typename MS>
+__host__ __device__ constexpr int nr_defer_smem_per_block() {
+  return sizeof(MS) == 4 ? kVoxelBlock * 12 * 8 + (kVoxelBlock / 32) * kDeferCap * 4 : 0;
+}
+
+// The FP64 Newton solve of one queued voxel (q: its warp's queue, k: the entry)
+// and the end of its update.  Returns whether its NR stopped at the cap.
+template <int NEXP, bool kTauSmem, class C>
+__device__ __forceinline__ bool fp64_step_queued(const NRParams& p, const C& cs, long long n,
+                                                 const FieldPtrs<float>& f, const uint32_t* q,
+                                                 int k, float* msm, float* tsm, double* acc) {
+  constexpr int bs = kVoxelBlock;
+  const uint32_t code = q[k];
+  const long long v = (long long)(code & ~kDeferRestart);
+  double s[5], lam[5], d[5], ed[5];
+  load5(f.sigma, n, v, s);
+  load5(f.lambda, n, v, lam);
+  load5(f.work, n, v, d);
+#pragma unroll
+  for (int c = 0; c < 5; ++c) ed[c] = cs.edot(c) + d[c];
+  voxel_schmid<kTauSmem>(f, n, v, msm, tsm, bs);
+  if (code & kDeferRestart) {
+    const double mx = max_resolved<kTauSmem>(msm, tsm, bs, p, s);
+#pragma unroll
+    for (int c = 0; c < 5; ++c) s[c] /= mx;
+  }
+  double el[5], e[5];
+  bool capped, tight;
+  nr_constrained_smem<NEXP, kTauSmem, float, C, true>(msm, tsm, bs, p, cs, lam, ed, s, nullptr,
+                                                      &capped, el, &tight);
+  if (!capped && tight) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) e[c] = el[c];
+  } else {
+    apply_smem<NEXP, kTauSmem>(msm, tsm, bs, p, s, e);
+  }
+  finish_voxel<kVoxelBlock>(cs, n, f, v, s, e, lam, d, ed, acc);
+  return capped;
+}
+
+// The per-voxel body of the fixed-point loop in mixed precision.  Each voxel
+// runs an FP32 Newton predictor from its previous stress (the reference's
+// iteration and stopping rule in single precision), then the FP64 residual at
+// the predicted point: the strain rate S(sigma) in FP64 and
+// y = L0^-1 (sigma - lambda) + S - Edot - d~.  Where the Newton step that
+// residual asks for, estimated with the predictor's last FP32 factors, is
+// below the certification bound (|step|^2 <= cert2 |sigma|^2), the predicted
+// stress is accepted with its FP64 strain rate and no step is taken.  Every
+// other voxel (and every voxel whose predictor failed) takes the FP64 Newton
+// step (FP64 residual and Jacobian, the small system solved in FP32): it is
+// queued in its warp's shared-memory queue, and whenever 32 are waiting the
+// warp solves them together, one per lane, so that the FP64 work runs in full
+// warps instead of the few lanes that need it in each group of 32 voxels.
+// The voxel -> warp assignment and the order of every sum are fixed, so the
+// results are deterministic run to run.
+template <int NEXP, bool kTauSmem, bool kFull, class C>
+__device__ __forceinline__ void nr_update_body_mixed(const NRParams& p, const C& cs, long long n,
+                                                     const FieldPtrs<float>& f, double* partials,
+                                                     IterCtrl* ctrl, int blk, int nblk,
+                                                     float* msm, float* tsm, uint32_t* q,
+                                                     double* acc) {
+  constexpr int bs = kVoxelBlock;  // every launch of these kernels uses kVoxelBlock threads
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < 12; ++k) acc[k * bs] = 0.0;
+  unsigned long long capped_count = 0, fp64_count = 0;
+  int status = 0;
+  int waiting = 0;  // queued voxels of this warp (warp-uniform)
+  const long long stride = (long long)nblk * bs;
+  for (long long base = (long long)blk * bs + (threadIdx.x & ~31); base < n; base += stride) {
+    const long long v = base + lane;
+    bool defer = false;
+    uint32_t code = 0;
+    // the voxel's FP32 fields; sp: the predictor's stress (from the previous one)
+    float sp[5], lam[5], d[5];
+    if (v < n) {
+      voxel_schmid<kTauSmem>(f, n, v, msm, tsm, bs);
+#pragma unroll
+      for (int c = 0; c < 5; ++c) {
+        sp[c] = f.sigma[c * n + v];
+        lam[c] = f.lambda[c * n + v];
+        d[c] = f.work[c * n + v];
+      }
+      if (f.dkeep) {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) f.dkeep[c * n + v] = d[c];
+      }
+      float e32[5];
+#pragma unroll
+      for (int c = 0; c < 5; ++c) e32[c] = (float)(cs.edot(c) + (double)d[c]);
+      float mx0;
+      Ldl5<float> fac;
+      const bool ok = nr_predict_fp32<NEXP, kTauSmem, kFull>(msm, tsm, bs, p, cs, lam, e32, sp, 8,
+                                                             &mx0, &fac);
+      if (mx0 < 1e-10f) status |= kStatusMaxRssTiny;
+      bool certified = false;
+      double s64[5], e[5];
+      if (ok) {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) s64[c] = (double)sp[c];
+        const bool adm = strain_rate_fp64<NEXP, kTauSmem>(msm, tsm, bs, p, s64, e);
+        float y[5], st[5];
+#pragma unroll
+        for (int i = 0; i < 5; ++i) {
+          double a = e[i] - (cs.edot(i) + (double)d[i]);
+#pragma unroll
+          for (int j = 0; j < 5; ++j) a += cs.L0inv(sym5(i, j)) * (s64[j] - (double)lam[j]);
+          y[i] = (float)(-a);
+        }
+        ldlt5_subst(fac, y, st);
+        float dn = 0.f, sn = 0.f;
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+          dn += st[c] * st[c];
+          sn += sp[c] * sp[c];
+        }
+        certified = adm && dn <= p.cert2_f * sn;
+      }
+      if (certified) {
+        double lamd[5], dd[5], ed[5];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+          lamd[c] = (double)lam[c];
+          dd[c] = (double)d[c];
+          ed[c] = cs.edot(c) + dd[c];
+        }
+        finish_voxel<bs>(cs, n, f, v, s64, e, lamd, dd, ed, acc);
+      } else {
+        defer = true;
+        code = (uint32_t)v | (ok ? 0u : kDeferRestart);
+        if (ok) {  // the FP64 step starts at the predicted stress
+#pragma unroll
+          for (int c = 0; c < 5; ++c) f.sigma[c * n + v] = sp[c];
+        }
+      }
+    }
+    const unsigned dm = __ballot_sync(0xffffffffu, defer);
+    if (defer) q[waiting + __popc(dm & ((1u << lane) - 1u))] = code;
+    waiting += __popc(dm);
+    if (waiting >= 32) {
+      __syncwarp();
+      waiting -= 32;
+      capped_count += fp64_step_queued<NEXP, kTauSmem>(p, cs, n, f, q, waiting + lane, msm, tsm,
+                                                       acc) ? 1 : 0;
+      fp64_count++;
+      __syncwarp();
+    }
+  }
+  __syncwarp();
+  if (lane < waiting) {
+    capped_count +=
+        fp64_step_queued<NEXP, kTauSmem>(p, cs, n, f, q, lane, msm, tsm, acc) ? 1 : 0;
+    fp64_count++;
+  }
+  if (status) atomicOr(&ctrl->status, status);
+  if (capped_count) atomicAdd(&ctrl->nr_capped, capped_count);
+  if (fp64_count) atomicAdd(&ctrl->nr_fp64, fp64_count);
+  double sums[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) sums[k] = acc[k * bs];
+  block_reduce_store<12, kVoxelBlock>(sums, partials + (long long)blk * 12);
+}
+
+// Dynamic shared memory of the loop's NR kernels: the Schmid staging, plus the
+// FP64-step queues of the mixed sweep.
+template <typename MS>
+__host__ __device__ constexpr size_t nr_loop_smem(bool tau) {
+  return (size_t)kVoxelBlock * nr_smem_per_thread<MS>(tau) + nr_defer_smem_per_block<MS>();
+}
+
+// The loop's per-voxel body for either precision.
+template <typename S, typename MS, int NEXP, bool kTauSmem, bool kFull, class C>
+__device__ __forceinline__ void nr_loop_body(const NRParams& p, const C& cs, long long n,
+                                             const FieldPtrs<S>& f, double* partials,
+                                             IterCtrl* ctrl, int blk, int nblk,
+                                             unsigned char* smem) {
+  MS* msm = reinterpret_cast<MS*>(smem) + SL<MS>::kThreadStride * threadIdx.x;
+  MS* tsm = msm + 60 * kVoxelBlock;
+  if constexpr (sizeof(S) == 4) {
+    unsigned char* extra = smem + (size_t)kVoxelBlock * nr_smem_per_thread<MS>(kTauSmem);
+    double* acc = reinterpret_cast<double*>(extra) + threadIdx.x;
+    uint32_t* q = reinterpret_cast<uint32_t*>(extra + kVoxelBlock * 12 * sizeof(double)) +
+                  (threadIdx.x >> 5) * kDeferCap;
+    nr_update_body_mixed<NEXP, kTauSmem, kFull>(p, cs, n, f, partials, ctrl, blk, nblk, msm, tsm,
+                                                q, acc);
+  } else {
+    nr_update_body<S, MS, NEXP, kTauSmem, kFull>(p, cs, n, f, partials, ctrl, blk, nblk, msm,
+                                                 tsm);
+  }
 }
 
 template <typename S, typename MS, int NEXP, bool kTauSmem>
@@ -235,10 +419,8 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_loop_min_blocks<MS>())
                 double* partials, IterCtrl* ctrl) {
   if (ctrl->done) return;
   extern __shared__ __align__(16) unsigned char nr_smem[];
-  MS* msm = reinterpret_cast<MS*>(nr_smem) + SL<MS>::kThreadStride * threadIdx.x;
-  MS* tsm = msm + 60 * kVoxelBlock;
-  nr_update_body<S, MS, NEXP, kTauSmem, true>(p, ParamConsts{p}, p.n, f, partials, ctrl,
-                                              blockIdx.x, gridDim.x, msm, tsm);
+  nr_loop_body<S, MS, NEXP, kTauSmem, true>(p, ParamConsts{p}, p.n, f, partials, ctrl, blockIdx.x,
+                                            gridDim.x, nr_smem);
 }
 
 template <typename S, typename MS, int NEXP, bool kTauSmem>
@@ -254,12 +436,10 @@ __global__ void __launch_bounds__(kVoxelBlock, nr_loop_batch_min_blocks<MS>())
   copy_struct(&sp, &d.nr);
   copy_struct(&sf, &d.f);
   __syncthreads();
-  MS* msm = reinterpret_cast<MS*>(nr_smem) + SL<MS>::kThreadStride * threadIdx.x;
-  MS* tsm = msm + 60 * kVoxelBlock;
   // material and solver constants (the same for every RVE of a batch) from the
   // kernel parameter; the slot's strain rate and reference medium from shared memory
-  nr_update_body<S, MS, NEXP, kTauSmem, false>(pm, SharedConsts{&sp}, sp.n, sf, d.partials,
-                                               d.ctrl, lb, d.nr_blocks, msm, tsm);
+  nr_loop_body<S, MS, NEXP, kTauSmem, false>(pm, SharedConsts{&sp}, sp.n, sf, d.partials, d.ctrl,
+                                             lb, d.nr_blocks, nr_smem);
 }
 
 
@@ -309,7 +489,7 @@ template <typename S, int NEXP, bool TAU>
 int nr_t(const NRParams& p, const FieldPtrs<S>& f, double* partials, IterCtrl* ctrl, double* hist,
          cudaStream_t st, cudaEvent_t* ev) {
   auto kern = k_nr_update<S, S, NEXP, TAU>;
-  const size_t smem = (size_t)kVoxelBlock * nr_smem_per_thread<S>(TAU);
+  const size_t smem = nr_loop_smem<S>(TAU);
   const int nb = persistent_blocks((const void*)kern, smem, p.n);
   kern<<<nb, kVoxelBlock, smem, st>>>(p, f, partials, ctrl);
   if (ev) cudaEventRecord(ev[0], st);
@@ -320,7 +500,8 @@ int nr_t(const NRParams& p, const FieldPtrs<S>& f, double* partials, IterCtrl* c
 
 template <typename S, int NEXP, bool TAU>
 int blocks_t(const NRParams& p, bool init) {
-  const size_t smem = (size_t)kVoxelBlock * nr_smem_per_thread<S>(TAU);
+  const size_t smem = init ? (size_t)kVoxelBlock * nr_smem_per_thread<S>(TAU)
+                           : nr_loop_smem<S>(TAU);
   const void* kern = init ? (const void*)k_init<S, S, NEXP, TAU>
                           : (const void*)k_nr_update<S, S, NEXP, TAU>;
   return persistent_blocks(kern, smem, p.n);
@@ -345,7 +526,7 @@ template <typename S, int NEXP, bool TAU>
 int nr_batch_t(const SlotDesc<S>* d, const BatchLaunch& bl, const BatchLaunch& bls,
                const NRParams& material, cudaStream_t st) {
   auto kern = k_nr_update_batch<S, S, NEXP, TAU>;
-  const size_t smem = (size_t)kVoxelBlock * nr_smem_per_thread<S>(TAU);
+  const size_t smem = nr_loop_smem<S>(TAU);
   smem_optin(kern, smem);
   kern<<<bl.blocks, kVoxelBlock, smem, st>>>(d, bl, material);
   k_iter_finish_batch<S><<<bls.m, kFinishThreads, 0, st>>>(d, bls);
