@@ -187,6 +187,38 @@ __device__ __forceinline__ void schmid_to_smem(const MS R[9], MS* msm, int bs) {
   });
 }
 
+// The FP32 staging of schmid_to_smem with paired arithmetic: systems q and q+1
+// in the two lanes of a float2 (FMUL2/FFMA2), stored as one 8-byte value per
+// component at the pair-interleaved offsets of SL<float>.  q11 - q00 is
+// formed as fma(q00, -1, q11), which rounds like the subtraction.
+__device__ __forceinline__ void schmid_to_smem_pairs(const float R[9], float* msm, int bs) {
+  float2* m2 = reinterpret_cast<float2*>(msm);
+  const float2 c23 = make_float2((float)VPFFT_INV_2SQRT3, (float)VPFFT_INV_2SQRT3);
+  const float2 c6 = make_float2((float)(1.0 / 6.0), (float)(1.0 / 6.0));
+  const float2 m1 = make_float2(-1.f, -1.f), two = make_float2(2.f, 2.f);
+  static_for_s<0, kNS / 2>([&](auto pc) {
+    constexpr int pq = decltype(pc)::value;
+    float ba[3], na[3], bb[3], nb[3];
+    rotated_slip<2 * pq>(R, ba, na);
+    rotated_slip<2 * pq + 1>(R, bb, nb);
+    float2 b[3], n[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      b[i] = make_float2(ba[i], bb[i]);
+      n[i] = make_float2(na[i], nb[i]);
+    }
+    const float2 q00 = __fmul2_rn(b[0], n[0]), q11 = __fmul2_rn(b[1], n[1]);
+    const float2 q22 = __fmul2_rn(b[2], n[2]);
+    float2 t = __ffma2_rn(q00, m1, __fmul2_rn(q22, two));
+    t = __ffma2_rn(q11, m1, t);
+    m2[(pq * 5 + 0) * bs] = __fmul2_rn(__ffma2_rn(q00, m1, q11), c23);
+    m2[(pq * 5 + 1) * bs] = __fmul2_rn(t, c6);
+    m2[(pq * 5 + 2) * bs] = __fmul2_rn(__ffma2_rn(b[1], n[2], __fmul2_rn(b[2], n[1])), c23);
+    m2[(pq * 5 + 3) * bs] = __fmul2_rn(__ffma2_rn(b[0], n[2], __fmul2_rn(b[2], n[0])), c23);
+    m2[(pq * 5 + 4) * bs] = __fmul2_rn(__ffma2_rn(b[0], n[1], __fmul2_rn(b[1], n[0])), c23);
+  });
+}
+
 template <typename MS>
 __device__ __forceinline__ void load_m(const MS* msm, int bs, int s, double m[5]) {
 #pragma unroll

@@ -50,10 +50,20 @@ __device__ __forceinline__ void voxel_schmid(const FieldPtrs<S>& f, long long n,
   MS R[9];
 #pragma unroll
   for (int k = 0; k < 9; ++k) R[k] = (MS)f.R[k * n + v];
-  schmid_to_smem<MS>(R, msm, bs);
+  if constexpr (sizeof(MS) == 4)
+    schmid_to_smem_pairs(R, msm, bs);
+  else
+    schmid_to_smem<MS>(R, msm, bs);
   if constexpr (kTauSmem) {
+    // 1/CRSS: IEEE FP64 division for the FP64 path, the correctly rounded
+    // FP32 reciprocal of the FP32 CRSS for the mixed path's FP32 staging
 #pragma unroll
-    for (int q = 0; q < kNS; ++q) tsm[SL<MS>::t(q, bs)] = (MS)(1.0 / (double)f.crss[q * n + v]);
+    for (int q = 0; q < kNS; ++q) {
+      if constexpr (sizeof(MS) == 4)
+        tsm[SL<MS>::t(q, bs)] = __frcp_rn((float)f.crss[q * n + v]);
+      else
+        tsm[SL<MS>::t(q, bs)] = (MS)(1.0 / (double)f.crss[q * n + v]);
+    }
   }
 }
 
