@@ -444,9 +444,9 @@ __device__ __forceinline__ bool accumulate_pairs(const float* msm, const float* 
 // caller then takes the accepted step with FP64 residual and Jacobian.
 // *rmax0 gets max_s |r_s| at the starting point.
 // fac (optional): the LDL^T factors of the converged step's Newton matrix.
-template <int NEXP, bool kTauSmem, bool kFull = true, typename MS, class C>
 // l32, e32: lambda and Edot + d~ rounded to FP32; cur: the starting stress in,
 // the converged iterate out (undefined when the predictor fails).
+template <int NEXP, bool kTauSmem, bool kFull = true, typename MS, class C>
 __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, int bs,
                                                 const NRParams& p, const C& cs,
                                                 const float l32[5], const float e32[5],
