@@ -191,7 +191,11 @@ __device__ __forceinline__ void schmid_to_smem(const MS R[9], MS* msm, int bs) {
 // in the two lanes of a float2 (FMUL2/FFMA2), stored as one 8-byte value per
 // component at the pair-interleaved offsets of SL<float>.  q11 - q00 is
 // formed as fma(q00, -1, q11), which rounds like the subtraction.
-__device__ __forceinline__ void schmid_to_smem_pairs(const float R[9], float* msm, int bs) {
+// (A template, so that only the sm_100a device code that calls it instantiates
+// the paired intrinsics.)
+template <typename T = float>
+__device__ __forceinline__ void schmid_to_smem_pairs(const T R[9], T* msm, int bs) {
+  static_assert(sizeof(T) == 4, "FP32 staging");
   float2* m2 = reinterpret_cast<float2*>(msm);
   const float2 c23 = make_float2((float)VPFFT_INV_2SQRT3, (float)VPFFT_INV_2SQRT3);
   const float2 c6 = make_float2((float)(1.0 / 6.0), (float)(1.0 / 6.0));
