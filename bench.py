@@ -397,15 +397,17 @@ def batched_arm(n_rves: int) -> dict:
     }
 
 
-def serving_arm(n_requests: int) -> dict:
+def serving_arm(n_requests: int, budget: int = 256 << 20) -> dict:
     """Serving: Poisson arrivals (mean 500/s) of one-increment requests on a
     pool of 64 persistent RVEs with edges {32, 48, 64, 96} (weights
     0.4/0.3/0.2/0.1), each request with its own random traceless velocity
-    gradient; continuous batching through one mixed-precision batch."""
+    gradient; continuous batching through one mixed-precision batch.  The HBM
+    budget for the requests' spectra (256 MiB) is about half of what all 64
+    RVEs in flight would hold, so admission waits for memory as well as for
+    slots (the line counts those waits)."""
     import vpfft_b200 as vp
     from vpfft_b200 import serving
 
-    budget = 2 << 30
     sizes, weights = [32, 48, 64, 96], [0.4, 0.3, 0.2, 0.1]
     b = vp.Batch("mixed", material=material_n10(), max_slots=64, iterations_per_tick=4,
                  hbm_budget_bytes=budget)
