@@ -34,11 +34,11 @@ def material(n=20):
                        theta0=20.0, theta1=1.0)
 
 
-def run(precision, certify=None, n=20):
-    R = fixtures.polycrystal(*DIMS, GRAINS, SEED)
+def run(precision, certify=None, n=20, dims=DIMS):
+    R = fixtures.polycrystal(*dims, GRAINS, SEED)
     e = fixtures.edot_from_matrix(np.diag([1.0, 0.0, -1.0]))
     opts = capi.solver_options(mixed_certify_step=certify) if certify is not None else None
-    g = vp.MaterialGrid(*DIMS, material=material(n), precision=precision, options=opts)
+    g = vp.MaterialGrid(*dims, material=material(n), precision=precision, options=opts)
     g.SendDataAndInitialize(R, None)
     g.InitializeComputation(e)
     g.BuildLinearRefMediumStiffness()
@@ -48,13 +48,15 @@ def run(precision, certify=None, n=20):
     return out
 
 
-@pytest.mark.parametrize("n", [20, 7])
-def test_certified_and_queued_steps_against_fp64(lib, n):
-    nvox = int(np.prod(DIMS))
-    h64, s64, k64 = run("fp64", n=n)
+# (15, 12, 10): 1800 voxels, not a multiple of 32, so the last warp of the
+# sweep is partial and its queue is flushed part-full
+@pytest.mark.parametrize("n,dims", [(20, DIMS), (7, DIMS), (20, (15, 12, 10))])
+def test_certified_and_queued_steps_against_fp64(lib, n, dims):
+    nvox = int(np.prod(dims))
+    h64, s64, k64 = run("fp64", n=n, dims=dims)
     assert k64 == 0
-    hd, sd, kd = run("mixed", n=n)
-    h0, s0, k0 = run("mixed", 0.0, n=n)
+    hd, sd, kd = run("mixed", n=n, dims=dims)
+    h0, s0, k0 = run("mixed", 0.0, n=n, dims=dims)
     assert k0 == nvox * ITERS  # bound 0: every voxel-iteration took the FP64 step
     assert 0 <= kd < k0
     print(f"\nn={n}: FP64 steps per voxel-iteration, default bound {kd / (nvox * ITERS):.2e}")
