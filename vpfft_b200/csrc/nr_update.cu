@@ -1,6 +1,7 @@
 // nr_update.cu -- the Newton-Raphson kernels of the initialisation and of the
 // fixed-point loop (see nr_kernel.cuh for the per-voxel arithmetic), their
 // launchers, and the batched Solvers entry points built on the same code.
+#include <cuda_pipeline.h>
 #include <cuda_runtime.h>
 
 #include <map>
@@ -287,12 +288,15 @@ __device__ __forceinline__ bool fp64_step_queued(const NRParams& p, const C& cs,
 // warps instead of the few lanes that need it in each group of 32 voxels.
 // The voxel -> warp assignment and the order of every sum are fixed, so the
 // results are deterministic run to run.
-template <int NEXP, bool kTauSmem, bool kFull, class C>
+// kPrefetch: each thread copies its next voxel's fields (R, sigma, lambda, d~)
+// into its column of pf with asynchronous copies while it solves the current
+// one, so their global-memory latency is not exposed at the start of a voxel.
+template <int NEXP, bool kTauSmem, bool kFull, bool kPrefetch, class C>
 __device__ __forceinline__ void nr_update_body_mixed(const NRParams& p, const C& cs, long long n,
                                                      const FieldPtrs<float>& f, double* partials,
                                                      IterCtrl* ctrl, int blk, int nblk,
                                                      float* msm, float* tsm, uint32_t* q,
-                                                     double* acc) {
+                                                     double* acc, float* pf) {
   constexpr int bs = kVoxelBlock;  // every launch of these kernels uses kVoxelBlock threads
   const int lane = threadIdx.x & 31;
 #pragma unroll
@@ -301,19 +305,53 @@ __device__ __forceinline__ void nr_update_body_mixed(const NRParams& p, const C&
   int status = 0;
   int waiting = 0;  // queued voxels of this warp (warp-uniform)
   const long long stride = (long long)nblk * bs;
+  auto prefetch = [&](long long w) {
+    if (w < n) {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) __pipeline_memcpy_async(&pf[k * bs], &f.R[k * n + w], 4);
+#pragma unroll
+      for (int c = 0; c < 5; ++c) {
+        __pipeline_memcpy_async(&pf[(9 + c) * bs], &f.sigma[c * n + w], 4);
+        __pipeline_memcpy_async(&pf[(14 + c) * bs], &f.lambda[c * n + w], 4);
+        __pipeline_memcpy_async(&pf[(19 + c) * bs], &f.work[c * n + w], 4);
+      }
+    }
+    __pipeline_commit();
+  };
+  if constexpr (kPrefetch) prefetch((long long)blk * bs + threadIdx.x);
   for (long long base = (long long)blk * bs + (threadIdx.x & ~31); base < n; base += stride) {
     const long long v = base + lane;
     bool defer = false;
     uint32_t code = 0;
     // the voxel's FP32 fields; sp: the predictor's stress (from the previous one)
     float sp[5], lam[5], d[5];
+    if constexpr (kPrefetch) __pipeline_wait_prior(0);
     if (v < n) {
-      voxel_schmid<kTauSmem>(f, n, v, msm, tsm, bs);
+      if constexpr (kPrefetch) {
+        float R[9];
 #pragma unroll
-      for (int c = 0; c < 5; ++c) {
-        sp[c] = f.sigma[c * n + v];
-        lam[c] = f.lambda[c * n + v];
-        d[c] = f.work[c * n + v];
+        for (int k = 0; k < 9; ++k) R[k] = pf[k * bs];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+          sp[c] = pf[(9 + c) * bs];
+          lam[c] = pf[(14 + c) * bs];
+          d[c] = pf[(19 + c) * bs];
+        }
+        prefetch(v + stride);
+        schmid_to_smem_pairs(R, msm, bs);
+        if constexpr (kTauSmem) {
+#pragma unroll
+          for (int q2 = 0; q2 < kNS; ++q2)
+            tsm[SL<float>::t(q2, bs)] = __frcp_rn(f.crss[q2 * n + v]);
+        }
+      } else {
+        voxel_schmid<kTauSmem>(f, n, v, msm, tsm, bs);
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+          sp[c] = f.sigma[c * n + v];
+          lam[c] = f.lambda[c * n + v];
+          d[c] = f.work[c * n + v];
+        }
       }
       if (f.dkeep) {
 #pragma unroll
@@ -396,10 +434,13 @@ __device__ __forceinline__ void nr_update_body_mixed(const NRParams& p, const C&
 }
 
 // Dynamic shared memory of the loop's NR kernels: the Schmid staging, plus the
-// FP64-step queues of the mixed sweep.
+// FP64-step queues and running sums of the mixed sweep, plus (single-grid
+// mixed sweep) the prefetch staging of the next voxel's fields.
+constexpr int kPrefetchWords = 24;  // R (9), sigma, lambda, d~ (5 each)
 template <typename MS>
-__host__ __device__ constexpr size_t nr_loop_smem(bool tau) {
-  return (size_t)kVoxelBlock * nr_smem_per_thread<MS>(tau) + nr_defer_smem_per_block<MS>();
+__host__ __device__ constexpr size_t nr_loop_smem(bool tau, bool prefetch = false) {
+  return (size_t)kVoxelBlock * nr_smem_per_thread<MS>(tau) + nr_defer_smem_per_block<MS>() +
+         (prefetch && sizeof(MS) == 4 ? (size_t)kVoxelBlock * kPrefetchWords * 4 : 0);
 }
 
 // The loop's per-voxel body for either precision.
@@ -415,8 +456,13 @@ __device__ __forceinline__ void nr_loop_body(const NRParams& p, const C& cs, lon
     double* acc = reinterpret_cast<double*>(extra) + threadIdx.x;
     uint32_t* q = reinterpret_cast<uint32_t*>(extra + kVoxelBlock * 12 * sizeof(double)) +
                   (threadIdx.x >> 5) * kDeferCap;
-    nr_update_body_mixed<NEXP, kTauSmem, kFull>(p, cs, n, f, partials, ctrl, blk, nblk, msm, tsm,
-                                                q, acc);
+    // the single-grid sweep (kFull) prefetches; the batched one, whose threads
+    // have one or two voxels each in small RVEs, does not
+    float* pf = kFull ? reinterpret_cast<float*>(extra + (size_t)nr_defer_smem_per_block<MS>()) +
+                            threadIdx.x
+                      : nullptr;
+    nr_update_body_mixed<NEXP, kTauSmem, kFull, kFull>(p, cs, n, f, partials, ctrl, blk, nblk,
+                                                       msm, tsm, q, acc, pf);
   } else {
     nr_update_body<S, MS, NEXP, kTauSmem, kFull>(p, cs, n, f, partials, ctrl, blk, nblk, msm,
                                                  tsm);
@@ -499,7 +545,7 @@ template <typename S, int NEXP, bool TAU>
 int nr_t(const NRParams& p, const FieldPtrs<S>& f, double* partials, IterCtrl* ctrl, double* hist,
          cudaStream_t st, cudaEvent_t* ev) {
   auto kern = k_nr_update<S, S, NEXP, TAU>;
-  const size_t smem = nr_loop_smem<S>(TAU);
+  const size_t smem = nr_loop_smem<S>(TAU, true);
   const int nb = persistent_blocks((const void*)kern, smem, p.n);
   kern<<<nb, kVoxelBlock, smem, st>>>(p, f, partials, ctrl);
   if (ev) cudaEventRecord(ev[0], st);
@@ -511,7 +557,7 @@ int nr_t(const NRParams& p, const FieldPtrs<S>& f, double* partials, IterCtrl* c
 template <typename S, int NEXP, bool TAU>
 int blocks_t(const NRParams& p, bool init) {
   const size_t smem = init ? (size_t)kVoxelBlock * nr_smem_per_thread<S>(TAU)
-                           : nr_loop_smem<S>(TAU);
+                           : nr_loop_smem<S>(TAU, true);
   const void* kern = init ? (const void*)k_init<S, S, NEXP, TAU>
                           : (const void*)k_nr_update<S, S, NEXP, TAU>;
   return persistent_blocks(kern, smem, p.n);
