@@ -65,8 +65,10 @@ typedef enum {
 
 typedef enum {
   VPFFT_PREC_FP64 = 0,  /* everything in FP64: the GPU oracle path */
-  VPFFT_PREC_MIXED = 1  /* FP32 fields, FFT and Green operator; FP64 Newton-Raphson
-                           residual/Jacobian and FP64 compensated reductions */
+  VPFFT_PREC_MIXED = 1  /* FP32 fields, FFT and Green operator; an FP32 Newton predictor
+                           whose stress an FP64 residual certifies, else an FP64 Newton
+                           step (FP64 residual and Jacobian); FP64 reductions with a
+                           compensated final sum (vpfft_solver_options.mixed_certify_step) */
 } vpfft_precision;
 
 /* Per-slip-system material constants.  The reference hard-codes them in
