@@ -307,7 +307,7 @@ def green_operator_arm(edges=(64, 128, 256)) -> dict:
     return out
 
 
-def batched_arm(n_rves: int) -> dict:
+def batched_arm(n_rves: int, iterations_per_tick: int = 8) -> dict:
     """Batched RVE solves: n_rves RVEs with edges uniform in {16, 32, 48, 64},
     8-200 Voronoi grains, random traceless velocity gradients (equivalent
     strain rate 1), n = 10, one increment each (max 100 iterations, eps 1e-5),
@@ -325,7 +325,8 @@ def batched_arm(n_rves: int) -> dict:
     voxels = sum(e ** 3 for e, _ in specs)
 
     def run_batch(precision, grids):
-        b = vp.Batch(precision, material=mat, max_slots=len(grids))
+        b = vp.Batch(precision, material=mat, max_slots=len(grids),
+                     iterations_per_tick=iterations_per_tick)
         gs = [b.new_grid(e, e, e) for e, _ in grids]
         return b, gs
 
