@@ -503,14 +503,17 @@ __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, in
 // The strain rate S(s) = sum_s m_s gdot_s |r_s|^(n-1) r_s in FP64 and the
 // admissibility of s (every |r_s| within the cap): the FP64 residual pass of
 // the mixed path, the S half of `accumulate` for the constrained solver.
-template <int NEXP, bool kTauSmem, typename MS>
+// kFull: the pass over the 12 systems fully unrolled (the single-grid sweep:
+// measured 4.7 % faster at 256^3 than by 2), else by 2 (the batched sweep,
+// which has 128 registers).
+template <int NEXP, bool kTauSmem, bool kFull = true, typename MS>
 __device__ __forceinline__ bool strain_rate_fp64(const MS* msm, const MS* tsm, int bs,
                                                  const NRParams& p, const double s[5],
                                                  double S[5]) {
   bool adm = true;
 #pragma unroll
   for (int c = 0; c < 5; ++c) S[c] = 0.0;
-#pragma unroll 2
+#pragma unroll(kFull ? kNS : 2)
   for (int q = 0; q < kNS; ++q) {
     double m[5];
     load_m(msm, bs, q, m);

@@ -370,7 +370,7 @@ __device__ __forceinline__ void nr_update_body_mixed(const NRParams& p, const C&
       if (ok) {
 #pragma unroll
         for (int c = 0; c < 5; ++c) s64[c] = (double)sp[c];
-        const bool adm = strain_rate_fp64<NEXP, kTauSmem>(msm, tsm, bs, p, s64, e);
+        const bool adm = strain_rate_fp64<NEXP, kTauSmem, kFull>(msm, tsm, bs, p, s64, e);
         float y[5], st[5];
 #pragma unroll
         for (int i = 0; i < 5; ++i) {
