@@ -939,11 +939,11 @@ def main(argv=None):
 # divided by the voxel count) from the ncu capture at 192^3 summarised in
 # profiles/k_nr_update_192cubed_mixed.md; the kernel's traffic is proportional to
 # the voxel count (it streams each voxel's fields once), so it scales to 256^3.
-TRAFFIC_PER_VOXEL: dict = {("mixed", "nr_update"): 1055.53e6 / 192 ** 3}
+TRAFFIC_PER_VOXEL: dict = {("mixed", "nr_update"): 1055.5e6 / 192 ** 3}
 # Warp instructions per voxel of one launch (smsp__inst_executed.sum divided by
 # the voxel count) from the same capture; the per-voxel instruction count does
 # not depend on the grid size (each voxel's solve is independent of it).
-WARP_INST_PER_VOXEL: dict = {("mixed", "nr_update"): 0.7228e9 / 192 ** 3}
+WARP_INST_PER_VOXEL: dict = {("mixed", "nr_update"): 0.6927e9 / 192 ** 3}
 
 
 if __name__ == "__main__":
