@@ -504,8 +504,9 @@ __device__ __forceinline__ bool nr_predict_fp32(const MS* msm, const MS* tsm, in
 // admissibility of s (every |r_s| within the cap): the FP64 residual pass of
 // the mixed path, the S half of `accumulate` for the constrained solver.
 // kFull: the pass over the 12 systems fully unrolled (the single-grid sweep:
-// measured 4.7 % faster at 256^3 than by 2), else by 2 (the batched sweep,
-// which has 128 registers).
+// measured 4.7 % faster at 256^3 than by 2), else by 4 (the batched sweep,
+// which has 128 registers: 388 solves/s against 377-384 by 2 and 382 fully
+// unrolled on the 256-RVE workload).
 template <int NEXP, bool kTauSmem, bool kFull = true, typename MS>
 __device__ __forceinline__ bool strain_rate_fp64(const MS* msm, const MS* tsm, int bs,
                                                  const NRParams& p, const double s[5],
@@ -513,7 +514,7 @@ __device__ __forceinline__ bool strain_rate_fp64(const MS* msm, const MS* tsm, i
   bool adm = true;
 #pragma unroll
   for (int c = 0; c < 5; ++c) S[c] = 0.0;
-#pragma unroll(kFull ? kNS : 2)
+#pragma unroll(kFull ? kNS : 4)
   for (int q = 0; q < kNS; ++q) {
     double m[5];
     load_m(msm, bs, q, m);
