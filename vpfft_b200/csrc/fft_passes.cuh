@@ -18,7 +18,7 @@
 // kz ny + ky), so a tile may span several rows of a small grid.  Global reads
 // and writes go in runs that are contiguous in the layout being read or
 // written; the transpose between the two happens in the shared-memory tile.
-// No multicast or cluster features are used.
+// No thread-block cluster features are used.
 #pragma once
 
 #include <cuda_runtime.h>

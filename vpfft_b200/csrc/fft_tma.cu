@@ -16,7 +16,8 @@
 //     box, and a 3D tiled TMA store writes it; the store drains while the
 //     next tile is loaded and transformed (bulk async-group, waited on only
 //     before the staging box is rewritten).
-// Only this GPU's memory is addressed; no load uses cluster multicast.  Box
+// Only this GPU's memory is addressed; every load fills its own block's
+// shared memory only (no cluster-wide delivery).  Box
 // coordinates along the innermost axis are multiples of the tile's lines
 // (>= 8 complex values), so every box starts on a 16-byte boundary.
 //
