@@ -37,6 +37,25 @@ def test_unsupported_sizes_rejected(lib):
             capi.ERR_UNSUPPORTED_SIZE
 
 
+def test_solver_option_defaults_and_checks(lib):
+    """The reference's NR constants by default, the mixed-precision certificate
+    bound 1e-5; options out of range are refused before any device work."""
+    o = capi.solver_options()
+    assert (o.nr_epsilon, o.nr_max_iter, o.nr_max_resolved) == (5e-4, 100, 1e9)
+    assert (o.init_nr_epsilon, o.init_nr_max_iter) == (5e-4, 1000)
+    assert o.mixed_certify_step == 1e-5 and o.green_operator == 0
+    assert capi.solver_options(mixed_certify_step=0.0).mixed_certify_step == 0.0
+    h = C.c_void_p()
+    for bad in (-1e-6, 0.5, float("nan")):
+        opt = capi.solver_options(mixed_certify_step=bad)
+        st = lib.vpfft_grid_create(8, 8, 8, None, C.byref(opt), capi.PREC_MIXED, C.byref(h))
+        assert st == capi.ERR_INVALID_ARGUMENT, bad
+        assert b"mixed_certify_step" in lib.vpfft_last_error(None)
+    opt = capi.solver_options(green_operator=3)
+    assert lib.vpfft_grid_create(8, 8, 8, None, C.byref(opt), capi.PREC_MIXED,
+                                 C.byref(h)) == capi.ERR_INVALID_ARGUMENT
+
+
 def test_material_defaults_are_the_reference_constants(lib):
     m = capi.Material()
     lib.vpfft_material_default(C.byref(m))
